@@ -1,0 +1,230 @@
+"""ctypes mirror of ``include/fdtd_b200.h`` and the library loader.
+
+The library is built in-tree (``beamz_b200/_fdtd_b200.so``).  Loading checks
+the ABI version and ``sizeof(FdtdProgram)`` against this mirror before any
+launch, the way beamz validates its extension manifest
+(beamz/simulation/backend.py:139-157).  There is no fallback: when the library
+is missing or mismatched, :class:`CudaBackendUnavailable` is raised.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
+
+FDTD_ABI_VERSION = 1
+FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
+FDTD_FLAG_GRAPH_CACHE = 1 << 7
+FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
+FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL = 0, 1
+FDTD_TIMING_PRE_E, FDTD_TIMING_H, FDTD_TIMING_E = 0, 1, 2
+FDTD_MAX_SOURCES = 16
+FDTD_MAX_MONITORS = 16
+TIMINGS = {"pre_e": FDTD_TIMING_PRE_E, "h": FDTD_TIMING_H, "e": FDTD_TIMING_E}
+# Wall bits (front, back, bottom, top, left, right), beamz/simulation/cuda/runtime.py:38-40.
+EDGE_BITS = {"front": 0, "back": 1, "bottom": 2, "top": 3, "left": 4, "right": 5}
+
+#: Every symbol ``include/fdtd_b200.h`` declares.
+EXPORTED_SYMBOLS = (
+    "fdtd_abi_version",
+    "fdtd_program_size",
+    "fdtd_validate",
+    "fdtd_launch_phase",
+    "fdtd_launch_program",
+    "fdtd_apply_sources",
+    "fdtd_accumulate_dft",
+    "fdtd_clear_graph_cache",
+    "fdtd_error_string",
+)
+
+
+class CudaBackendUnavailable(RuntimeError):
+    """The native library is missing, mismatched, or no CUDA device is usable."""
+
+
+class FdtdError(RuntimeError):
+    """A native call returned a non-zero CUDA error code."""
+
+    def __init__(self, code: int, name: str, where: str):
+        super().__init__(f"{where} failed: {code} ({name})")
+        self.code = code
+        self.name = name
+
+
+class FdtdBuffer(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("rank", ctypes.c_int32),
+        ("element_type", ctypes.c_int32),
+        ("dims", ctypes.c_int64 * 4),
+    ]
+
+
+class FdtdCpmlTerm(ctypes.Structure):
+    _fields_ = [
+        ("axis", ctypes.c_int32),
+        ("low", ctypes.c_int32),
+        ("high", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("a", FdtdBuffer),
+        ("b", FdtdBuffer),
+        ("inv_kappa", FdtdBuffer),
+        ("psi", FdtdBuffer),
+        ("psi_alt", FdtdBuffer),
+    ]
+
+
+class FdtdSource(ctypes.Structure):
+    _fields_ = [
+        ("component", ctypes.c_int32),
+        ("timing", ctypes.c_int32),
+        ("start", ctypes.c_int32 * 3),
+        ("reserved", ctypes.c_int32),
+        ("coeff", FdtdBuffer),
+        ("waveform", FdtdBuffer),
+    ]
+
+
+class FdtdDft(ctypes.Structure):
+    _fields_ = [
+        ("monitor_count", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("indices", FdtdBuffer),
+        ("weights", FdtdBuffer),
+        ("freqs", FdtdBuffer),
+        ("masks", FdtdBuffer),
+        ("counts", FdtdBuffer),
+        ("codes", FdtdBuffer),
+        ("windows", FdtdBuffer),
+        ("re", FdtdBuffer),
+        ("im", FdtdBuffer),
+        ("weight_sum", FdtdBuffer),
+    ]
+
+
+class FdtdProgram(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("polarization", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("material_kind", ctypes.c_int32),
+        ("metallic_edges", ctypes.c_int32),
+        ("cpml", ctypes.c_int32),
+        ("nsteps", ctypes.c_int32),
+        ("source_count", ctypes.c_int32),
+        ("cells", ctypes.c_int64 * 3),
+        ("dt", ctypes.c_float),
+        ("resolution", ctypes.c_float),
+        ("inv_resolution", ctypes.c_float),
+        ("dt_over_eps", ctypes.c_float),
+        ("dt_over_mu", ctypes.c_float),
+        ("h_source", ctypes.c_float),
+        ("tile_x", ctypes.c_int32),
+        ("tile_y", ctypes.c_int32),
+        ("z_chunk", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("fields", FdtdBuffer * 6),
+        ("fields_alt", FdtdBuffer * 6),
+        ("e_decay", FdtdBuffer * 3),
+        ("e_source", FdtdBuffer * 3),
+        ("h_decay", FdtdBuffer * 3),
+        ("h_source_site", FdtdBuffer * 3),
+        ("voxels", FdtdBuffer),
+        ("eps_table", FdtdBuffer),
+        ("h_terms", FdtdCpmlTerm * 6),
+        ("e_terms", FdtdCpmlTerm * 6),
+        ("sources", FdtdSource * FDTD_MAX_SOURCES),
+        ("dft", FdtdDft),
+        ("step_counter", FdtdBuffer),
+        ("step_time", FdtdBuffer),
+    ]
+
+
+_TORCH_DTYPES = None
+
+
+def buffer_of(tensor) -> FdtdBuffer:
+    """Describe a contiguous torch tensor (device memory) as an FdtdBuffer."""
+    global _TORCH_DTYPES
+    import torch
+
+    if _TORCH_DTYPES is None:
+        _TORCH_DTYPES = {torch.float32: FDTD_F32, torch.int32: FDTD_S32, torch.bfloat16: FDTD_BF16,
+                         torch.uint8: FDTD_U8}
+    buf = FdtdBuffer()
+    if tensor is None:
+        return buf
+    if not tensor.is_contiguous():
+        raise ValueError("FDTD buffers must be contiguous")
+    if tensor.dim() > 4:
+        raise ValueError("FDTD buffers have rank <= 4")
+    buf.data = tensor.data_ptr() if tensor.numel() else None
+    buf.rank = tensor.dim()
+    buf.element_type = _TORCH_DTYPES[tensor.dtype]
+    for a, n in enumerate(tensor.shape):
+        buf.dims[a] = int(n)
+    return buf
+
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+def load_library(path: str | None = None):
+    """Load and check the native library (no GPU needed)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is not None and path is None:
+            return _LIB
+        lib_path = path or LIB_PATH
+        if not os.path.exists(lib_path):
+            raise CudaBackendUnavailable(
+                f"{lib_path} is missing; build it with `python -m beamz_b200.build`"
+            )
+        try:
+            lib = ctypes.CDLL(lib_path)
+        except OSError as exc:  # pragma: no cover - loader failure
+            raise CudaBackendUnavailable(f"cannot load {lib_path}: {exc}") from exc
+        for name in EXPORTED_SYMBOLS:
+            if not hasattr(lib, name):
+                raise CudaBackendUnavailable(f"{lib_path} does not export {name}")
+        lib.fdtd_abi_version.restype = ctypes.c_int
+        lib.fdtd_program_size.restype = ctypes.c_int64
+        lib.fdtd_validate.argtypes = [ctypes.POINTER(FdtdProgram)]
+        lib.fdtd_validate.restype = ctypes.c_int
+        lib.fdtd_launch_phase.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32]
+        lib.fdtd_launch_phase.restype = ctypes.c_int
+        lib.fdtd_launch_program.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram)]
+        lib.fdtd_launch_program.restype = ctypes.c_int
+        lib.fdtd_apply_sources.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32,
+                                           ctypes.c_int32]
+        lib.fdtd_apply_sources.restype = ctypes.c_int
+        lib.fdtd_accumulate_dft.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32]
+        lib.fdtd_accumulate_dft.restype = ctypes.c_int
+        lib.fdtd_clear_graph_cache.restype = None
+        lib.fdtd_error_string.argtypes = [ctypes.c_int]
+        lib.fdtd_error_string.restype = ctypes.c_char_p
+        version = lib.fdtd_abi_version()
+        if version != FDTD_ABI_VERSION:
+            raise CudaBackendUnavailable(f"ABI mismatch: library {version}, bindings {FDTD_ABI_VERSION}")
+        size = lib.fdtd_program_size()
+        if size != ctypes.sizeof(FdtdProgram):
+            raise CudaBackendUnavailable(
+                f"FdtdProgram layout mismatch: library {size} bytes, bindings {ctypes.sizeof(FdtdProgram)}"
+            )
+        if path is None:
+            _LIB = lib
+        return lib
+
+
+def check(code: int, where: str) -> None:
+    if code != 0:
+        lib = load_library()
+        name = lib.fdtd_error_string(int(code))
+        raise FdtdError(int(code), name.decode() if name else "unknown", where)

@@ -1,0 +1,137 @@
+// Slab sources, DFT monitors and the device step counter.
+
+#include "kernels.cuh"
+
+namespace fdtd {
+
+namespace {
+
+// field[start + idx] += coeff[idx] * waveform[clamp(step)]
+// (beamz/simulation/execute.py:374-433; cuda/src/io.cu:65-168).  H/E-timing
+// additions on PEC-constrained cells are skipped: the step zeroes those cells
+// after the update, and beamz re-applies its masks after the injection
+// (execute.py:506-522), so the two orders agree.
+__global__ void source_kernel(SourceDev s, float* target, Dims td, int timing, int metallic, const int* counter,
+                              int step_offset) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= s.ex || y >= s.ey || z >= s.ez) return;
+  const int k = s.z0 + z, j = s.y0 + y, i = s.x0 + x;
+  if (k < 0 || j < 0 || i < 0 || k >= td.z || j >= td.y || i >= td.x) return;
+  if (timing == FDTD_TIMING_H && h_constrained(metallic, s.component, td, k, j, i)) return;
+  if (timing == FDTD_TIMING_E && e_constrained(metallic, s.component, td, k, j, i)) return;
+  const float amp = source_amplitude(s, counter[0] + step_offset);
+  const int64_t co = (static_cast<int64_t>(z) * s.ey + y) * s.ex + x;
+  const int64_t to = lin(td, k, j, i);
+  target[to] = target[to] + s.coeff[co] * amp;
+}
+
+// One block per (monitor, component, point tile).  The per-frequency phase and
+// window are evaluated once per block into shared memory.
+// beamz/simulation/observe.py:327-357 (gate, window, scale) and 529-585.
+constexpr int kDftThreads = 256;
+constexpr int kDftMaxFreqs = 64;
+
+__global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* counter, int step_offset) {
+  const int mc = blockIdx.y;
+  const int m = mc / 6;
+  const int c = mc % 6;
+  const int* cnt = d.counts + 5 * m;
+  // Counts live on the device; clamp them to the arena extents so that a
+  // malformed plan can never address outside the buffers it names.
+  const int nf = min(max(cnt[0], 0), d.max_freqs);
+  const int np = min(max(cnt[1], 0), d.max_points);
+  const int interval = cnt[2] > 0 ? cnt[2] : 1;
+  const int voff = cnt[3], woff = cnt[4];
+  const int step = counter[0] + step_offset;
+  if (step % interval != 0) return;
+  int ti = step < 0 ? 0 : step;
+  ti = ti >= d.step_time_len ? d.step_time_len - 1 : ti;
+  const float t = d.step_time[ti];
+  const float t0 = d.windows[3 * m], t1 = d.windows[3 * m + 1], unit = d.windows[3 * m + 2];
+  if (!(t >= t0 && t <= t1)) return;
+
+  __shared__ float s_cos[kDftMaxFreqs];
+  __shared__ float s_sin[kDftMaxFreqs];
+  __shared__ float s_scale;
+  __shared__ float s_window;
+  if (threadIdx.x == 0) {
+    float window = 1.0f;
+    if (d.codes[2 * m] == 1 && isfinite(t1) && t1 > t0) {
+      const float span = fmaxf(t1 - t0, 1e-30f);
+      const float tau = fminf(fmaxf((t - t0) / span, 0.0f), 1.0f);
+      window = 0.5f * (1.0f - cosf(6.2831855f * tau));
+    }
+    float scale = fmaxf(window, 0.0f);
+    if (d.codes[2 * m + 1] == 1) {
+      // ((dt * interval) * c / L) / sqrt(2 pi), each step in float32 (observe.py:352-356).
+      const float phys = ((d.dt * static_cast<float>(interval)) * 299792458.0f) / unit;
+      scale = scale * (phys / sqrtf(6.2831855f));
+    }
+    s_scale = scale;
+    s_window = window;
+  }
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+    // theta = (fl32(2 pi) * f) * t, all float32 (observe.py:533-538).
+    const float theta = (6.2831855f * d.freqs[m * d.max_freqs + f]) * t;
+    float sn, cs;
+    sincosf(theta, &sn, &cs);
+    s_cos[f] = cs;
+    s_sin[f] = sn;
+  }
+  __syncthreads();
+  if (c == 0 && blockIdx.x == 0) {
+    for (int f = threadIdx.x; f < nf; f += blockDim.x)
+      if (woff >= 0 && woff + f < d.weight_len) d.weight_sum[woff + f] += s_window;
+  }
+  const float mask = d.masks[m * 6 + c];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || mask == 0.0f) return;
+  if (voff < 0 || voff + static_cast<int64_t>(6) * nf * np > d.arena_len) return;
+  const int K = d.neighbors;
+  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * d.max_points + p) * K;
+  const float* field = d.fields[c];
+  float v = 0.0f;
+  for (int n = 0; n < K; ++n) {
+    const float w = d.weights[base + n];
+    const int idx = d.indices[base + n];
+    if (w != 0.0f && idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
+  }
+  const float sm = s_scale * mask;
+  const int64_t out = voff + (static_cast<int64_t>(c) * nf) * np + p;
+  for (int f = 0; f < nf; ++f) {
+    d.re[out + static_cast<int64_t>(f) * np] += sm * (s_cos[f] * v);
+    d.im[out + static_cast<int64_t>(f) * np] += sm * (s_sin[f] * v);
+  }
+}
+
+__global__ void counter_kernel(int* counter, int nsteps) { counter[0] += nsteps; }
+
+}  // namespace
+
+cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int timing, int metallic,
+                          const int* counter, int step_offset) {
+  if (src.ex <= 0 || src.ey <= 0 || src.ez <= 0) return cudaSuccess;
+  const int bx = src.ex >= 32 ? 32 : (src.ex >= 8 ? 8 : 1);
+  const int by = 256 / bx > 32 ? 32 : 256 / bx;
+  const dim3 block(bx, by, 1);
+  const dim3 grid((src.ex + bx - 1) / bx, (src.ey + by - 1) / by, src.ez);
+  source_kernel<<<grid, block, 0, s>>>(src, target, td, timing, metallic, counter, step_offset);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, int step_offset) {
+  if (dft.monitor_count <= 0 || dft.max_points <= 0) return cudaSuccess;
+  if (dft.max_freqs > kDftMaxFreqs) return cudaErrorInvalidValue;
+  const dim3 grid((dft.max_points + kDftThreads - 1) / kDftThreads, dft.monitor_count * 6, 1);
+  dft_kernel<<<grid, kDftThreads, 0, s>>>(dft, counter, step_offset);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_counter_advance(cudaStream_t s, int* counter, int nsteps) {
+  counter_kernel<<<1, 1, 0, s>>>(counter, nsteps);
+  return cudaPeekAtLastError();
+}
+
+}  // namespace fdtd

@@ -1,0 +1,121 @@
+// Device helpers shared by the phase and fused step kernels, and the host
+// launcher declarations.
+#pragma once
+
+#include "params.cuh"
+
+namespace fdtd {
+
+// Active-component masks (bit c = component c, order Ex Ey Ez Hx Hy Hz).
+constexpr int kActive3D = 0x3F;
+constexpr int kActiveTM = (1 << 2) | (1 << 3) | (1 << 4);  // Ez Hx Hy
+constexpr int kActiveTE = (1 << 0) | (1 << 1) | (1 << 5);  // Ex Ey Hz
+
+// H <- decay * H - source * curl (beamz: cuda/src/update.cu:402-409; with
+// decay == 1 and source == fl(dt)/fl(mu0) this is kernels.py:497-500 exactly).
+__device__ __forceinline__ float h_update(const HMaterial& m, int c, int64_t o, float h, float curl) {
+  const float dec = m.decay[c][m.decay_full[c] ? o : 0];
+  const float src = m.source[c][m.source_full[c] ? o : 0];
+  return dec * h - src * curl;
+}
+
+__device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+
+__device__ __forceinline__ float vox_eps(const EMaterial& m, int Z, int Y, int X, int k, int j, int i) {
+  k = clampi(k, Z - 1);
+  j = clampi(j, Y - 1);
+  i = clampi(i, X - 1);
+  return m.eps_table[m.voxels[(static_cast<int64_t>(k) * Y + j) * X + i]];
+}
+
+// Centered E-site permittivity from the voxel grid, in the averaging order of
+// beamz/lattice.py:732-786 (axes z, y, x; 0.5 * (lo + hi) on face-aligned axes).
+__device__ __forceinline__ float site_eps(const Step3D& p, int c, int k, int j, int i) {
+  const EMaterial& m = p.em;
+  const int Z = p.Z, Y = p.Y, X = p.X;
+  if (c == 0) {  // Ex: average z, then y; x owned.
+    const float a = 0.5f * (vox_eps(m, Z, Y, X, k - 1, j - 1, i) + vox_eps(m, Z, Y, X, k, j - 1, i));
+    const float b = 0.5f * (vox_eps(m, Z, Y, X, k - 1, j, i) + vox_eps(m, Z, Y, X, k, j, i));
+    return 0.5f * (a + b);
+  }
+  if (c == 1) {  // Ey: average z, then x; y owned.
+    const float a = 0.5f * (vox_eps(m, Z, Y, X, k - 1, j, i - 1) + vox_eps(m, Z, Y, X, k, j, i - 1));
+    const float b = 0.5f * (vox_eps(m, Z, Y, X, k - 1, j, i) + vox_eps(m, Z, Y, X, k, j, i));
+    return 0.5f * (a + b);
+  }
+  // Ez: average y, then x; z owned.
+  const float a = 0.5f * (vox_eps(m, Z, Y, X, k, j - 1, i - 1) + vox_eps(m, Z, Y, X, k, j, i - 1));
+  const float b = 0.5f * (vox_eps(m, Z, Y, X, k, j - 1, i) + vox_eps(m, Z, Y, X, k, j, i));
+  return 0.5f * (a + b);
+}
+
+// E <- E + (dt/eps0 * 1/eps) * curl for voxel materials (kernels.py:612-623 with
+// zero conductivity), or decay * E + source * curl for per-site coefficients.
+template <int Mat>
+__device__ __forceinline__ float e_update(const Step3D& p, int c, int64_t o, int k, int j, int i, float e,
+                                          float curl) {
+  if (Mat == FDTD_MATERIAL_VOXEL) {
+    const float inv = __frcp_rn(site_eps(p, c, k, j, i));
+    return e + (p.dt_over_eps * inv) * curl;
+  } else {
+    const float dec = p.em.decay[c][p.em.decay_full[c] ? o : 0];
+    const float src = p.em.source[c][p.em.source_full[c] ? o : 0];
+    return dec * e + src * curl;
+  }
+}
+
+// PEC: an E component is constrained on a metallic wall normal to either of
+// its two transverse axes (beamz/devices/_boundary_compile.py:129-136).
+__device__ __forceinline__ bool e_constrained(int metallic, int c, const Dims& d, int k, int j, int i) {
+  const int normal = 2 - c;
+  const int coord[3] = {k, j, i};
+  const int n[3] = {d.z, d.y, d.x};
+  for (int a = 0; a < 3; ++a) {
+    if (a == normal) continue;
+    if ((coord[a] == 0 && wall(metallic, a, false)) || (coord[a] == n[a] - 1 && wall(metallic, a, true)))
+      return true;
+  }
+  return false;
+}
+
+// H components are constrained only on walls normal to themselves.
+__device__ __forceinline__ bool h_constrained(int metallic, int c, const Dims& d, int k, int j, int i) {
+  const int normal = 2 - (c - 3);
+  const int coord = normal == 0 ? k : (normal == 1 ? j : i);
+  const int n = normal == 0 ? d.z : (normal == 1 ? d.y : d.x);
+  return (coord == 0 && wall(metallic, normal, false)) || (coord == n - 1 && wall(metallic, normal, true));
+}
+
+// ---- host launchers -------------------------------------------------------
+cudaError_t launch_phase(cudaStream_t s, const Step3D& p, int phase, int mat, int active_mask);
+cudaError_t launch_fused(cudaStream_t s, const Step3D& p, int mat, int active_mask, int tile_x, int tile_y);
+cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int timing,
+                          int metallic, const int* counter, int step_offset);
+struct DftDev;
+cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, int step_offset);
+cudaError_t launch_counter_advance(cudaStream_t s, int* counter, int nsteps);
+
+// DFT arena view (see FdtdDft in fdtd_b200.h).
+struct DftDev {
+  int monitor_count;
+  int max_points, neighbors, max_freqs;
+  const int* indices;
+  const float* weights;
+  const float* freqs;
+  const float* masks;
+  const int* counts;
+  const int* codes;
+  const float* windows;
+  float* re;
+  float* im;
+  float* weight_sum;
+  int64_t arena_len;   // elements of re / im
+  int64_t weight_len;  // elements of weight_sum
+  const float* fields[6];
+  int64_t field_len[6];
+  const float* step_time;
+  int step_time_len;
+  float dt;
+};
+
+}  // namespace fdtd

@@ -1,0 +1,65 @@
+// Kernel parameter blocks built from an FdtdProgram by the host code.
+#pragma once
+
+#include "fdtd_common.cuh"
+
+namespace fdtd {
+
+// Electric material for the E update.
+struct EMaterial {
+  // FDTD_MATERIAL_SITE: per-site (stride 1) or uniform (stride 0) decay/source.
+  const float* decay[3];
+  const float* source[3];
+  int decay_full[3];
+  int source_full[3];
+  // FDTD_MATERIAL_VOXEL: voxel ids [Z, Y, X] and permittivity table [256].
+  const uint8_t* voxels;
+  const float* eps_table;
+};
+
+// Magnetic update coefficients (uniform or per-site).
+struct HMaterial {
+  const float* decay[3];
+  const float* source[3];
+  int decay_full[3];
+  int source_full[3];
+};
+
+// Everything a 3D step/phase kernel reads.
+struct Step3D {
+  int Z, Y, X;
+  const float* ein[3];
+  const float* hin[3];
+  float* eout[3];
+  float* hout[3];
+  float res, inv_res;
+  float dt_over_eps;
+  int metallic;
+  int cpml;
+  EMaterial em;
+  HMaterial hm;
+  CpmlTermDev ht[6];
+  CpmlTermDev et[6];
+  // h-timing sources fused into the step kernel (FDTD_SCHEDULE_FUSED).
+  int n_hsrc;
+  SourceDev hsrc[kMaxFusedSources];
+  const int* step_counter;
+  int step_offset;
+  int z_chunk;
+};
+
+// 2D (canonical xy plane) step/phase parameters; z extent is 1.
+struct Step2D {
+  int Y, X, pol;
+  const float* fin[6];
+  float* fout[6];
+  float res, inv_res;
+  int metallic;
+  int cpml;
+  EMaterial em;
+  HMaterial hm;
+  CpmlTermDev ht[2];
+  CpmlTermDev et[2];
+};
+
+}  // namespace fdtd

@@ -1,0 +1,488 @@
+// C ABI: validation, parameter packing, step schedules and the CUDA-graph cache.
+//
+// beamz counterparts: program validation and schedules in cuda/src/program.cu
+// (110-354), phase validation in cuda/src/update.cu (47-146) and the graph
+// cache in cuda/src/graph.cu (11-154).
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "kernels.cuh"
+
+namespace fdtd {
+namespace {
+
+constexpr int kInvalid = static_cast<int>(cudaErrorInvalidValue);
+
+int64_t elements(const FdtdBuffer& b) {
+  if (b.rank < 0 || b.rank > 4) return -1;
+  int64_t n = 1;
+  for (int a = 0; a < b.rank; ++a) {
+    if (b.dims[a] < 0) return -1;
+    n *= b.dims[a];
+  }
+  return n;
+}
+
+bool is_f32(const FdtdBuffer& b) { return b.element_type == FDTD_F32; }
+
+struct Layout {
+  int Z, Y, X;  // internal 3D cell extents (2D TM: Z = 1, 2D TE: Z = 0)
+  int active;
+};
+
+bool layout_of(const FdtdProgram& p, Layout* out) {
+  if (p.ndim == 3) {
+    if (p.cells[0] < 1 || p.cells[1] < 1 || p.cells[2] < 1) return false;
+    *out = {static_cast<int>(p.cells[0]), static_cast<int>(p.cells[1]), static_cast<int>(p.cells[2]), kActive3D};
+  } else if (p.ndim == 2) {
+    if (p.cells[1] < 1 || p.cells[2] < 1) return false;
+    if (p.polarization == 0) {
+      *out = {1, static_cast<int>(p.cells[1]), static_cast<int>(p.cells[2]), kActiveTM};
+    } else if (p.polarization == 1) {
+      *out = {0, static_cast<int>(p.cells[1]), static_cast<int>(p.cells[2]), kActiveTE};
+    } else {
+      return false;
+    }
+  } else {
+    return false;
+  }
+  // Element offsets are 64-bit; per-plane coordinates stay 32-bit.
+  const int64_t lim = (int64_t{1} << 30);
+  return out->Y < lim && out->X < lim && out->Z < lim;
+}
+
+int64_t dims_count(const Dims& d) { return static_cast<int64_t>(d.z) * d.y * d.x; }
+
+// 2D programs name CPML axes in (y, x) storage terms and use two terms per
+// phase; they land in the 3D term slots that carry the same derivative.
+int term_slot(int ndim, int pol, bool h, int t) {
+  if (ndim == 3) return t;
+  if (pol == 0) return h ? (t == 0 ? 0 : 3) : (t == 0 ? 4 : 5);
+  return h ? (t == 0 ? 4 : 5) : (t == 0 ? 0 : 3);
+}
+
+// Target component and derivative axis of each 3D term slot.
+constexpr int kHTermComp[6] = {3, 3, 4, 4, 5, 5};
+constexpr int kHTermAxis[6] = {1, 0, 0, 2, 2, 1};
+constexpr int kETermComp[6] = {0, 0, 1, 1, 2, 2};
+constexpr int kETermAxis[6] = {1, 0, 0, 2, 2, 1};
+
+bool check_coeff(const FdtdBuffer& b, int64_t full) {
+  if (!is_f32(b) || b.data == nullptr) return false;
+  const int64_t n = elements(b);
+  return n == 1 || n == full;
+}
+
+int validate(const FdtdProgram& p) {
+  if (p.abi_version != FDTD_ABI_VERSION) return kInvalid;
+  Layout L;
+  if (!layout_of(p, &L)) return kInvalid;
+  if (p.schedule != FDTD_SCHEDULE_PHASES && p.schedule != FDTD_SCHEDULE_FUSED) return kInvalid;
+  if (p.material_kind != FDTD_MATERIAL_SITE && p.material_kind != FDTD_MATERIAL_VOXEL) return kInvalid;
+  if (p.material_kind == FDTD_MATERIAL_VOXEL && p.ndim != 3) return kInvalid;
+  if (p.nsteps < 0 || p.source_count < 0 || p.source_count > FDTD_MAX_SOURCES) return kInvalid;
+  if (!(p.resolution > 0.0f) || !(p.inv_resolution > 0.0f)) return kInvalid;
+  if (p.metallic_edges & ~0x3F) return kInvalid;
+  for (int c = 0; c < 6; ++c) {
+    if (!((L.active >> c) & 1)) continue;
+    const int64_t n = dims_count(component_dims(c, L.Z, L.Y, L.X));
+    if (!is_f32(p.fields[c]) || elements(p.fields[c]) != n || (n > 0 && p.fields[c].data == nullptr)) return kInvalid;
+    if (p.schedule == FDTD_SCHEDULE_FUSED &&
+        (!is_f32(p.fields_alt[c]) || elements(p.fields_alt[c]) != n || (n > 0 && p.fields_alt[c].data == nullptr)))
+      return kInvalid;
+    if (c < 3) {
+      if (p.material_kind == FDTD_MATERIAL_SITE &&
+          (!check_coeff(p.e_decay[c], n) || !check_coeff(p.e_source[c], n)))
+        return kInvalid;
+    } else {
+      if (!check_coeff(p.h_decay[c - 3], n) || !check_coeff(p.h_source_site[c - 3], n)) return kInvalid;
+    }
+  }
+  if (p.material_kind == FDTD_MATERIAL_VOXEL) {
+    if (p.voxels.element_type != FDTD_U8 || elements(p.voxels) != static_cast<int64_t>(L.Z) * L.Y * L.X ||
+        p.voxels.data == nullptr)
+      return kInvalid;
+    if (!is_f32(p.eps_table) || elements(p.eps_table) != 256 || p.eps_table.data == nullptr) return kInvalid;
+  }
+  if (p.cpml) {
+    const int nterms = p.ndim == 3 ? 6 : 2;
+    for (int h = 0; h < 2; ++h) {
+      for (int t = 0; t < nterms; ++t) {
+        const FdtdCpmlTerm& term = h ? p.h_terms[t] : p.e_terms[t];
+        const int slot = term_slot(p.ndim, p.polarization, h, t);
+        const int comp = h ? kHTermComp[slot] : kETermComp[slot];
+        const int axis = h ? kHTermAxis[slot] : kETermAxis[slot];
+        const int given_axis = p.ndim == 3 ? term.axis : term.axis + 1;
+        if (given_axis != axis) return kInvalid;
+        const Dims d = component_dims(comp, L.Z, L.Y, L.X);
+        const int n_axis = axis == 0 ? d.z : (axis == 1 ? d.y : d.x);
+        if (term.low < 0 || term.high < 0 || term.low + term.high > n_axis) return kInvalid;
+        const int w = term.low + term.high;
+        if (w == 0) continue;
+        for (const FdtdBuffer* b : {&term.a, &term.b, &term.inv_kappa}) {
+          if (!is_f32(*b) || elements(*b) < w || b->data == nullptr) return kInvalid;
+        }
+        Dims pd = d;
+        if (axis == 0) pd.z = w;
+        if (axis == 1) pd.y = w;
+        if (axis == 2) pd.x = w;
+        if (!is_f32(term.psi) || elements(term.psi) != dims_count(pd) || term.psi.data == nullptr) return kInvalid;
+        if (h && p.schedule == FDTD_SCHEDULE_FUSED &&
+            (!is_f32(term.psi_alt) || elements(term.psi_alt) != dims_count(pd) || term.psi_alt.data == nullptr))
+          return kInvalid;
+      }
+    }
+  }
+  for (int s = 0; s < p.source_count; ++s) {
+    const FdtdSource& src = p.sources[s];
+    if (src.component < 0 || src.component > 5 || !((L.active >> src.component) & 1)) return kInvalid;
+    if (src.timing < FDTD_TIMING_PRE_E || src.timing > FDTD_TIMING_E) return kInvalid;
+    const bool is_h = src.component >= 3;
+    if ((src.timing == FDTD_TIMING_H) != is_h) return kInvalid;
+    if (!is_f32(src.coeff) || src.coeff.data == nullptr || src.coeff.rank < 1 || src.coeff.rank > 3) return kInvalid;
+    if (!is_f32(src.waveform) || src.waveform.data == nullptr || elements(src.waveform) < 1) return kInvalid;
+    const Dims d = component_dims(src.component, L.Z, L.Y, L.X);
+    int64_t ext[3] = {1, 1, 1};
+    for (int a = 0; a < src.coeff.rank; ++a) ext[3 - src.coeff.rank + a] = src.coeff.dims[a];
+    const int64_t lo[3] = {src.start[0], src.start[1], src.start[2]};
+    const int64_t hi[3] = {d.z, d.y, d.x};
+    for (int a = 0; a < 3; ++a) {
+      if (ext[a] < 1 || lo[a] < 0 || lo[a] + ext[a] > hi[a]) return kInvalid;
+    }
+  }
+  if (p.step_counter.element_type != FDTD_S32 || elements(p.step_counter) < 1 || p.step_counter.data == nullptr)
+    return kInvalid;
+  if (p.dft.monitor_count < 0 || p.dft.monitor_count > FDTD_MAX_MONITORS) return kInvalid;
+  if (p.dft.monitor_count > 0) {
+    const FdtdDft& d = p.dft;
+    const int M = d.monitor_count;
+    if (d.indices.element_type != FDTD_S32 || d.indices.rank != 4 || d.indices.dims[0] != M || d.indices.dims[1] != 6)
+      return kInvalid;
+    if (!is_f32(d.weights) || d.weights.rank != 4) return kInvalid;
+    for (int a = 0; a < 4; ++a)
+      if (d.weights.dims[a] != d.indices.dims[a]) return kInvalid;
+    if (!is_f32(d.freqs) || d.freqs.rank != 2 || d.freqs.dims[0] != M || d.freqs.dims[1] > 64) return kInvalid;
+    if (!is_f32(d.masks) || elements(d.masks) != 6 * M) return kInvalid;
+    if (d.counts.element_type != FDTD_S32 || elements(d.counts) != 5 * M) return kInvalid;
+    if (d.codes.element_type != FDTD_S32 || elements(d.codes) != 2 * M) return kInvalid;
+    if (!is_f32(d.windows) || elements(d.windows) != 3 * M) return kInvalid;
+    if (!is_f32(d.re) || !is_f32(d.im) || elements(d.re) != elements(d.im) || !is_f32(d.weight_sum)) return kInvalid;
+    if (!is_f32(p.step_time) || elements(p.step_time) < 1 || p.step_time.data == nullptr) return kInvalid;
+    for (const FdtdBuffer* b : {&d.indices, &d.weights, &d.freqs, &d.masks, &d.counts, &d.codes, &d.windows, &d.re,
+                                &d.im, &d.weight_sum})
+      if (b->data == nullptr && elements(*b) > 0) return kInvalid;
+  }
+  return 0;
+}
+
+CpmlTermDev term_dev(const FdtdCpmlTerm& t, const Dims& target, int axis, bool alt_in, bool alt_out) {
+  CpmlTermDev d{};
+  d.low = t.low;
+  d.high = t.high;
+  // An empty term keeps its true axis extent so that no coordinate maps into it.
+  d.n_axis = axis == 0 ? target.z : (axis == 1 ? target.y : target.x);
+  if (t.low + t.high == 0) return d;
+  d.a = static_cast<const float*>(t.a.data);
+  d.b = static_cast<const float*>(t.b.data);
+  d.k = static_cast<const float*>(t.inv_kappa.data);
+  d.psi_in = static_cast<const float*>(alt_in ? t.psi_alt.data : t.psi.data);
+  d.psi_out = static_cast<float*>(alt_out ? t.psi_alt.data : t.psi.data);
+  const int w = t.low + t.high;
+  d.pdy = axis == 1 ? w : target.y;
+  d.pdx = axis == 2 ? w : target.x;
+  return d;
+}
+
+// Kernel parameters for one step.  `bank` selects which field bank is the input
+// (0 = fields, 1 = fields_alt); for the one-bank schedule input == output.
+Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, int step_offset) {
+  Step3D s{};
+  s.Z = L.Z;
+  s.Y = L.Y;
+  s.X = L.X;
+  const FdtdBuffer* in = bank == 0 ? p.fields : p.fields_alt;
+  const FdtdBuffer* out = fused ? (bank == 0 ? p.fields_alt : p.fields) : in;
+  for (int c = 0; c < 3; ++c) {
+    s.ein[c] = static_cast<const float*>(in[c].data);
+    s.eout[c] = static_cast<float*>(out[c].data);
+    s.hin[c] = static_cast<const float*>(in[c + 3].data);
+    s.hout[c] = static_cast<float*>(out[c + 3].data);
+  }
+  s.res = p.resolution;
+  s.inv_res = p.inv_resolution;
+  s.dt_over_eps = p.dt_over_eps;
+  s.metallic = p.metallic_edges;
+  if (p.ndim == 2) s.metallic &= ~(FDTD_EDGE_FRONT | FDTD_EDGE_BACK);
+  s.cpml = p.cpml;
+  for (int c = 0; c < 3; ++c) {
+    const bool ea = (L.active >> c) & 1, ha = (L.active >> (c + 3)) & 1;
+    if (ea && p.material_kind == FDTD_MATERIAL_SITE) {
+      s.em.decay[c] = static_cast<const float*>(p.e_decay[c].data);
+      s.em.source[c] = static_cast<const float*>(p.e_source[c].data);
+      s.em.decay_full[c] = elements(p.e_decay[c]) > 1;
+      s.em.source_full[c] = elements(p.e_source[c]) > 1;
+    }
+    if (ha) {
+      s.hm.decay[c] = static_cast<const float*>(p.h_decay[c].data);
+      s.hm.source[c] = static_cast<const float*>(p.h_source_site[c].data);
+      s.hm.decay_full[c] = elements(p.h_decay[c]) > 1;
+      s.hm.source_full[c] = elements(p.h_source_site[c]) > 1;
+    }
+  }
+  if (p.material_kind == FDTD_MATERIAL_VOXEL) {
+    s.em.voxels = static_cast<const uint8_t*>(p.voxels.data);
+    s.em.eps_table = static_cast<const float*>(p.eps_table.data);
+  }
+  if (p.cpml) {
+    const int nterms = p.ndim == 3 ? 6 : 2;
+    for (int t = 0; t < nterms; ++t) {
+      const int hs = term_slot(p.ndim, p.polarization, true, t);
+      const int es = term_slot(p.ndim, p.polarization, false, t);
+      const Dims hd = component_dims(kHTermComp[hs], L.Z, L.Y, L.X);
+      const Dims ed = component_dims(kETermComp[es], L.Z, L.Y, L.X);
+      // H memories are double-banked under the fused schedule.
+      s.ht[hs] = term_dev(p.h_terms[t], hd, kHTermAxis[hs], fused && bank == 1, fused && bank == 0);
+      s.et[es] = term_dev(p.e_terms[t], ed, kETermAxis[es], false, false);
+    }
+  }
+  s.step_counter = static_cast<const int*>(p.step_counter.data);
+  s.step_offset = step_offset;
+  s.z_chunk = p.z_chunk;
+  return s;
+}
+
+SourceDev source_dev(const FdtdSource& src) {
+  SourceDev d{};
+  d.coeff = static_cast<const float*>(src.coeff.data);
+  d.waveform = static_cast<const float*>(src.waveform.data);
+  d.wave_len = static_cast<int>(elements(src.waveform));
+  d.component = src.component;
+  d.z0 = src.start[0];
+  d.y0 = src.start[1];
+  d.x0 = src.start[2];
+  int64_t ext[3] = {1, 1, 1};
+  for (int a = 0; a < src.coeff.rank; ++a) ext[3 - src.coeff.rank + a] = src.coeff.dims[a];
+  d.ez = static_cast<int>(ext[0]);
+  d.ey = static_cast<int>(ext[1]);
+  d.ex = static_cast<int>(ext[2]);
+  return d;
+}
+
+cudaError_t enqueue_sources(cudaStream_t s, const FdtdProgram& p, const Layout& L, const FdtdBuffer* bank_fields,
+                            int timing, int step_offset) {
+  const int metallic = p.ndim == 2 ? (p.metallic_edges & ~(FDTD_EDGE_FRONT | FDTD_EDGE_BACK)) : p.metallic_edges;
+  for (int i = 0; i < p.source_count; ++i) {
+    const FdtdSource& src = p.sources[i];
+    if (src.timing != timing) continue;
+    const Dims td = component_dims(src.component, L.Z, L.Y, L.X);
+    cudaError_t err = launch_source(s, source_dev(src), static_cast<float*>(bank_fields[src.component].data), td,
+                                    timing, metallic, static_cast<const int*>(p.step_counter.data), step_offset);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+DftDev make_dft(const FdtdProgram& p, const FdtdBuffer* bank_fields) {
+  DftDev d{};
+  const FdtdDft& m = p.dft;
+  d.monitor_count = m.monitor_count;
+  if (m.monitor_count == 0) return d;
+  d.max_points = static_cast<int>(m.indices.dims[2]);
+  d.neighbors = static_cast<int>(m.indices.dims[3]);
+  d.max_freqs = static_cast<int>(m.freqs.dims[1]);
+  d.indices = static_cast<const int*>(m.indices.data);
+  d.weights = static_cast<const float*>(m.weights.data);
+  d.freqs = static_cast<const float*>(m.freqs.data);
+  d.masks = static_cast<const float*>(m.masks.data);
+  d.counts = static_cast<const int*>(m.counts.data);
+  d.codes = static_cast<const int*>(m.codes.data);
+  d.windows = static_cast<const float*>(m.windows.data);
+  d.re = static_cast<float*>(m.re.data);
+  d.im = static_cast<float*>(m.im.data);
+  d.weight_sum = static_cast<float*>(m.weight_sum.data);
+  d.arena_len = elements(m.re);
+  d.weight_len = elements(m.weight_sum);
+  for (int c = 0; c < 6; ++c) {
+    d.fields[c] = static_cast<const float*>(bank_fields[c].data);
+    d.field_len[c] = elements(bank_fields[c]);
+  }
+  d.step_time = static_cast<const float*>(p.step_time.data);
+  d.step_time_len = static_cast<int>(elements(p.step_time));
+  d.dt = p.dt;
+  return d;
+}
+
+// Enqueue `nsteps` steps.  Under the fused schedule step s reads bank (s & 1).
+cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
+  Layout L;
+  layout_of(p, &L);
+  const bool fused = p.schedule == FDTD_SCHEDULE_FUSED;
+  const int* counter = static_cast<const int*>(p.step_counter.data);
+  // Sources of H timing ride inside the fused kernel.
+  int n_hsrc = 0;
+  SourceDev hsrc[kMaxFusedSources];
+  for (int i = 0; i < p.source_count; ++i)
+    if (p.sources[i].timing == FDTD_TIMING_H) hsrc[n_hsrc++] = source_dev(p.sources[i]);
+  for (int step = 0; step < p.nsteps; ++step) {
+    const int bank = fused ? (step & 1) : 0;
+    const FdtdBuffer* a = bank == 0 ? p.fields : p.fields_alt;
+    const FdtdBuffer* b = fused ? (bank == 0 ? p.fields_alt : p.fields) : a;
+    cudaError_t err = enqueue_sources(s, p, L, a, FDTD_TIMING_PRE_E, step);
+    if (err != cudaSuccess) return err;
+    Step3D sp = make_step(p, L, bank, fused, step);
+    if (fused) {
+      sp.n_hsrc = n_hsrc;
+      for (int i = 0; i < n_hsrc; ++i) sp.hsrc[i] = hsrc[i];
+      err = launch_fused(s, sp, p.material_kind, L.active, p.tile_x, p.tile_y);
+      if (err != cudaSuccess) return err;
+    } else {
+      err = launch_phase(s, sp, 0, p.material_kind, L.active);
+      if (err != cudaSuccess) return err;
+      err = enqueue_sources(s, p, L, a, FDTD_TIMING_H, step);
+      if (err != cudaSuccess) return err;
+      err = launch_phase(s, sp, 1, p.material_kind, L.active);
+      if (err != cudaSuccess) return err;
+    }
+    err = enqueue_sources(s, p, L, b, FDTD_TIMING_E, step);
+    if (err != cudaSuccess) return err;
+    if (p.dft.monitor_count > 0) {
+      err = launch_dft(s, make_dft(p, b), counter, step);
+      if (err != cudaSuccess) return err;
+    }
+  }
+  if (p.nsteps > 0) return launch_counter_advance(s, static_cast<int*>(p.step_counter.data), p.nsteps);
+  return cudaSuccess;
+}
+
+// ---- graph cache (beamz: cuda/src/graph.cu:84-154) -------------------------
+struct GraphCache {
+  std::mutex mu;
+  std::unordered_map<std::string, cudaGraphExec_t> graphs;
+};
+
+GraphCache& cache() {
+  static GraphCache* c = new GraphCache();
+  return *c;
+}
+
+constexpr size_t kMaxGraphs = 32;
+
+std::string graph_key(const FdtdProgram& p, cudaStream_t s) {
+  int device = 0;
+  cudaGetDevice(&device);
+  std::string key(reinterpret_cast<const char*>(&p), sizeof(FdtdProgram));
+  key.append(reinterpret_cast<const char*>(&s), sizeof(s));
+  key.append(reinterpret_cast<const char*>(&device), sizeof(device));
+  return key;
+}
+
+cudaError_t launch_with_graph(cudaStream_t s, const FdtdProgram& p) {
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  cudaError_t err = cudaStreamIsCapturing(s, &status);
+  if (err != cudaSuccess) return err;
+  if (status != cudaStreamCaptureStatusNone || s == nullptr) return enqueue_program(s, p);
+  const std::string key = graph_key(p, s);
+  GraphCache& gc = cache();
+  std::lock_guard<std::mutex> lock(gc.mu);
+  auto it = gc.graphs.find(key);
+  if (it == gc.graphs.end()) {
+    err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      return enqueue_program(s, p);
+    }
+    cudaError_t enq = enqueue_program(s, p);
+    cudaGraph_t graph = nullptr;
+    err = cudaStreamEndCapture(s, &graph);
+    if (enq != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return enq;
+    }
+    if (err != cudaSuccess) return err;
+    cudaGraphExec_t exec = nullptr;
+    err = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) return err;
+    if (gc.graphs.size() >= kMaxGraphs) {
+      for (auto& kv : gc.graphs) cudaGraphExecDestroy(kv.second);
+      gc.graphs.clear();
+    }
+    it = gc.graphs.emplace(key, exec).first;
+  }
+  return cudaGraphLaunch(it->second, s);
+}
+
+}  // namespace
+}  // namespace fdtd
+
+extern "C" {
+
+int fdtd_abi_version(void) { return FDTD_ABI_VERSION; }
+
+int64_t fdtd_program_size(void) { return static_cast<int64_t>(sizeof(FdtdProgram)); }
+
+int fdtd_validate(const FdtdProgram* program) {
+  if (program == nullptr) return fdtd::kInvalid;
+  return fdtd::validate(*program);
+}
+
+int fdtd_launch_phase(void* stream, const FdtdProgram* program, int32_t phase) {
+  if (program == nullptr || (phase != 0 && phase != 1)) return fdtd::kInvalid;
+  FdtdProgram p = *program;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  const fdtd::Step3D sp = fdtd::make_step(p, L, 0, false, 0);
+  return static_cast<int>(
+      fdtd::launch_phase(static_cast<cudaStream_t>(stream), sp, phase, p.material_kind, L.active));
+}
+
+int fdtd_launch_program(void* stream, const FdtdProgram* program) {
+  if (program == nullptr) return fdtd::kInvalid;
+  const int v = fdtd::validate(*program);
+  if (v != 0) return v;
+  if (program->nsteps == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (program->flags & FDTD_FLAG_GRAPH_CACHE) return static_cast<int>(fdtd::launch_with_graph(s, *program));
+  return static_cast<int>(fdtd::enqueue_program(s, *program));
+}
+
+int fdtd_apply_sources(void* stream, const FdtdProgram* program, int32_t timing, int32_t step_offset) {
+  if (program == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *program;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  if (timing < FDTD_TIMING_PRE_E || timing > FDTD_TIMING_E) return fdtd::kInvalid;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  return static_cast<int>(
+      fdtd::enqueue_sources(static_cast<cudaStream_t>(stream), p, L, p.fields, timing, step_offset));
+}
+
+int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_offset) {
+  if (program == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *program;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  if (p.dft.monitor_count == 0) return 0;
+  return static_cast<int>(fdtd::launch_dft(static_cast<cudaStream_t>(stream), fdtd::make_dft(p, p.fields),
+                                           static_cast<const int*>(p.step_counter.data), step_offset));
+}
+
+void fdtd_clear_graph_cache(void) {
+  fdtd::GraphCache& gc = fdtd::cache();
+  std::lock_guard<std::mutex> lock(gc.mu);
+  for (auto& kv : gc.graphs) cudaGraphExecDestroy(kv.second);
+  gc.graphs.clear();
+}
+
+const char* fdtd_error_string(int code) { return cudaGetErrorString(static_cast<cudaError_t>(code)); }
+
+}  // extern "C"

@@ -1,0 +1,432 @@
+"""Host-side planning: everything the step kernels consume, built on the CPU.
+
+This is setup, not the hot path.  It produces, in beamz's conventions, the
+inputs that beamz's compiler hands its native step (beamz/simulation/compile.py
+:241-305 and 540-733): packed CPML recurrence slabs, material encodings,
+slab sources with sampled waveforms, DFT gather plans and the float32 clock.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# beamz/const.py:1-5
+LIGHT_SPEED = 299792458.0
+EPS_0 = 8.8541878128e-12
+MU_0 = 1.25663706212e-6
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+COMPONENT_INDEX = {c: i for i, c in enumerate(COMPONENTS)}
+ACTIVE = {3: COMPONENTS, "tm": ("Ez", "Hx", "Hy"), "te": ("Ex", "Ey", "Hz")}
+
+# Which axes (z, y, x) carry a +1 sample on each Yee support (beamz/lattice.py:14-45).
+_FACE_AXES_3D = {
+    "Ex": (1, 1, 0), "Ey": (1, 0, 1), "Ez": (0, 1, 1),
+    "Hx": (0, 0, 1), "Hy": (0, 1, 0), "Hz": (1, 0, 0),
+}
+_SHAPE_2D = {
+    "tm": {"Ez": (1, 1), "Hx": (0, 1), "Hy": (1, 0)},
+    "te": {"Ex": (1, 0), "Ey": (0, 1), "Hz": (0, 0)},
+}
+
+
+def component_shape(component: str, grid_shape, polarization: str = "tm") -> tuple:
+    """Complete stored Yee support of one component (beamz/lattice.py:32-45, 789-813)."""
+    if len(grid_shape) == 3:
+        return tuple(int(n) + e for n, e in zip(grid_shape, _FACE_AXES_3D[component]))
+    extra = _SHAPE_2D[polarization].get(component)
+    if extra is None:
+        return (1, 1)
+    return tuple(int(n) + e for n, e in zip(grid_shape, extra))
+
+
+def active_components(ndim: int, polarization: str = "tm") -> tuple:
+    return ACTIVE[3] if ndim == 3 else ACTIVE[polarization]
+
+
+# ---------------------------------------------------------------------------
+# CPML
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class CpmlTermPlan:
+    """A packed recurrence: a, b, 1/kappa over the low and high slabs of
+    ``axis`` (beamz/simulation/model.py:306-324)."""
+
+    component: str
+    axis: int  # storage axis of the component's array (3D: 0=z 1=y 2=x; 2D: 0=y 1=x)
+    sign: float
+    low: int
+    high: int
+    a: np.ndarray
+    b: np.ndarray
+    inv_kappa: np.ndarray
+
+    @property
+    def width(self) -> int:
+        return self.low + self.high
+
+    def psi_shape(self, target_shape) -> tuple:
+        shape = list(target_shape)
+        shape[self.axis] = self.width
+        return tuple(shape)
+
+
+# (component, axis, sign) per 3D derivative term, beamz/devices/_boundary_compile.py:44-60
+# and beamz/simulation/compile.py:271-283.
+TERMS_3D_H = (("Hx", 1, 1.0), ("Hx", 0, -1.0), ("Hy", 0, 1.0), ("Hy", 2, -1.0), ("Hz", 2, 1.0), ("Hz", 1, -1.0))
+TERMS_3D_E = (("Ex", 1, 1.0), ("Ex", 0, -1.0), ("Ey", 0, 1.0), ("Ey", 2, -1.0), ("Ez", 2, 1.0), ("Ez", 1, -1.0))
+# 2D terms, beamz/simulation/compile.py:285-304.
+TERMS_2D = {
+    "tm": ((("Hx", 0, 1.0), ("Hy", 1, -1.0)), (("Ez", 1, 1.0), ("Ez", 0, -1.0))),
+    "te": ((("Hz", 1, 1.0), ("Hz", 0, -1.0)), (("Ex", 0, 1.0), ("Ey", 1, -1.0))),
+}
+_WALLS_3D = (("front", "back"), ("bottom", "top"), ("left", "right"))
+_WALLS_2D = (("bottom", "top"), ("left", "right"))
+ALL_EDGES_3D = ("left", "right", "top", "bottom", "front", "back")
+ALL_EDGES_2D = ("left", "right", "top", "bottom")
+
+
+def _graded_profile(samples, pml_cells, on_low, on_high, electric, sigma_max, alpha_max, kappa_max, order):
+    """Staggered sigma/kappa/alpha along one axis in float32
+    (beamz/devices/_boundary_compile.py:479-614, uniform grid)."""
+    f32 = np.float32
+    pml = max(int(pml_cells), 1)
+    n_cells = samples - 1 if electric else samples
+    pos = np.arange(samples, dtype=f32) + (f32(0.0) if electric else f32(0.5))
+    sigma = np.zeros(samples, f32)
+    kappa = np.ones(samples, f32)
+    alpha = np.zeros(samples, f32)
+    distances = []
+    if on_low:
+        distances.append(np.clip(f32(pml) - pos, f32(0.0), f32(pml)))
+    if on_high:
+        distances.append(np.clip(pos - f32(n_cells - pml), f32(0.0), f32(pml)))
+    for dist in distances:
+        inside = dist > 0
+        u = np.clip(dist / f32(pml), f32(0.0), f32(1.0))
+        graded = np.power(u, f32(order))
+        sigma = np.where(inside, np.maximum(sigma, f32(sigma_max) * graded), sigma)
+        kappa = np.where(inside, np.maximum(kappa, f32(1.0) + (f32(kappa_max) - f32(1.0)) * graded), kappa)
+        alpha = np.where(inside, np.maximum(alpha, f32(alpha_max) * np.power(f32(1.0) - u, f32(1.0))), alpha)
+    return sigma, kappa, alpha
+
+
+def recurrence_coefficients(sigma, kappa, alpha, dt):
+    """a, b, 1/kappa of one CPML recurrence in float32 (beamz/simulation/kernels.py:130-144)."""
+    f32 = np.float32
+    kappa = np.maximum(kappa.astype(f32), f32(1.0))
+    rate = (sigma / kappa + alpha) * (f32(dt) / f32(EPS_0))
+    b = np.exp(-rate).astype(f32)
+    den = np.maximum((sigma + kappa * alpha) * kappa, f32(1e-30))
+    a = np.nan_to_num(((b - f32(1.0)) * sigma) / den).astype(f32)
+    return a, b, (f32(1.0) / kappa).astype(f32)
+
+
+def _slab_extent(a, inv_kappa):
+    """Active run lengths from each end (beamz/simulation/kernels.py:225-235)."""
+    on = (np.abs(a) > 1e-30) | (np.abs(inv_kappa - 1.0) > 1e-7)
+    low = int(np.argmin(on)) if not on.all() else on.size
+    rest = on[low:][::-1]
+    high = int(np.argmin(rest)) if not rest.all() else rest.size
+    return low, high
+
+
+def plan_cpml(grid_shape, dt, resolution, pml_cells=12, edges=None, polarization="tm",
+              kappa_max=2.0, order=3, reflection=1e-6):
+    """Every CPML term of a uniform grid, H terms then E terms.
+
+    sigma_max = -(m+1) ln R / (2 eta d), alpha_max = 2 eps0 a_n / dt with a_n =
+    0.05 (3D) or 0.1 (2D) (beamz/devices/_boundary_compile.py:244-261,
+    beamz/devices/boundaries.py:133-141).
+    """
+    ndim = len(grid_shape)
+    edges = set(ALL_EDGES_3D if ndim == 3 else ALL_EDGES_2D) if edges is None else set(edges)
+    eta = np.sqrt(MU_0 / EPS_0)
+    thickness = max(pml_cells * float(resolution), float(resolution))
+    sigma_max = -(order + 1) * np.log(max(reflection, 1e-16)) / (2.0 * eta * thickness)
+    alpha_max = 2.0 * EPS_0 * (0.05 if ndim == 3 else 0.1) / max(float(dt), 1e-30)
+    if ndim == 3:
+        specs_h, specs_e, walls = TERMS_3D_H, TERMS_3D_E, _WALLS_3D
+    else:
+        (specs_h, specs_e), walls = TERMS_2D[polarization], _WALLS_2D
+
+    def one(component, axis, sign):
+        shape = component_shape(component, grid_shape, polarization)
+        n = shape[axis]
+        electric = component.startswith("E") if ndim == 2 else _FACE_AXES_3D[component][axis] == 1
+        lo_wall, hi_wall = walls[axis]
+        s, k, al = _graded_profile(n, pml_cells, lo_wall in edges, hi_wall in edges, electric,
+                                   sigma_max, alpha_max, kappa_max, order)
+        a, b, ik = recurrence_coefficients(s, k, al, dt)
+        low, high = _slab_extent(a, ik)
+        keep = np.concatenate([np.arange(low), np.arange(n - high, n)]).astype(np.int64)
+        return CpmlTermPlan(component, axis, sign, low, high, a[keep], b[keep], ik[keep])
+
+    return [one(*s) for s in specs_h], [one(*s) for s in specs_e]
+
+
+def absorber_edge_counts(grid_shape, pml_cells, edges=None, resolution=None, explicit_thickness=False):
+    """Cells of each active wall that the absorber covers, in beamz's wall order
+    (beamz/devices/_boundary_compile.py:278-319, 404-440)."""
+    ndim = len(grid_shape)
+    order = ALL_EDGES_3D if ndim == 3 else ALL_EDGES_2D
+    chosen = order if edges is None else tuple(edges)
+    axis_of = {"left": ndim - 1, "right": ndim - 1, "bottom": ndim - 2, "top": ndim - 2, "front": 0, "back": 0}
+    out = []
+    for edge in chosen:
+        if ndim == 2 and edge in ("front", "back"):
+            continue
+        axis = axis_of[edge]
+        n = int(grid_shape[axis])
+        if explicit_thickness:
+            centers = np.linspace(0, float(n * float(resolution)), n).astype(np.float32)
+            span, depth = np.float32(n * float(resolution)), np.float32(pml_cells * float(resolution))
+        else:
+            centers = np.arange(n, dtype=np.float32) + np.float32(0.5)
+            span, depth = np.float32(n), np.float32(pml_cells)
+        if edge in ("left", "bottom", "front"):
+            covered = (depth - centers) > 0
+            side = "low"
+        else:
+            covered = (centers - (span - depth)) > 0
+            covered = covered[::-1]
+            side = "high"
+        count = int(np.argmin(covered)) if not covered.all() else 0
+        out.append((edge, axis, side, count))
+    return out
+
+
+def extend_into_absorber(grid: np.ndarray, counts) -> np.ndarray:
+    """Copy the first interior layer outward through every absorber slab
+    (beamz/devices/_boundary_compile.py:334-363)."""
+    out = np.array(grid, copy=True)
+    for _edge, axis, side, count in counts:
+        n = out.shape[axis]
+        if count <= 0 or count >= n:
+            continue
+        src = count if side == "low" else n - count - 1
+        dst = slice(0, count) if side == "low" else slice(n - count, n)
+        index = [slice(None)] * out.ndim
+        index[axis] = dst
+        ref = [slice(None)] * out.ndim
+        ref[axis] = slice(src, src + 1)
+        out[tuple(index)] = out[tuple(ref)]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Materials
+# ---------------------------------------------------------------------------
+
+
+def voxel_codebook(eps_grid: np.ndarray):
+    """uint8 voxel ids and a 256-entry float32 permittivity table."""
+    table, ids = np.unique(np.asarray(eps_grid, dtype=np.float32), return_inverse=True)
+    if table.size > 256:
+        raise ValueError(f"voxel material needs <= 256 distinct permittivities, got {table.size}")
+    padded = np.ones(256, np.float32)
+    padded[: table.size] = table
+    return ids.reshape(np.shape(eps_grid)).astype(np.uint8), padded
+
+
+def site_values_2d(eps_grid: np.ndarray, component: str, polarization: str = "tm") -> np.ndarray:
+    """2D supports take the owning voxel (beamz/lattice.py:935-972)."""
+    ny, nx = eps_grid.shape
+    sy, sx = component_shape(component, (ny, nx), polarization)
+    half = {"Ez": (0, 0), "Hx": (1, 0), "Hy": (0, 1), "Ex": (0, 1), "Ey": (1, 0), "Hz": (1, 1)}[component]
+    rows = np.minimum((2 * np.arange(sy) + half[0]) // 2, ny - 1)
+    cols = np.minimum((2 * np.arange(sx) + half[1]) // 2, nx - 1)
+    return np.asarray(eps_grid)[rows][:, cols]
+
+
+def e_source_2d(eps_site: np.ndarray, dt: float) -> np.ndarray:
+    """dt / (EPS_0 * eps) in float32 (beamz/simulation/kernels.py:711-728)."""
+    f32 = np.float32
+    return (f32(dt) / (f32(EPS_0) * np.asarray(eps_site, f32))).astype(f32)
+
+
+# ---------------------------------------------------------------------------
+# Sources and monitors
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class SourcePlan:
+    """field[start + idx] += coeff[idx] * waveform[clamp(step)] at one timing."""
+
+    component: str
+    timing: str  # "pre_e" | "h" | "e"
+    start: tuple
+    coeff: np.ndarray
+    waveform: np.ndarray
+
+
+def gaussian_pulse(times, freq0, fwidth, amplitude=1.0, offset=4.0, remove_dc=True) -> np.ndarray:
+    """Gaussian-modulated carrier sampled at ``times`` (beamz/devices/sources/time.py:459-487)."""
+    t = np.asarray(times, dtype=np.float64)
+    sigma_t = 1.0 / (2.0 * np.pi * max(float(fwidth), 1e-30))
+    t_peak = float(offset) / max(float(fwidth), 1e-30)
+    wave = float(amplitude) * np.exp(-0.5 * ((t - t_peak) / sigma_t) ** 2) * np.cos(2.0 * np.pi * float(freq0) * t)
+    if remove_dc and wave.size:
+        wave = wave - wave.mean()
+    return wave.astype(np.float32)
+
+
+@dataclass
+class DftMonitorPlan:
+    """A vector-DFT monitor (beamz/devices/monitors/compiler.py:62-102)."""
+
+    freqs: np.ndarray
+    indices: list  # 6 x (P, K) int32 flat offsets
+    weights: list  # 6 x (P, K) float32
+    component_mask: np.ndarray  # (6,) float32
+    t_start: float = 0.0
+    t_end: float = float("inf")
+    interval: int = 1
+    window_code: int = 0
+    normalization_code: int = 0
+    length_unit: float = 1e-6
+
+    @property
+    def points(self) -> int:
+        return int(self.indices[0].shape[0])
+
+
+def _axis_samples(n, offset, resolution):
+    return (np.arange(n, dtype=np.float64) + offset) * float(resolution)
+
+
+def _bracket(src, dst):
+    """Linear interpolation brackets and weights (beamz/lattice.py:241-271)."""
+    src = np.asarray(src, np.float64)
+    dst = np.asarray(dst, np.float64)
+    if src.size == 1:
+        z = np.zeros(dst.size, np.int32)
+        return z, z, np.ones(dst.size, np.float32), np.zeros(dst.size, np.float32)
+    hi = np.clip(np.searchsorted(src, dst, side="right"), 1, src.size - 1)
+    lo = hi - 1
+    below, above = dst <= src[0], dst >= src[-1]
+    lo[below] = hi[below] = 0
+    lo[above] = hi[above] = src.size - 1
+    span = src[hi] - src[lo]
+    frac = np.zeros_like(dst)
+    ok = (hi != lo) & (np.abs(span) > 0)
+    frac[ok] = (dst[ok] - src[lo[ok]]) / span[ok]
+    w_hi = frac.astype(np.float32)
+    w_lo = (1.0 - frac).astype(np.float32)
+    same = hi == lo
+    w_lo[same], w_hi[same] = 1.0, 0.0
+    return lo.astype(np.int32), hi.astype(np.int32), w_lo, w_hi
+
+
+def plane_gather(component, normal_axis, position, coords_a, coords_b, resolution, grid_shape):
+    """Trilinear gather plan of one component onto a plane's sample points
+    (beamz/lattice.py:274-355).  Axes are named "z", "y", "x"; ``coords_a``
+    and ``coords_b`` lie on the two in-plane axes in storage order."""
+    names = ("z", "y", "x")
+    shape = component_shape(component, grid_shape)
+    offs = {n: 0.0 if e else 0.5 for n, e in zip(names, _FACE_AXES_3D[component])}
+    in_plane = [n for n in names if n != normal_axis]
+    ga, gb = np.meshgrid(np.asarray(coords_a, float), np.asarray(coords_b, float), indexing="ij")
+    targets = {in_plane[0]: ga.ravel(), in_plane[1]: gb.ravel(), normal_axis: np.full(ga.size, float(position))}
+    axes = {}
+    for ax, n in zip(names, shape):
+        axes[ax] = _bracket(_axis_samples(n, offs[ax], resolution), targets[ax])
+    corner = np.array([[a, b, c] for a in (0, 1) for b in (0, 1) for c in (0, 1)])
+    order = (in_plane[0], in_plane[1], normal_axis)
+    pick = {}
+    weight = np.ones((ga.size, 8), np.float32)
+    for d, ax in enumerate(order):
+        lo, hi, wl, wh = axes[ax]
+        use_hi = corner[:, d][None, :] == 1
+        pick[ax] = np.where(use_hi, hi[:, None], lo[:, None])
+        weight = weight * np.where(use_hi, wh[:, None], wl[:, None])
+    flat = (pick["z"].astype(np.int64) * shape[1] + pick["y"]) * shape[2] + pick["x"]
+    keep = np.abs(weight) > 4.0 * np.finfo(np.float32).eps
+    weight = np.where(keep, weight, np.float32(0.0))
+    total = weight.sum(axis=1, keepdims=True)
+    weight = np.where(np.abs(total) > 0, weight / np.where(total == 0, 1, total), 0).astype(np.float32)
+    width = int(keep.sum(axis=1).max(initial=0))
+    if 0 < width < 8:
+        idx = np.argsort(~keep, axis=1, kind="stable")[:, :width]
+        flat = np.take_along_axis(flat, idx, axis=1)
+        weight = np.take_along_axis(weight, idx, axis=1)
+    return flat.astype(np.int32), weight.astype(np.float32)
+
+
+def plane_monitor(grid_shape, resolution, normal_axis, position, coords_a, coords_b, freqs,
+                  components=("Ey", "Ez", "Hy", "Hz"), **kwargs) -> DftMonitorPlan:
+    """A plane DFT monitor over the named components (others masked off)."""
+    idx, w = [], []
+    for c in COMPONENTS:
+        i, ww = plane_gather(c, normal_axis, position, coords_a, coords_b, resolution, grid_shape)
+        idx.append(i)
+        w.append(ww)
+    k = max(a.shape[1] for a in idx)
+    idx = [np.pad(a, ((0, 0), (0, k - a.shape[1]))) for a in idx]
+    w = [np.pad(a, ((0, 0), (0, k - a.shape[1]))) for a in w]
+    mask = np.array([1.0 if c in components else 0.0 for c in COMPONENTS], np.float32)
+    return DftMonitorPlan(np.asarray(freqs, np.float32), idx, w, mask, **kwargs)
+
+
+def step_times(t0: float, dt: float, nsteps: int) -> np.ndarray:
+    """t + dt after each step, accumulated in float32 like beamz's clock
+    (beamz/simulation/execute.py:524-541)."""
+    out = np.empty(max(int(nsteps), 1), np.float32)
+    t = np.float32(t0)
+    d = np.float32(dt)
+    for s in range(out.size):
+        t = np.float32(t + d)
+        out[s] = t
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Program description
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class ProgramSpec:
+    """Host description of one simulation's step program."""
+
+    grid_shape: tuple
+    dt: float
+    resolution: float
+    polarization: str = "tm"
+    # Voxel material (3D): uint8 ids [nz, ny, nx] and a 256-entry eps table.
+    voxel_ids: np.ndarray | None = None
+    eps_table: np.ndarray | None = None
+    # Per-site material: component -> (decay, source), scalars or full arrays.
+    e_site: dict | None = None
+    h_site: dict | None = None
+    h_terms: list = field(default_factory=list)
+    e_terms: list = field(default_factory=list)
+    metallic_edges: frozenset = frozenset()
+    sources: list = field(default_factory=list)
+    monitors: list = field(default_factory=list)
+    total_steps: int = 1
+    t0: float = 0.0
+
+    @property
+    def ndim(self) -> int:
+        return len(self.grid_shape)
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.grid_shape))
+
+    def h_coefficients(self):
+        """Uniform H decay/source: fl32(dt)/fl32(mu0) in 3D (kernels.py:495-500),
+        fl32(dt/mu0) in 2D (kernels.py:704-708)."""
+        if self.h_site is not None:
+            return self.h_site
+        if self.ndim == 3:
+            src = np.float32(np.float32(self.dt) / np.float32(MU_0))
+        else:
+            src = np.float32(float(self.dt) / MU_0)
+        return {c: (np.float32(1.0), src) for c in ("Hx", "Hy", "Hz")}

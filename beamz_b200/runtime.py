@@ -1,0 +1,387 @@
+"""Python side of the C ABI: device programs, device state and step entry points.
+
+Mirrors beamz's native runtime surface (beamz/simulation/cuda/runtime.py):
+``update_h`` / ``update_e`` advance one half step in place (184, 234),
+``run_steps`` / ``run_program_steps`` advance whole leapfrog steps with
+sources and monitors (621, 685) and ``pack_dft_monitors`` builds the monitor
+arena (530).  PyTorch tensors own every device buffer; the library only sees
+raw pointers.  There is no CPU fallback: without the library or a CUDA device
+these functions raise :class:`~beamz_b200.abi.CudaBackendUnavailable`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .plan import COMPONENT_INDEX, COMPONENTS, EPS_0, MU_0, ProgramSpec, active_components, component_shape, step_times
+
+#: Steps per native call; beamz replays 256-step CUDA-graph chunks
+#: (beamz/simulation/execute.py:64).
+GRAPH_CHUNK_STEPS = 256
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _require_cuda(device):
+    torch = _torch()
+    dev = torch.device(device)
+    if dev.type != "cuda" or not torch.cuda.is_available():
+        raise abi.CudaBackendUnavailable("beamz_b200 runs on a CUDA device only (no CPU fallback)")
+    return dev
+
+
+def _f32(x, device):
+    torch = _torch()
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(x, dtype=np.float32)), device=device)
+
+
+def _pad_last(arrays, k):
+    return [np.pad(a, ((0, 0), (0, k - a.shape[1]))) for a in arrays]
+
+
+@dataclass
+class DftArena:
+    """Device buffers of the packed monitor plan (beamz/simulation/cuda/runtime.py:530-618)."""
+
+    indices: object
+    weights: object
+    freqs: object
+    masks: object
+    counts: object
+    codes: object
+    windows: object
+    value_count: int
+    weight_count: int
+    layout: list  # per monitor: (value_offset, freq_count, point_count, weight_offset)
+
+
+def pack_dft_monitors(monitors, device) -> DftArena | None:
+    """Pad every monitor to a common (P, K, F) and lay out the ragged arena."""
+    if not monitors:
+        return None
+    M = len(monitors)
+    P = max(m.points for m in monitors)
+    K = max(max(a.shape[1] for a in m.indices) for m in monitors)
+    F = max(len(m.freqs) for m in monitors)
+    if F > 64:
+        raise ValueError("at most 64 frequencies per monitor")
+    indices = np.zeros((M, 6, P, K), np.int32)
+    weights = np.zeros((M, 6, P, K), np.float32)
+    freqs = np.zeros((M, F), np.float32)
+    masks = np.zeros((M, 6), np.float32)
+    counts = np.zeros((M, 5), np.int32)
+    codes = np.zeros((M, 2), np.int32)
+    windows = np.zeros((M, 3), np.float32)
+    voff = woff = 0
+    layout = []
+    for m, mon in enumerate(monitors):
+        p, nf = mon.points, len(mon.freqs)
+        for c in range(6):
+            ic, wc = mon.indices[c], mon.weights[c]
+            indices[m, c, :p, : ic.shape[1]] = ic
+            weights[m, c, :p, : wc.shape[1]] = wc
+        freqs[m, :nf] = mon.freqs
+        masks[m] = mon.component_mask
+        counts[m] = (nf, p, max(1, int(mon.interval)), voff, woff)
+        codes[m] = (int(mon.window_code), int(mon.normalization_code))
+        windows[m] = (mon.t_start, mon.t_end, mon.length_unit)
+        layout.append((voff, nf, p, woff))
+        voff += 6 * nf * p
+        woff += nf
+    torch = _torch()
+    t = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
+    return DftArena(t(indices), t(weights), t(freqs), t(masks), t(counts), t(codes), t(windows), voff, woff, layout)
+
+
+class DeviceProgram:
+    """A compiled program: every static input of the step, resident on the device."""
+
+    def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=0,
+                 graphs=True):
+        self.lib = abi.load_library()
+        self.device = _require_cuda(device)
+        torch = _torch()
+        self.spec = spec
+        self.ndim = spec.ndim
+        self.polarization = spec.polarization
+        self.active = active_components(spec.ndim, spec.polarization)
+        self.schedule = {"fused": abi.FDTD_SCHEDULE_FUSED, "phases": abi.FDTD_SCHEDULE_PHASES}[schedule]
+        self.shapes = {c: component_shape(c, spec.grid_shape, spec.polarization) for c in COMPONENTS}
+        dev = self.device
+        s = abi.FdtdProgram()
+        s.abi_version = abi.FDTD_ABI_VERSION
+        s.flags = abi.FDTD_FLAG_GRAPH_CACHE if graphs else 0
+        s.ndim = spec.ndim
+        s.polarization = 0 if spec.polarization == "tm" else 1
+        s.schedule = self.schedule
+        mask = 0
+        for edge in spec.metallic_edges:
+            mask |= 1 << abi.EDGE_BITS[edge]
+        s.metallic_edges = mask
+        if spec.ndim == 3:
+            s.cells[:] = [int(v) for v in spec.grid_shape]
+        else:
+            s.cells[:] = [1, int(spec.grid_shape[0]), int(spec.grid_shape[1])]
+        f32 = np.float32
+        s.dt = f32(spec.dt)
+        s.resolution = f32(spec.resolution)
+        s.inv_resolution = f32(1.0) / f32(spec.resolution)
+        s.dt_over_eps = f32(spec.dt) / f32(EPS_0)
+        s.dt_over_mu = f32(spec.dt) / f32(MU_0)
+        s.h_source = f32(float(spec.dt) / MU_0)
+        s.tile_x, s.tile_y = int(tile[0]), int(tile[1])
+        s.z_chunk = int(z_chunk)
+        self._keep = []  # tensors referenced by the struct
+
+        def buf(t):
+            self._keep.append(t)
+            return abi.buffer_of(t)
+
+        # Material.
+        if spec.voxel_ids is not None:
+            s.material_kind = abi.FDTD_MATERIAL_VOXEL
+            self.voxels = torch.as_tensor(np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8), device=dev)
+            table = np.ones(256, np.float32)
+            table[: len(spec.eps_table)] = spec.eps_table
+            self.eps_table = _f32(table, dev)
+            s.voxels = buf(self.voxels)
+            s.eps_table = buf(self.eps_table)
+        else:
+            s.material_kind = abi.FDTD_MATERIAL_SITE
+            for c in ("Ex", "Ey", "Ez"):
+                if c not in self.active:
+                    continue
+                dec, src = spec.e_site[c]
+                i = COMPONENT_INDEX[c]
+                s.e_decay[i] = buf(_f32(dec, dev))
+                s.e_source[i] = buf(_f32(src, dev))
+        for c, (dec, src) in spec.h_coefficients().items():
+            if c not in self.active:
+                continue
+            i = COMPONENT_INDEX[c] - 3
+            s.h_decay[i] = buf(_f32(dec, dev))
+            s.h_source_site[i] = buf(_f32(src, dev))
+        # CPML coefficient slabs.
+        s.cpml = 1 if (spec.h_terms or spec.e_terms) else 0
+        self.h_terms, self.e_terms = list(spec.h_terms), list(spec.e_terms)
+        for dst, terms in ((s.h_terms, self.h_terms), (s.e_terms, self.e_terms)):
+            for t, term in enumerate(terms):
+                dst[t].axis, dst[t].low, dst[t].high = term.axis, term.low, term.high
+                if term.width:
+                    dst[t].a = buf(_f32(term.a, dev))
+                    dst[t].b = buf(_f32(term.b, dev))
+                    dst[t].inv_kappa = buf(_f32(term.inv_kappa, dev))
+        # Sources.
+        if len(spec.sources) > abi.FDTD_MAX_SOURCES:
+            raise ValueError(f"at most {abi.FDTD_MAX_SOURCES} sources")
+        s.source_count = len(spec.sources)
+        for n, src in enumerate(spec.sources):
+            d = s.sources[n]
+            d.component = COMPONENT_INDEX[src.component]
+            d.timing = abi.TIMINGS[src.timing]
+            start = tuple(int(v) for v in src.start)
+            d.start[:] = list(start) if spec.ndim == 3 else [0, *start]
+            coeff = np.asarray(src.coeff, np.float32)
+            if spec.ndim == 2:
+                coeff = coeff.reshape((1, *coeff.shape))
+            d.coeff = buf(_f32(coeff, dev))
+            d.waveform = buf(_f32(np.asarray(src.waveform, np.float32).reshape(-1), dev))
+        # Monitors.
+        self.arena = pack_dft_monitors(spec.monitors, dev)
+        if self.arena is not None:
+            a = self.arena
+            s.dft.monitor_count = len(spec.monitors)
+            for name in ("indices", "weights", "freqs", "masks", "counts", "codes", "windows"):
+                setattr(s.dft, name, buf(getattr(a, name)))
+        self._times_for(max(int(spec.total_steps), 1))
+        self.struct = s
+
+    def _times_for(self, nsteps: int):
+        have = getattr(self, "_step_time_len", 0)
+        if nsteps <= have:
+            return
+        n = max(nsteps, 2 * have)
+        self.step_time_host = step_times(self.spec.t0, self.spec.dt, n)
+        self.step_time = _f32(self.step_time_host, self.device)
+        self._step_time_len = n
+
+    def clock_after(self, step: int) -> float:
+        """Float32 clock after ``step`` completed steps."""
+        if step <= 0:
+            return float(np.float32(self.spec.t0))
+        self._times_for(step)
+        return float(self.step_time_host[step - 1])
+
+    # -- struct assembly ---------------------------------------------------
+    def fill(self, state: "DeviceState", nsteps: int) -> abi.FdtdProgram:
+        s = abi.FdtdProgram.from_buffer_copy(self.struct)
+        s.nsteps = int(nsteps)
+        for c in range(6):
+            s.fields[c] = abi.buffer_of(state.fields[c])
+            if state.alt is not None:
+                s.fields_alt[c] = abi.buffer_of(state.alt[c])
+        for t, term in enumerate(self.h_terms):
+            if term.width:
+                s.h_terms[t].psi = abi.buffer_of(state.psi_h[t])
+                if state.psi_h_alt is not None:
+                    s.h_terms[t].psi_alt = abi.buffer_of(state.psi_h_alt[t])
+        for t, term in enumerate(self.e_terms):
+            if term.width:
+                s.e_terms[t].psi = abi.buffer_of(state.psi_e[t])
+        if self.arena is not None:
+            s.dft.re = abi.buffer_of(state.dft_re)
+            s.dft.im = abi.buffer_of(state.dft_im)
+            s.dft.weight_sum = abi.buffer_of(state.dft_w)
+        s.step_counter = abi.buffer_of(state.counter)
+        s.step_time = abi.buffer_of(self.step_time)
+        return s
+
+
+class DeviceState:
+    """Evolving fields, CPML memories, DFT arena and clocks (beamz/simulation/model.py:127-259)."""
+
+    def __init__(self, program: DeviceProgram, fields=None, psi_h=None, psi_e=None, step: int = 0):
+        torch = _torch()
+        dev = program.device
+        self.program = program
+        sh = program.shapes
+        empty = torch.zeros(0, dtype=torch.float32, device=dev)
+
+        def zeros(c):
+            return torch.zeros(sh[c], dtype=torch.float32, device=dev) if c in program.active else empty
+
+        if fields is None:
+            self.fields = [zeros(c) for c in COMPONENTS]
+        else:
+            self.fields = [
+                _f32(fields[c], dev).reshape(sh[c]).contiguous() if c in program.active else empty
+                for c in COMPONENTS
+            ]
+        fused = program.schedule == abi.FDTD_SCHEDULE_FUSED
+        self.alt = [torch.empty_like(f) for f in self.fields] if fused else None
+
+        def psi_list(terms, given):
+            out = []
+            for i, t in enumerate(terms):
+                shape = t.psi_shape(sh[t.component])
+                if given is not None:
+                    out.append(_f32(given[i], dev).reshape(shape).contiguous())
+                else:
+                    out.append(torch.zeros(shape, dtype=torch.float32, device=dev))
+            return out
+
+        self.psi_h = psi_list(program.h_terms, psi_h)
+        self.psi_e = psi_list(program.e_terms, psi_e)
+        self.psi_h_alt = [torch.empty_like(p) for p in self.psi_h] if fused else None
+        a = program.arena
+        nv = a.value_count if a else 0
+        nw = a.weight_count if a else 0
+        self.dft_re = torch.zeros(nv, dtype=torch.float32, device=dev)
+        self.dft_im = torch.zeros(nv, dtype=torch.float32, device=dev)
+        self.dft_w = torch.zeros(nw, dtype=torch.float32, device=dev)
+        self.counter = torch.full((1,), int(step), dtype=torch.int32, device=dev)
+        self.step = int(step)
+        self.t = program.clock_after(self.step)
+
+    def swap_banks(self):
+        self.fields, self.alt = self.alt, self.fields
+        if self.psi_h_alt is not None:
+            self.psi_h, self.psi_h_alt = self.psi_h_alt, self.psi_h
+
+    def numpy(self) -> dict:
+        """Host copies of every field, memory and accumulator."""
+        out = {c: self.fields[i].cpu().numpy() for i, c in enumerate(COMPONENTS) if c in self.program.active}
+        out["psi_h"] = [p.cpu().numpy() for p in self.psi_h]
+        out["psi_e"] = [p.cpu().numpy() for p in self.psi_e]
+        out["dft_re"] = self.dft_re.cpu().numpy()
+        out["dft_im"] = self.dft_im.cpu().numpy()
+        out["dft_w"] = self.dft_w.cpu().numpy()
+        out["t"] = np.float32(self.t)
+        out["step"] = self.step
+        return out
+
+
+def compile_program(spec: ProgramSpec, device="cuda", **kwargs) -> DeviceProgram:
+    """Upload a program's static inputs (beamz/simulation/compile.py:796-895 analogue)."""
+    return DeviceProgram(spec, device=device, **kwargs)
+
+
+def initial_state(program: DeviceProgram, **kwargs) -> DeviceState:
+    return DeviceState(program, **kwargs)
+
+
+def _stream(program: DeviceProgram):
+    return ctypes.c_void_p(_torch().cuda.current_stream(program.device).cuda_stream)
+
+
+def update_h(state: DeviceState, program: DeviceProgram) -> DeviceState:
+    """H half step in place, with CPML and PEC (beamz/simulation/cuda/runtime.py:184)."""
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_launch_phase(_stream(program), ctypes.byref(s), 0), "fdtd_launch_phase(H)")
+    return state
+
+
+def update_e(state: DeviceState, program: DeviceProgram) -> DeviceState:
+    """E half step in place, with CPML and PEC (beamz/simulation/cuda/runtime.py:234)."""
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_launch_phase(_stream(program), ctypes.byref(s), 1), "fdtd_launch_phase(E)")
+    return state
+
+
+def apply_sources(state: DeviceState, program: DeviceProgram, timing: str) -> DeviceState:
+    """Inject every source of one timing at the state's current step."""
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_apply_sources(_stream(program), ctypes.byref(s), abi.TIMINGS[timing], 0),
+              "fdtd_apply_sources")
+    return state
+
+
+def accumulate_monitors(state: DeviceState, program: DeviceProgram) -> DeviceState:
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_accumulate_dft(_stream(program), ctypes.byref(s), 0), "fdtd_accumulate_dft")
+    return state
+
+
+def step_by_phases(state: DeviceState, program: DeviceProgram) -> DeviceState:
+    """One step composed from the phase-level entries in beamz's order
+    (beamz/simulation/execute.py:467-541)."""
+    apply_sources(state, program, "pre_e")
+    update_h(state, program)
+    apply_sources(state, program, "h")
+    update_e(state, program)
+    apply_sources(state, program, "e")
+    accumulate_monitors(state, program)
+    state.counter += 1
+    state.step += 1
+    state.t = program.clock_after(state.step)
+    return state
+
+
+def run_steps(state: DeviceState, program: DeviceProgram, nsteps: int, chunk: int = GRAPH_CHUNK_STEPS) -> DeviceState:
+    """Advance ``nsteps`` complete steps (beamz/simulation/cuda/runtime.py:621/685)."""
+    if nsteps < 0:
+        raise ValueError("step count must be non-negative")
+    program._times_for(state.step + nsteps)
+    done = 0
+    stream = _stream(program)
+    while done < nsteps:
+        n = min(chunk, nsteps - done)
+        s = program.fill(state, n)
+        abi.check(program.lib.fdtd_launch_program(stream, ctypes.byref(s)), "fdtd_launch_program")
+        if program.schedule == abi.FDTD_SCHEDULE_FUSED and n % 2 == 1:
+            state.swap_banks()
+        done += n
+    state.step += nsteps
+    state.t = program.clock_after(state.step)
+    return state
+
+
+run_program_steps = run_steps

@@ -1,0 +1,221 @@
+/*
+ * fdtd_b200.h -- C ABI of the B200 FDTD leapfrog engine (sm_100a).
+ *
+ * This is the drop-in boundary for beamz's native step path.  beamz's Python
+ * runtime hands non-owning device buffers to a native library and receives a
+ * CUDA error code back (beamz: cuda/src/launch.h:12-82,
+ * beamz/simulation/cuda/runtime.py:80-86, cuda/src/ffi_handler.cc:666-708).
+ * Here the same contract is a plain C ABI: every pointer is a device pointer
+ * owned by the caller (in practice PyTorch tensors), every call enqueues work
+ * on the caller's CUDA stream and returns 0 or a cudaError_t code.  No torch
+ * or JAX type appears in any signature.
+ *
+ * Storage order is (z, y, x), row-major and contiguous, with the complete Yee
+ * supports of beamz/lattice.py:32-45 (3D) and 789-813 (2D).  Component slots
+ * are always ordered Ex, Ey, Ez, Hx, Hy, Hz.
+ */
+#ifndef FDTD_B200_H_
+#define FDTD_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
+#define FDTD_ABI_VERSION 1
+
+/* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
+enum {
+  FDTD_F32 = 0,
+  FDTD_S32 = 1,
+  FDTD_BF16 = 2,
+  FDTD_U8 = 3,
+};
+
+/* Flags (beamz: abi_layout.json "flags"; bit 7 keeps its meaning). */
+#define FDTD_FLAG_GRAPH_CACHE (1 << 7) /* capture multi-step programs into CUDA graphs */
+
+/* Step schedules. */
+enum {
+  FDTD_SCHEDULE_PHASES = 0, /* in place: H kernel, then E kernel (one field bank) */
+  FDTD_SCHEDULE_FUSED = 1,  /* one z-marching kernel per step, bank A -> bank B  */
+};
+
+/* Material encodings for the electric update. */
+enum {
+  FDTD_MATERIAL_SITE = 0,  /* per-site (or scalar) decay/source arrays, E = d*E + s*curl      */
+  FDTD_MATERIAL_VOXEL = 1, /* uint8 voxel ids + eps table; E-site eps averaged on the fly     */
+};
+
+/* Source timings (beamz/simulation/execute.py:48-52). */
+enum {
+  FDTD_TIMING_PRE_E = 0, /* added to E before the H update               */
+  FDTD_TIMING_H = 1,     /* added to H after the H update, before PEC     */
+  FDTD_TIMING_E = 2,     /* added to E after the E update, before PEC     */
+};
+
+/* Metallic (PEC) walls bitmask, order (front, back, bottom, top, left, right)
+ * = (z low, z high, y low, y high, x low, x high)
+ * (beamz/simulation/cuda/runtime.py:38-40). */
+#define FDTD_EDGE_FRONT (1 << 0)
+#define FDTD_EDGE_BACK (1 << 1)
+#define FDTD_EDGE_BOTTOM (1 << 2)
+#define FDTD_EDGE_TOP (1 << 3)
+#define FDTD_EDGE_LEFT (1 << 4)
+#define FDTD_EDGE_RIGHT (1 << 5)
+
+#define FDTD_MAX_SOURCES 16
+#define FDTD_MAX_MONITORS 16
+
+/* Non-owning buffer (replaces BeamzBuffer, beamz: cuda/src/launch.h:12-17).
+ * rank 0 = scalar; dims beyond rank are ignored. */
+typedef struct FdtdBuffer {
+  void* data;
+  int32_t rank;
+  int32_t element_type;
+  int64_t dims[4];
+} FdtdBuffer;
+
+/* One packed CPML recurrence (beamz/simulation/model.py:306-324,
+ * beamz/simulation/kernels.py:238-264).  a/b/inv_kappa are 1-D of length
+ * low + high along `axis` (0 = z, 1 = y, 2 = x of the target component);
+ * psi has the target component's shape with that axis replaced by low + high.
+ * psi_alt is the second psi bank used by FDTD_SCHEDULE_FUSED for H terms. */
+typedef struct FdtdCpmlTerm {
+  int32_t axis;
+  int32_t low;
+  int32_t high;
+  int32_t reserved;
+  FdtdBuffer a;
+  FdtdBuffer b;
+  FdtdBuffer inv_kappa;
+  FdtdBuffer psi;
+  FdtdBuffer psi_alt;
+} FdtdCpmlTerm;
+
+/* One slab injection field[start + idx] += coeff[idx] * waveform[clamp(step)]
+ * (beamz/devices/sources/compiler.py:116-129, beamz/simulation/execute.py:374-433,
+ * cuda/src/io.cu:122-168).  coeff has rank 3 (extent z, y, x); waveform rank 1. */
+typedef struct FdtdSource {
+  int32_t component; /* 0..5 = Ex..Hz */
+  int32_t timing;    /* FDTD_TIMING_* */
+  int32_t start[3];  /* z, y, x (2D: z = 0) */
+  int32_t reserved;
+  FdtdBuffer coeff;
+  FdtdBuffer waveform;
+} FdtdSource;
+
+/* Vector-DFT monitor arena (beamz: cuda/src/launch.h:47-61, observe.py:529-585).
+ *  indices  S32 [M, 6, P, K]  flat offsets into each component
+ *  weights  F32 [M, 6, P, K]
+ *  freqs    F32 [M, F]
+ *  masks    F32 [M, 6]
+ *  counts   S32 [M, 5]: freq_count, point_count, interval, value_offset, weight_offset
+ *  codes    S32 [M, 2]: window code (1 = Hann), normalization code (1 = physical)
+ *  windows  F32 [M, 3]: t_start, t_end, length_unit
+ *  re, im   F32 arena, accumulated at value_offset + (c * F + f) * P + p
+ *  weight_sum F32 arena, accumulated at weight_offset + f                       */
+typedef struct FdtdDft {
+  int32_t monitor_count;
+  int32_t reserved;
+  FdtdBuffer indices;
+  FdtdBuffer weights;
+  FdtdBuffer freqs;
+  FdtdBuffer masks;
+  FdtdBuffer counts;
+  FdtdBuffer codes;
+  FdtdBuffer windows;
+  FdtdBuffer re;
+  FdtdBuffer im;
+  FdtdBuffer weight_sum;
+} FdtdDft;
+
+/* A complete step program (replaces BeamzLaunch + BeamzProgramLaunch,
+ * beamz: cuda/src/launch.h:19-77). */
+typedef struct FdtdProgram {
+  int32_t abi_version;    /* FDTD_ABI_VERSION */
+  int32_t flags;          /* FDTD_FLAG_* */
+  int32_t ndim;           /* 2 or 3 */
+  int32_t polarization;   /* 2D: 0 = TM (Ez, Hx, Hy), 1 = TE (Ex, Ey, Hz) */
+  int32_t schedule;       /* FDTD_SCHEDULE_* */
+  int32_t material_kind;  /* FDTD_MATERIAL_* */
+  int32_t metallic_edges; /* FDTD_EDGE_* bitmask */
+  int32_t cpml;           /* 0, or 1 when h_terms/e_terms are populated */
+  int32_t nsteps;         /* steps enqueued by fdtd_launch_program */
+  int32_t source_count;
+  int64_t cells[3];       /* nz, ny, nx material cells (2D: 1, ny, nx) */
+  float dt;
+  float resolution;
+  float inv_resolution;
+  float dt_over_eps;      /* fl32(dt) / fl32(EPS_0) */
+  float dt_over_mu;       /* fl32(dt) / fl32(MU_0) */
+  float h_source;         /* 2D and scalar-H: fl32(dt / MU_0) */
+  int32_t tile_x;         /* fused-kernel tile (0 = default) */
+  int32_t tile_y;
+  int32_t z_chunk;        /* fused-kernel z planes per CTA (0 = whole axis) */
+  int32_t reserved;
+  FdtdBuffer fields[6];     /* bank A (in/out) */
+  FdtdBuffer fields_alt[6]; /* bank B (FDTD_SCHEDULE_FUSED only) */
+  /* FDTD_MATERIAL_SITE: e_decay[c], e_source[c] are rank-0 or full E-component
+   * arrays; h_decay/h_source likewise for H (rank 0 = uniform). */
+  FdtdBuffer e_decay[3];
+  FdtdBuffer e_source[3];
+  FdtdBuffer h_decay[3];
+  FdtdBuffer h_source_site[3];
+  /* FDTD_MATERIAL_VOXEL: U8 [nz, ny, nx] ids and F32 [256] permittivity table. */
+  FdtdBuffer voxels;
+  FdtdBuffer eps_table;
+  FdtdCpmlTerm h_terms[6]; /* 3D: Hxy Hxz Hyz Hyx Hzx Hzy; 2D: first 2 */
+  FdtdCpmlTerm e_terms[6]; /* 3D: Exy Exz Eyz Eyx Ezx Ezy; 2D: first 2 */
+  FdtdSource sources[FDTD_MAX_SOURCES];
+  FdtdDft dft;
+  FdtdBuffer step_counter; /* S32 [1]: absolute step of the next step, advanced on device */
+  FdtdBuffer step_time;    /* F32 [T]: t + dt after absolute step s (FP32-accumulated clock) */
+} FdtdProgram;
+
+/* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */
+int fdtd_abi_version(void);
+
+/* sizeof(FdtdProgram) as compiled into the library, so a binding can check its
+ * struct mirror before the first call (beamz: backend.py:139-157 validates the
+ * extension manifest the same way). */
+int64_t fdtd_program_size(void);
+
+/* Validate a program without enqueueing work; 0 or cudaErrorInvalidValue (1).
+ * (beamz: cuda/src/program.cu:110-170, update.cu:66-146) */
+int fdtd_validate(const FdtdProgram* program);
+
+/* One in-place half step: phase 0 = H from E, phase 1 = E from H, including
+ * CPML psi and PEC zeroing of constrained cells (beamz: BeamzLaunchStreamed,
+ * cuda/src/update.cu:919-971; beamz/simulation/cuda/runtime.py:184/234). */
+int fdtd_launch_phase(void* stream, const FdtdProgram* program, int32_t phase);
+
+/* Enqueue program->nsteps complete leapfrog steps -- sources at their three
+ * timings, H, E, PEC, DFT monitors, step counter -- on `stream`
+ * (beamz: BeamzLaunchProgram, cuda/src/program.cu:339-354;
+ * beamz/simulation/cuda/runtime.py:496/621/685).  With FDTD_SCHEDULE_FUSED
+ * an odd step count leaves the result in fields_alt / psi_alt (the caller
+ * swaps its handles); an even count leaves it in fields / psi. */
+int fdtd_launch_program(void* stream, const FdtdProgram* program);
+
+/* Add every source of `timing` for absolute step counter[0] + step_offset to
+ * its target field in `program->fields` (beamz: cuda/src/io.cu:250-286). */
+int fdtd_apply_sources(void* stream, const FdtdProgram* program, int32_t timing, int32_t step_offset);
+
+/* Accumulate the DFT monitors once from `program->fields` for absolute step
+ * counter[0] + step_offset (beamz: cuda/src/io.cu:381-401). */
+int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_offset);
+
+/* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
+void fdtd_clear_graph_cache(void);
+
+/* Human-readable name of a returned error code. */
+const char* fdtd_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDTD_B200_H_ */

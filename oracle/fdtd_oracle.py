@@ -858,7 +858,9 @@ def dft_sample_scale(weight, code, base_dt, interval, length_unit, dtype=np.floa
     native = np.maximum(f(weight), f(0.0))
     if code != 1:
         return native
-    return native * (f(base_dt * interval * LIGHT_SPEED / length_unit) / np.sqrt(f(2.0 * np.pi)))
+    # base_dt is the float32 clock scalar, so each product rounds in dtype.
+    phys = ((f(base_dt) * f(interval)) * f(LIGHT_SPEED)) / f(length_unit)
+    return native * (phys / np.sqrt(f(2.0 * np.pi)))
 
 
 def accumulate_dft(mon: DftMonitor, arena, fields, t_phys, step, dt):

@@ -1,0 +1,205 @@
+"""CUDA path (through the C ABI) against the CPU oracle and the golden vectors.
+
+Tolerances: the step is float32 arithmetic in the reference's order of
+operations, so fields are expected to agree to a few ulps
+is relative L2 <= 1e-5 for fields and <= 1e-4 for DFT accumulators, and both
+are asserted here.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from beamz_b200 import plan as P  # noqa: E402
+from beamz_b200 import runtime as R  # noqa: E402
+from oracle import fdtd_oracle as O  # noqa: E402
+from tests.golden_io import load, terms3d  # noqa: E402
+from tests.scenarios import oracle_state, random_initial_fields, scenario_2d, scenario_3d, to_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-5
+DFT_TOL = 1e-4
+
+
+def _compare(gpu: dict, st: O.OracleState, active, tol=FIELD_TOL, dft_tol=DFT_TOL):
+    for c in active:
+        err = O.relative_l2(gpu[c], st.fields[c])
+        assert err <= tol, f"{c}: rel L2 {err:.3e}"
+    for i, p in enumerate(st.psi_h):
+        if p.size:
+            assert O.relative_l2(gpu["psi_h"][i], p) <= max(tol, 1e-5), f"psi_h{i}"
+    for i, p in enumerate(st.psi_e):
+        if p.size:
+            assert O.relative_l2(gpu["psi_e"][i], p) <= max(tol, 1e-5), f"psi_e{i}"
+    if st.dft_re is not None and st.dft_re.size:
+        assert O.relative_l2(gpu["dft_re"], st.dft_re) <= dft_tol
+        assert O.relative_l2(gpu["dft_im"], st.dft_im) <= dft_tol
+        np.testing.assert_allclose(gpu["dft_w"], st.dft_w, rtol=1e-6, atol=1e-6)
+    assert np.float32(gpu["t"]) == np.float32(st.t)
+
+
+@pytest.mark.parametrize("schedule", ["fused", "phases"])
+def test_golden_steps3d(schedule):
+    """16 steps of the reference-composed fixture (CPML on 5 faces, PEC front)."""
+    d = load("steps3d")
+    grid = tuple(int(v) for v in d["grid"])
+    h_terms, e_terms, shapes = terms3d(d, grid)
+    to_plan = lambda ts: [P.CpmlTermPlan(t.component, t.axis, t.sign, t.low, t.high, t.a, t.b, t.inv_kappa) for t in ts]  # noqa: E731
+    ids, table = P.voxel_codebook(d["voxels"])
+    mon = P.DftMonitorPlan(d["freqs"], [d[f"idx_{i}"] for i in range(6)], [d[f"w_{i}"] for i in range(6)], d["cmask"])
+    spec = P.ProgramSpec(grid, float(d["dt"]), float(d["res"]), voxel_ids=ids, eps_table=table,
+                         h_terms=to_plan(h_terms), e_terms=to_plan(e_terms), metallic_edges=frozenset({"front"}),
+                         sources=[P.SourcePlan("Ey", "pre_e", (5, 5, 6), d["src_coeff"], d["wave"]),
+                                  P.SourcePlan("Hz", "h", (2, 3, 4), d["h_coeff"], d["hwave"])],
+                         monitors=[mon], total_steps=int(d["nsteps"]))
+    prog = R.compile_program(spec, schedule=schedule)
+    state = R.run_steps(R.initial_state(prog), prog, int(d["nsteps"]))
+    out = state.numpy()
+    for c in P.COMPONENTS:
+        assert O.relative_l2(out[c], d[f"out_{c}"]) <= FIELD_TOL, c
+    assert O.relative_l2(out["dft_re"], d["dft_re"]) <= DFT_TOL
+    assert O.relative_l2(out["dft_im"], d["dft_im"]) <= DFT_TOL
+    np.testing.assert_array_equal(out["dft_w"], d["dft_w"])
+    assert np.float32(out["t"]) == d["t"]
+
+
+def test_golden_single_phases():
+    """One H and one E phase from the update3d fixture (random fields and psi)."""
+    d = load("update3d")
+    grid = tuple(int(v) for v in d["grid"])
+    h_terms, e_terms, _ = terms3d(d, grid)
+    to_plan = lambda ts: [P.CpmlTermPlan(t.component, t.axis, t.sign, t.low, t.high, t.a, t.b, t.inv_kappa) for t in ts]  # noqa: E731
+    ids, table = P.voxel_codebook(d["voxels"])
+    for tag, metallic in (("open", frozenset()), ("pec", frozenset({"back", "bottom", "right"}))):
+        spec = P.ProgramSpec(grid, float(d["dt"]), float(d["res"]), voxel_ids=ids, eps_table=table,
+                             h_terms=to_plan(h_terms), e_terms=to_plan(e_terms), metallic_edges=metallic)
+        prog = R.compile_program(spec, schedule="phases")
+        fields = {c: d[f"in_{c}"] for c in P.COMPONENTS}
+        state = R.initial_state(prog, fields=fields, psi_h=[d[f"in_psi_h{i}"] for i in range(6)],
+                                psi_e=[d[f"in_psi_e{i}"] for i in range(6)])
+        R.update_h(state, prog)
+        torch.cuda.synchronize()
+        out = state.numpy()
+        if tag == "open":
+            for c in ("Hx", "Hy", "Hz"):
+                np.testing.assert_allclose(out[c], d[f"cpml_{c}"], rtol=2e-6, atol=1e-9)
+            for i in range(6):
+                np.testing.assert_allclose(out["psi_h"][i], d[f"cpml_psi_h{i}"], rtol=2e-6, atol=1e-9)
+        # E from the fixture's input H, not the updated one.
+        for i, c in enumerate(("Hx", "Hy", "Hz")):
+            state.fields[3 + i].copy_(torch.as_tensor(d[f"in_{c}"], device="cuda"))
+        R.update_e(state, prog)
+        out = state.numpy()
+        masks = O.pec_masks({c: d[f"in_{c}"].shape for c in P.COMPONENTS}, 3, metallic)
+        for c in ("Ex", "Ey", "Ez"):
+            expected = np.where(masks[c], 0.0, d[f"cpml_{tag}_{c}"])
+            np.testing.assert_allclose(out[c], expected, rtol=2e-6, atol=1e-6)
+        for i in range(6):
+            np.testing.assert_allclose(out["psi_e"][i], d[f"cpml_{tag}_psi_e{i}"], rtol=2e-6, atol=1e-6)
+
+
+CASES_3D = [
+    dict(grid=(9, 10, 11), metallic=()),
+    dict(grid=(7, 13, 5), metallic=("front", "top", "left")),
+    dict(grid=(12, 9, 40), metallic=("back", "right", "bottom"), pml_cells=4),
+    dict(grid=(6, 8, 37), cpml_edges=(), metallic=("front", "back", "bottom", "top", "left", "right")),
+    dict(grid=(10, 35, 9), cpml_edges=("left", "top", "back"), metallic=("right",)),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES_3D)))
+@pytest.mark.parametrize("schedule", ["fused", "phases"])
+def test_random_3d_against_oracle(case, schedule):
+    kw = dict(CASES_3D[case])
+    nsteps = 11
+    spec = scenario_3d(seed=case, nsteps=nsteps, **kw)
+    fields = random_initial_fields(spec, seed=case + 10)
+    prog = R.compile_program(spec, schedule=schedule)
+    state = R.run_steps(R.initial_state(prog, fields=fields), prog, nsteps)
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog, fields), oprog, nsteps)
+    _compare(state.numpy(), st, P.COMPONENTS)
+
+
+@pytest.mark.parametrize("tile", [(32, 4), (32, 8), (32, 16), (64, 4), (64, 8)])
+@pytest.mark.parametrize("z_chunk", [0, 3])
+def test_fused_tiles_and_z_chunks_are_bitwise_identical(tile, z_chunk):
+    spec = scenario_3d(grid=(11, 21, 70), seed=4, nsteps=6, metallic=("front",))
+    fields = random_initial_fields(spec, seed=5)
+    ref_prog = R.compile_program(spec, schedule="phases")
+    ref = R.run_steps(R.initial_state(ref_prog, fields=fields), ref_prog, 6).numpy()
+    prog = R.compile_program(spec, schedule="fused", tile=tile, z_chunk=z_chunk)
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, 6).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(out[c], ref[c], err_msg=c)
+    np.testing.assert_array_equal(out["dft_re"], ref["dft_re"])
+
+
+@pytest.mark.parametrize("pol", ["tm", "te"])
+@pytest.mark.parametrize("schedule", ["fused", "phases"])
+@pytest.mark.parametrize("metallic", [(), ("left", "top")])
+def test_2d_against_oracle(pol, schedule, metallic):
+    nsteps = 25
+    spec = scenario_2d(grid=(17, 23), polarization=pol, metallic=metallic, nsteps=nsteps)
+    fields = random_initial_fields(spec, seed=3)
+    prog = R.compile_program(spec, schedule=schedule)
+    state = R.run_steps(R.initial_state(prog, fields=fields), prog, nsteps)
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog, fields), oprog, nsteps)
+    _compare(state.numpy(), st, P.active_components(2, pol))
+
+
+def test_phase_entries_compose_to_the_program():
+    """pre-E sources, H, H sources, E, E sources, DFT through the phase-level ABI."""
+    spec = scenario_3d(grid=(8, 9, 10), seed=7, nsteps=5, metallic=("top",))
+    fields = random_initial_fields(spec, seed=8)
+    prog = R.compile_program(spec, schedule="phases")
+    a = R.initial_state(prog, fields=fields)
+    for _ in range(5):
+        R.step_by_phases(a, prog)
+    b = R.run_steps(R.initial_state(prog, fields=fields), prog, 5)
+    oa, ob = a.numpy(), b.numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(oa[c], ob[c])
+    np.testing.assert_array_equal(oa["dft_re"], ob["dft_re"])
+
+
+def test_chunked_runs_resume_exactly():
+    """Graph chunks, odd chunk lengths and continuation give the same state."""
+    spec = scenario_3d(grid=(8, 9, 33), seed=9, nsteps=40)
+    fields = random_initial_fields(spec, seed=2)
+    prog = R.compile_program(spec, schedule="fused")
+    one = R.run_steps(R.initial_state(prog, fields=fields), prog, 40).numpy()
+    st = R.initial_state(prog, fields=fields)
+    for n in (7, 1, 13, 19):
+        R.run_steps(st, prog, n, chunk=5)
+    two = st.numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(one[c], two[c])
+    np.testing.assert_array_equal(one["dft_im"], two["dft_im"])
+    assert one["step"] == two["step"] == 40
+
+
+def test_deterministic_across_runs():
+    spec = scenario_3d(grid=(10, 30, 41), seed=11, nsteps=8)
+    fields = random_initial_fields(spec, seed=12)
+    prog = R.compile_program(spec, schedule="fused", z_chunk=4)
+    a = R.run_steps(R.initial_state(prog, fields=fields), prog, 8).numpy()
+    b = R.run_steps(R.initial_state(prog, fields=fields), prog, 8).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(a[c], b[c])
+
+
+def test_fp64_error_is_reported_and_small():
+    """The FP32 CUDA result against the FP64 oracle (reported, loose bound)."""
+    spec = scenario_3d(grid=(10, 12, 14), seed=13, nsteps=30)
+    prog = R.compile_program(spec)
+    out = R.run_steps(R.initial_state(prog), prog, 30).numpy()
+    oprog = to_oracle(spec, np.float64)
+    st = O.run(oracle_state(oprog, dtype=np.float64), oprog, 30)
+    for c in ("Ex", "Ey", "Ez"):
+        assert O.relative_l2(out[c], st.fields[c]) <= 1e-4

@@ -1,0 +1,95 @@
+"""The product planner (beamz_b200.plan) against the oracle's restatement."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from beamz_b200 import plan as P
+from oracle import fdtd_oracle as O
+from tests.golden_io import load
+
+
+@pytest.mark.parametrize("grid", [(9, 10, 11), (20, 16, 24), (13, 15), (40, 41)])
+@pytest.mark.parametrize("pml", [3, 12])
+def test_cpml_terms_match_oracle(grid, pml):
+    if min(grid) <= 2 * pml:
+        pytest.skip("absorber would swallow the axis")
+    res = 20e-9
+    dt = 0.99 * res / (P.LIGHT_SPEED * np.sqrt(len(grid)))
+    pols = ("tm", "te") if len(grid) == 2 else ("tm",)
+    for pol in pols:
+        mh, me = P.plan_cpml(grid, dt, res, pml_cells=pml, polarization=pol)
+        oh, oe = O.plan_cpml(grid, dt, res, pml_cells=pml, polarization=pol)
+        for a, b in zip(mh + me, oh + oe):
+            assert (a.component, a.axis, a.sign, a.low, a.high) == (b.component, b.axis, b.sign, b.low, b.high)
+            np.testing.assert_array_equal(a.a, b.a)
+            np.testing.assert_array_equal(a.b, b.b)
+            np.testing.assert_array_equal(a.inv_kappa, b.inv_kappa)
+
+
+def test_cpml_terms_on_partial_edges():
+    grid = (12, 14, 16)
+    res = 20e-9
+    dt = 0.99 * res / (P.LIGHT_SPEED * np.sqrt(3))
+    edges = ("left", "top", "back")
+    mh, me = P.plan_cpml(grid, dt, res, pml_cells=4, edges=edges)
+    oh, oe = O.plan_cpml(grid, dt, res, pml_cells=4, edges=edges)
+    for a, b in zip(mh + me, oh + oe):
+        assert (a.low, a.high) == (b.low, b.high)
+        np.testing.assert_array_equal(a.a, b.a)
+
+
+@pytest.mark.parametrize("explicit", [False, True])
+def test_absorber_counts_and_extension(explicit):
+    for grid in ((30, 32, 34), (50, 60)):
+        mine = P.absorber_edge_counts(grid, 7, resolution=20e-9, explicit_thickness=explicit)
+        theirs = O.cpml_material_edge_counts(grid, 7, resolution=20e-9, explicit_thickness=explicit)
+        assert mine == theirs
+        rng = np.random.default_rng(3)
+        eps = rng.choice([2.085, 12.11], size=grid).astype(np.float32)
+        np.testing.assert_array_equal(P.extend_into_absorber(eps, mine), O.extend_materials_into_absorber(eps, theirs))
+
+
+def test_voxel_codebook_round_trips():
+    rng = np.random.default_rng(0)
+    eps = rng.choice(np.float32([1.0, 2.085, 3.5, 12.11]), size=(5, 6, 7))
+    ids, table = P.voxel_codebook(eps)
+    assert ids.dtype == np.uint8 and table.shape == (256,)
+    np.testing.assert_array_equal(table[ids], eps)
+    with pytest.raises(ValueError):
+        P.voxel_codebook(np.arange(300, dtype=np.float32))
+
+
+def test_site_sampling_2d_matches_oracle():
+    d = load("materials")
+    for pol, comps in (("tm", ("Ez", "Hx", "Hy")), ("te", ("Ex", "Ey", "Hz"))):
+        for c in comps:
+            np.testing.assert_array_equal(P.site_values_2d(d["voxels2d"], c, pol), d[f"site2d_{pol}_{c}"])
+    eps2 = P.site_values_2d(d["voxels2d"], "Ez", "tm")
+    np.testing.assert_allclose(P.e_source_2d(eps2, float(d["h2d_dt"])), d["e2d_source"], rtol=2e-7)
+
+
+def test_gaussian_pulse_matches_reference():
+    d = load("pulse")
+    f0 = float(d["f0"])
+    np.testing.assert_allclose(P.gaussian_pulse(d["times"], f0, 0.2 * f0, offset=0.5), d["signal"], rtol=1e-6,
+                               atol=1e-7)
+
+
+def test_plane_gather_matches_reference():
+    d = load("dft")
+    grid = tuple(int(v) for v in d["grid"])
+    res = 20e-9
+    for i, c in enumerate(P.COMPONENTS):
+        idx, w = P.plane_gather(c, "x", 3.25 * res, (np.arange(4) + 1.3) * res, (np.arange(5) + 0.7) * res, res, grid)
+        k = idx.shape[1]
+        np.testing.assert_array_equal(idx, d[f"idx_{i}"][:, :k])
+        np.testing.assert_allclose(w, d[f"w_{i}"][:, :k], rtol=1e-7, atol=0)
+
+
+def test_step_times_accumulate_in_float32():
+    d = load("steps3d")
+    times = P.step_times(0.0, float(d["dt"]), int(d["nsteps"]))
+    assert times[-1] == d["t"]
+    assert times.dtype == np.float32
