@@ -1,0 +1,151 @@
+"""Seeded synthetic scenes for the benchmark workloads.
+
+No public dataset is involved: permittivity voxels are written directly from
+seeded random geometry, the way beamz's own performance workloads do
+(tests/performance/h100_workloads.py:74-88 in beamz).
+
+* ``scene_3d_512``: 512 x 512 x 256 cells at 20 nm, 12-cell CPML on all faces,
+  oxide background (eps 2.085) with 8-16 Si boxes (eps 12.11, 220 nm tall,
+  200-2000 nm lateral) on one layer, an Ey Gaussian-pulse dipole at 1.55 um and
+  four x-normal DFT planes at five frequencies.
+* ``scene_capacity``: 1536 x 1024 x 1024 cells, 12-cell CPML, Si slab
+  waveguides with Gaussian sidewall roughness (sigma 2 cells).
+* ``scene_2d_400``: 400 x 400 TM cells, 20-cell CPML, a 500 nm Si strip along x,
+  a soft Ez source and one DFT line monitor at three frequencies.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import plan as P
+
+SI = 12.11
+OXIDE = 2.085
+RES = 20e-9
+F0 = P.LIGHT_SPEED / 1.55e-6
+
+
+def _dt(ndim, courant):
+    return courant * RES / (P.LIGHT_SPEED * np.sqrt(float(ndim)))
+
+
+def _dipole(component, site, eps_site, dt, total_steps, fwidth, offset, ndim=3):
+    """Point source with coeff -dt / (eps0 eps_r) at pre-E timing, sampled at
+    t0 + (i + 1/2) dt (beamz/devices/sources/compiler.py:419-461)."""
+    times = (np.arange(max(total_steps, 1), dtype=np.float64) + 0.5) * dt
+    wave = P.gaussian_pulse(times, F0, fwidth, offset=offset)
+    shape = (1,) * ndim
+    coeff = np.full(shape, -dt / (P.EPS_0 * eps_site), np.float32)
+    return P.SourcePlan(component, "pre_e", tuple(int(v) for v in site), coeff, wave)
+
+
+def _cpml_voxels(eps, pml_cells, dt, polarization="tm", explicit=False):
+    grid = eps.shape
+    h_terms, e_terms = P.plan_cpml(grid, dt, RES, pml_cells=pml_cells, polarization=polarization)
+    eps = P.extend_into_absorber(eps, P.absorber_edge_counts(grid, pml_cells, resolution=RES,
+                                                             explicit_thickness=explicit))
+    return eps, h_terms, e_terms
+
+
+def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, monitors=True, sources=True):
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    dt = _dt(3, 0.99)
+    eps = np.full(shape, OXIDE, np.float32)
+    z0 = nz // 2 - 5
+    for _ in range(int(rng.integers(8, 17))):
+        sy, sx = (int(v) for v in rng.integers(10, 101, size=2))
+        y0 = int(rng.integers(0, max(1, ny - sy)))
+        x0 = int(rng.integers(0, max(1, nx - sx)))
+        eps[z0:z0 + 11, y0:y0 + sy, x0:x0 + sx] = SI
+    eps, h_terms, e_terms = _cpml_voxels(eps, pml_cells, dt)
+    ids, table = P.voxel_codebook(eps)
+    srcs = []
+    if sources:
+        site = (nz // 2, ny // 2, nx // 2)
+        # Ey site permittivity: mean of the voxels sharing the edge.
+        k, j, i = site
+        e_site = 0.25 * (eps[k - 1, j, i - 1] + eps[k, j, i - 1] + eps[k - 1, j, i] + eps[k, j, i])
+        srcs.append(_dipole("Ey", site, float(e_site), dt, total_steps, 0.2 * F0, 0.5))
+    mons = []
+    if monitors:
+        zc = (np.arange(pml_cells, nz - pml_cells) + 0.5) * RES
+        yc = (np.arange(pml_cells, ny - pml_cells) + 0.5) * RES
+        freqs = np.linspace(0.9, 1.1, 5) * F0
+        for frac in (0.2, 0.4, 0.6, 0.8):
+            mons.append(P.plane_monitor(shape, RES, "x", frac * nx * RES, zc, yc, freqs,
+                                        components=("Ey", "Ez", "Hy", "Hz")))
+    return P.ProgramSpec(shape, dt, RES, voxel_ids=ids, eps_table=table, h_terms=h_terms, e_terms=e_terms,
+                         sources=srcs, monitors=mons, total_steps=total_steps)
+
+
+def scene_capacity(total_steps=500, seed=0, shape=(1024, 1024, 1536), pml_cells=12, monitors=False):
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    dt = _dt(3, 0.99)
+    ids = np.zeros(shape, np.uint8)  # id 0 = oxide, id 1 = Si
+    # Layered slab waveguides along x: 220 nm (11-cell) Si cores every 96 cells in
+    # z, sidewalls wandering with a smoothed Gaussian random walk (sigma 2 cells).
+    kernel = np.exp(-0.5 * (np.arange(-12, 13) / 4.0) ** 2)
+    kernel /= kernel.sum()
+    for zc in range(48, nz - 48, 96):
+        for yc in range(64, ny - 64, 128):
+            walk = np.convolve(rng.normal(0.0, 2.0, nx + 24), kernel, mode="same")[12:12 + nx]
+            lo = np.clip(np.round(yc - 12 + walk).astype(int), 0, ny)
+            hi = np.clip(np.round(yc + 12 + walk).astype(int), 0, ny)
+            for x in range(nx):
+                ids[zc - 5:zc + 6, lo[x]:hi[x], x] = 1
+    table = np.ones(256, np.float32)
+    table[0], table[1] = OXIDE, SI
+    counts = P.absorber_edge_counts(shape, pml_cells)
+    ids = P.extend_into_absorber(ids, counts)
+    h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells)
+    site = (nz // 2, ny // 2 + 64, nx // 4)
+    srcs = [_dipole("Ey", site, float(table[ids[site]]), dt, total_steps, 0.2 * F0, 0.5)]
+    return P.ProgramSpec(shape, dt, RES, voxel_ids=ids, eps_table=table, h_terms=h_terms, e_terms=e_terms,
+                         sources=srcs, monitors=[], total_steps=total_steps)
+
+
+def scene_2d_400(total_steps=2000, shape=(400, 400), pml_cells=20):
+    """2D TM (Ez, Hx, Hy): beamz's "TE with an Ez source" maps to its TM lattice
+    (beamz/lattice.py:789-813)."""
+    ny, nx = shape
+    dt = _dt(2, 0.7)
+    eps = np.full(shape, OXIDE, np.float32)
+    yc = ny // 2
+    eps[yc - 12:yc + 13, :] = SI  # 25 cells = 500 nm
+    h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells, polarization="tm")
+    eps = P.extend_into_absorber(eps, P.absorber_edge_counts(shape, pml_cells, resolution=RES, explicit_thickness=True))
+    e_site = {"Ez": (np.float32(1.0), P.e_source_2d(P.site_values_2d(eps, "Ez", "tm"), dt))}
+    site = (yc, nx // 4)
+    src = _dipole("Ez", site, float(eps[site]), dt, total_steps, 0.1 * F0, 0.5, ndim=2)
+    # Line monitor across the strip at x = 0.75 L: points along y at Ez nodes.
+    x_col = int(0.75 * nx)
+    ys = np.arange(yc - 40, yc + 41)
+    idx, w = [], []
+    for c in P.COMPONENTS:
+        sh = P.component_shape(c, shape, "tm")
+        rows = np.minimum(ys, sh[0] - 1)
+        col = min(x_col, sh[1] - 1)
+        idx.append((rows * sh[1] + col).astype(np.int32)[:, None])
+        w.append(np.ones((ys.size, 1), np.float32))
+    mask = np.array([0, 0, 1, 1, 1, 0], np.float32)
+    mon = P.DftMonitorPlan(np.array([0.95, 1.0, 1.05], np.float32) * np.float32(F0), idx, w, mask)
+    return P.ProgramSpec(shape, dt, RES, polarization="tm", e_site=e_site, h_terms=h_terms, e_terms=e_terms,
+                         sources=[src], monitors=[mon], total_steps=total_steps)
+
+
+SCENES = {"3d_512": scene_3d_512, "capacity": scene_capacity, "2d_400": scene_2d_400}
+
+
+def algorithmic_bytes(spec: P.ProgramSpec) -> int:
+    """DRAM bytes one step must move at minimum: every field element read and
+    written once (4 B each way), every voxel id read once, every CPML psi
+    element read and written once.  DFT and coefficient traffic is excluded."""
+    active = P.active_components(spec.ndim, spec.polarization)
+    shapes = {c: P.component_shape(c, spec.grid_shape, spec.polarization) for c in active}
+    field = sum(int(np.prod(s)) for s in shapes.values())
+    psi = sum(int(np.prod(t.psi_shape(shapes[t.component]))) for t in list(spec.h_terms) + list(spec.e_terms))
+    voxels = int(np.prod(spec.grid_shape)) if spec.voxel_ids is not None else 0
+    return 8 * field + voxels + 8 * psi

@@ -1,0 +1,323 @@
+"""Benchmark: 3D FP32 FDTD leapfrog steps on B200 (GCUPS and HBM roofline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--scene 3d_512|capacity|2d_400]
+
+One bench "step" is one leapfrog time step of the scene (pre-E source, H, E,
+CPML psi, PEC, DFT monitors).  The default scene is the 512 x 512 x 256
+CPML + Si-box + dipole + 4-plane DFT workload.  Every rank runs its own
+replica (the north star is single-GPU: no sharding, no collectives), so
+``value`` = cells x steps x ranks / max-over-ranks device time ("weak").
+
+``--impl reference`` times the CPU restatement of beamz's float32 step
+(oracle/fdtd_cpu.c, OpenMP over every host thread) on the same scene, each
+step a bounded z-slab sample of it, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scene", default="3d_512", choices=["3d_512", "capacity", "2d_400"])
+    ap.add_argument("--tile", default="32x8")
+    ap.add_argument("--z-chunk", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel-steps", type=int, default=200)
+    ap.add_argument("--shape", default=None, help="override the scene grid as ZxYxX (profiling runs)")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        return float(data["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(spec_fn, total_steps, budget_s, threads=0):
+    """Time the C restatement on z-slabs of the scene; returns (gcups, steps, shape, threads)."""
+    from oracle import cpu_port
+
+    cpu_port.build()
+    nthreads = threads or cpu_port.max_threads()
+    probe = spec_fn(total_steps=3, shape=(16, 512, 512), monitors=False)
+    run = cpu_port.HostRun(probe)
+    t0 = time.perf_counter()
+    run.run(2, threads=nthreads)
+    per_cell_step = (time.perf_counter() - t0) / (2 * probe.cells)
+    return per_cell_step, nthreads
+
+
+def reference_arm(args, scene_fn, cells_full):
+    """CPU restatement of the reference step: bounded z-slab samples per step."""
+    from oracle import cpu_port
+
+    per_cell, nthreads = cpu_sample(scene_fn, 3, 10.0)
+    steps = args.steps + args.warmup
+    budget = 150.0
+    nz = int(max(8, min(256, budget / max(steps, 1) / (per_cell * 512 * 512))))
+    spec = scene_fn(total_steps=steps, shape=(nz, 512, 512), monitors=True)
+    run = cpu_port.HostRun(spec)
+    run.run(args.warmup, threads=nthreads)
+    t0 = time.perf_counter()
+    run.run(args.steps, threads=nthreads)
+    dt = time.perf_counter() - t0
+    gcups = spec.cells * args.steps / dt / 1e9
+    sample = f"{args.steps} steps of a {nz}x512x512 z-slab of the 512x512x256 scene (CPML, Si boxes, dipole, 4 DFT planes)"
+    line = {
+        "impl": "reference", "metric": "GCUPS", "value": round(gcups, 4), "unit": "Gcell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "3d_512x512x256_cpml12_sibox_dipole_dft4x5", "cells": cells_full,
+                   "sample_cells": spec.cells, "threads": nthreads},
+        "cpu_baseline": {"value": round(gcups, 4), "unit": "Gcell-updates/s", "cores": nthreads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(gcups, 4), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from beamz_b200 import workloads as W
+
+    scene_fn = W.SCENES[args.scene]
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args, W.scene_3d_512, 512 * 512 * 256)
+        return
+
+    import torch.distributed as dist
+
+    from beamz_b200 import runtime as R
+
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    tile = tuple(int(v) for v in args.tile.split("x"))
+    total = args.warmup + args.steps
+    shape_kw = {"shape": tuple(int(v) for v in args.shape.split("x"))} if args.shape else {}
+    spec = scene_fn(total_steps=total, **shape_kw)
+    prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
+    state = R.initial_state(prog)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput -----------------------------------------
+    R.run_steps(state, prog, args.warmup)
+    torch.cuda.synchronize(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize(dev)
+        start.record(stream)
+        R.run_steps(state, prog, args.steps)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    ms = start.elapsed_time(end)
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    cells = spec.cells
+    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    n_src = len(spec.sources)
+    per_step = n_src + 1 + (1 if spec.monitors else 0)
+    launches = per_step * args.steps + -(-args.steps // R.GRAPH_CHUNK_STEPS)
+
+    # ---- dominant kernel alone: the fused step without sources or monitors ---
+    kspec = scene_fn(total_steps=args.kernel_steps + 3, monitors=False, sources=False, **shape_kw) \
+        if args.scene == "3d_512" else spec
+    kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
+    kstate = R.initial_state(kprog)
+    R.run_steps(kstate, kprog, 3)
+    torch.cuda.synchronize(dev)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    R.run_steps(kstate, kprog, args.kernel_steps)
+    k1.record(stream)
+    torch.cuda.synchronize(dev)
+    kernel_ms = k0.elapsed_time(k1) / args.kernel_steps
+    del kstate, kprog
+    alg_bytes = W.algorithmic_bytes(spec)
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"fused_step_{args.scene}.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            traffic = json.load(fh).get("dram_bytes_per_launch")
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        host = [torch.empty(f.shape, dtype=f.dtype, pin_memory=True) for f in state.fields]
+        for h, f in zip(host, state.fields):
+            h.copy_(f)
+        out_fields = [torch.empty_like(h, pin_memory=True) for h in host]
+        out_dft = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in (state.dft_re, state.dft_im, state.dft_w)]
+        h2d = sum(h.numel() * 4 for h in host)
+        d2h = h2d + sum(t.numel() * 4 for t in out_dft)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for f, h in zip(state.fields, host):
+            f.copy_(h, non_blocking=True)
+        R.run_steps(state, prog, args.steps)
+        for h, f in zip(out_fields, state.fields):
+            h.copy_(f, non_blocking=True)
+        for h, t in zip(out_dft, (state.dft_re, state.dft_im, state.dft_w)):
+            h.copy_(t, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
+        if world > 1:
+            dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+        e2e_value = cells * args.steps * world / (float(e2e_ms.item()) / 1e3) / 1e9
+        e2e = {"value": round(e2e_value, 3), "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
+               "transfers": "initial fields H2D from pinned host memory, final fields + DFT arena D2H, "
+                            "amortised over the run's steps"}
+
+    # ---- CPU baseline (rank 0, one GPU) -------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.scene == "3d_512" and not args.shape:
+        from oracle import cpu_port
+
+        cpu_port.build()
+        nthreads = cpu_port.max_threads()
+        per_cell, _ = cpu_sample(W.scene_3d_512, 3, 10.0, nthreads)
+        nz = int(max(8, min(256, 15.0 / 5 / (per_cell * 512 * 512))))
+        cspec = W.scene_3d_512(total_steps=5, shape=(nz, 512, 512))
+        run = cpu_port.HostRun(cspec)
+        t0 = time.perf_counter()
+        run.run(5, threads=nthreads)
+        cdt = time.perf_counter() - t0
+        cpu = {"value": round(cspec.cells * 5 / cdt / 1e9, 4), "unit": "Gcell-updates/s", "cores": nthreads,
+               "kind": "port",
+               "sample": f"5 steps of a {nz}x512x512 z-slab of the scene, C restatement (OpenMP, {nthreads} threads)"}
+
+    if rank == 0:
+        line = {
+            "metric": "GCUPS", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded voxels, beamz-style workload)",
+            "config": {"workload": f"{args.scene}" + ("_cpml12_sibox_dipole_dft4x5" if args.scene == "3d_512" else ""),
+                       "grid_zyx": list(spec.grid_shape), "cells": cells, "schedule": "fused", "tile": list(tile),
+                       "z_chunk": args.z_chunk, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (two field banks of %.1f GB)" % (2 * 4 * 6 * cells / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "fused_step_kernel", "kernel_ms": round(kernel_ms, 4),
+                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
