@@ -16,11 +16,12 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 1
+FDTD_ABI_VERSION = 2
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
 FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL = 0, 1
+FDTD_LAYOUT_DENSE, FDTD_LAYOUT_PITCHED = 0, 1
 FDTD_TIMING_PRE_E, FDTD_TIMING_H, FDTD_TIMING_E = 0, 1, 2
 FDTD_MAX_SOURCES = 16
 FDTD_MAX_MONITORS = 16
@@ -37,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_launch_program",
     "fdtd_apply_sources",
     "fdtd_accumulate_dft",
+    "fdtd_copy_component",
     "fdtd_clear_graph_cache",
     "fdtd_error_string",
 )
@@ -128,7 +130,9 @@ class FdtdProgram(ctypes.Structure):
         ("tile_x", ctypes.c_int32),
         ("tile_y", ctypes.c_int32),
         ("z_chunk", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("layout", ctypes.c_int32),
+        ("pitch", ctypes.c_int64),
+        ("voxel_pitch", ctypes.c_int64),
         ("fields", FdtdBuffer * 6),
         ("fields_alt", FdtdBuffer * 6),
         ("e_decay", FdtdBuffer * 3),
@@ -143,6 +147,7 @@ class FdtdProgram(ctypes.Structure):
         ("dft", FdtdDft),
         ("step_counter", FdtdBuffer),
         ("step_time", FdtdBuffer),
+        ("status", FdtdBuffer),
     ]
 
 
@@ -207,6 +212,9 @@ def load_library(path: str | None = None):
         lib.fdtd_apply_sources.restype = ctypes.c_int
         lib.fdtd_accumulate_dft.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32]
         lib.fdtd_accumulate_dft.restype = ctypes.c_int
+        lib.fdtd_copy_component.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdBuffer), ctypes.POINTER(FdtdBuffer),
+                                            ctypes.POINTER(ctypes.c_int64)]
+        lib.fdtd_copy_component.restype = ctypes.c_int
         lib.fdtd_clear_graph_cache.restype = None
         lib.fdtd_error_string.argtypes = [ctypes.c_int]
         lib.fdtd_error_string.restype = ctypes.c_char_p

@@ -366,10 +366,8 @@ cudaError_t launch_fused_t(cudaStream_t s, const Step3D& p) {
 
 template <int Active, bool Cpml, int Mat>
 cudaError_t launch_fused_tile(cudaStream_t s, const Step3D& p, int tx, int ty) {
-  if (tx == 32 && ty == 4) return launch_fused_t<32, 4, Active, Cpml, Mat>(s, p);
-  if (tx == 32 && ty == 16) return launch_fused_t<32, 16, Active, Cpml, Mat>(s, p);
-  if (tx == 64 && ty == 4) return launch_fused_t<64, 4, Active, Cpml, Mat>(s, p);
-  if (tx == 64 && ty == 8) return launch_fused_t<64, 8, Active, Cpml, Mat>(s, p);
+  (void)tx;
+  (void)ty;
   return launch_fused_t<32, 8, Active, Cpml, Mat>(s, p);
 }
 
@@ -384,8 +382,9 @@ cudaError_t launch_fused_a(cudaStream_t s, const Step3D& p, int mat, int tx, int
 }  // namespace
 
 cudaError_t launch_fused(cudaStream_t s, const Step3D& p, int mat, int active_mask, int tile_x, int tile_y) {
+  // 3D programs use the lean z-marching kernel (fused3d.cu); this one serves
+  // the 2D polarizations.
   switch (active_mask) {
-    case kActive3D: return launch_fused_a<kActive3D>(s, p, mat, tile_x, tile_y);
     case kActiveTM: return launch_fused_a<kActiveTM>(s, p, mat, tile_x, tile_y);
     case kActiveTE: return launch_fused_a<kActiveTE>(s, p, mat, tile_x, tile_y);
     default: return cudaErrorInvalidValue;

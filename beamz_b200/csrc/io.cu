@@ -11,8 +11,8 @@ namespace {
 // additions on PEC-constrained cells are skipped: the step zeroes those cells
 // after the update, and beamz re-applies its masks after the injection
 // (execute.py:506-522), so the two orders agree.
-__global__ void source_kernel(SourceDev s, float* target, Dims td, int timing, int metallic, const int* counter,
-                              int step_offset) {
+__global__ void source_kernel(SourceDev s, float* target, Dims td, int64_t row, int64_t plane, int timing,
+                              int metallic, const int* counter, int step_offset) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z;
@@ -23,8 +23,16 @@ __global__ void source_kernel(SourceDev s, float* target, Dims td, int timing, i
   if (timing == FDTD_TIMING_E && e_constrained(metallic, s.component, td, k, j, i)) return;
   const float amp = source_amplitude(s, counter[0] + step_offset);
   const int64_t co = (static_cast<int64_t>(z) * s.ey + y) * s.ex + x;
-  const int64_t to = lin(td, k, j, i);
+  const int64_t to = k * plane + j * row + i;
   target[to] = target[to] + s.coeff[co] * amp;
+}
+
+__global__ void copy3d_kernel(const float* src, int64_t sr, int64_t sp, float* dst, int64_t dr, int64_t dp,
+                              int64_t ny, int64_t nx) {
+  const int64_t k = blockIdx.z;
+  for (int64_t j = blockIdx.y * blockDim.y + threadIdx.y; j < ny; j += gridDim.y * blockDim.y)
+    for (int64_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
+      dst[k * dp + j * dr + i] = src[k * sp + j * sr + i];
 }
 
 // One block per (monitor, component, point tile).  The per-frequency phase and
@@ -110,14 +118,24 @@ __global__ void counter_kernel(int* counter, int nsteps) { counter[0] += nsteps;
 
 }  // namespace
 
-cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int timing, int metallic,
-                          const int* counter, int step_offset) {
+cudaError_t launch_copy3d(cudaStream_t s, const float* src, int64_t src_row, int64_t src_plane, float* dst,
+                          int64_t dst_row, int64_t dst_plane, int64_t nz, int64_t ny, int64_t nx) {
+  if (nz <= 0 || ny <= 0 || nx <= 0) return cudaSuccess;
+  const dim3 block(128, 2, 1);
+  const dim3 grid(static_cast<unsigned>((nx + 127) / 128 > 64 ? 64 : (nx + 127) / 128),
+                  static_cast<unsigned>((ny + 1) / 2 > 512 ? 512 : (ny + 1) / 2), static_cast<unsigned>(nz));
+  copy3d_kernel<<<grid, block, 0, s>>>(src, src_row, src_plane, dst, dst_row, dst_plane, ny, nx);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int64_t row, int64_t plane,
+                          int timing, int metallic, const int* counter, int step_offset) {
   if (src.ex <= 0 || src.ey <= 0 || src.ez <= 0) return cudaSuccess;
   const int bx = src.ex >= 32 ? 32 : (src.ex >= 8 ? 8 : 1);
   const int by = 256 / bx > 32 ? 32 : 256 / bx;
   const dim3 block(bx, by, 1);
   const dim3 grid((src.ex + bx - 1) / bx, (src.ey + by - 1) / by, src.ez);
-  source_kernel<<<grid, block, 0, s>>>(src, target, td, timing, metallic, counter, step_offset);
+  source_kernel<<<grid, block, 0, s>>>(src, target, td, row, plane, timing, metallic, counter, step_offset);
   return cudaPeekAtLastError();
 }
 

@@ -89,8 +89,13 @@ __device__ __forceinline__ bool h_constrained(int metallic, int c, const Dims& d
 // ---- host launchers -------------------------------------------------------
 cudaError_t launch_phase(cudaStream_t s, const Step3D& p, int phase, int mat, int active_mask);
 cudaError_t launch_fused(cudaStream_t s, const Step3D& p, int mat, int active_mask, int tile_x, int tile_y);
-cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int timing,
-                          int metallic, const int* counter, int step_offset);
+cudaError_t launch_fused_lean(cudaStream_t s, const Step3D& p, int mat, int tile_y);
+cudaError_t launch_fused_tma(cudaStream_t s, const Step3D& p, int tile_y);
+// `row`/`plane` are the target's element pitches (dense: dx and dy*dx).
+cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int64_t row,
+                          int64_t plane, int timing, int metallic, const int* counter, int step_offset);
+cudaError_t launch_copy3d(cudaStream_t s, const float* src, int64_t src_row, int64_t src_plane, float* dst,
+                          int64_t dst_row, int64_t dst_plane, int64_t nz, int64_t ny, int64_t nx);
 struct DftDev;
 cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, int step_offset);
 cudaError_t launch_counter_advance(cudaStream_t s, int* counter, int nsteps);

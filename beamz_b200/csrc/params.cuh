@@ -46,6 +46,13 @@ struct Step3D {
   const int* step_counter;
   int step_offset;
   int z_chunk;
+  // Per axis (z, y, x): coordinates [lo, hi) where no CPML term of that axis
+  // is active for any component; lets tiles and planes skip slot tests.
+  int cpml_inner[3][2];
+  // FDTD_LAYOUT_PITCHED: floats per field row, bytes per voxel row.
+  int pitch;
+  int64_t voxel_pitch;
+  int* status;  // optional error word for expired bounded waits
 };
 
 // 2D (canonical xy plane) step/phase parameters; z extent is 1.

@@ -49,9 +49,13 @@ bool layout_of(const FdtdProgram& p, Layout* out) {
   } else {
     return false;
   }
-  // Element offsets are 64-bit; per-plane coordinates stay 32-bit.
-  const int64_t lim = (int64_t{1} << 30);
-  return out->Y < lim && out->X < lim && out->Z < lim;
+  // The step kernels use 32-bit element offsets: every component array must
+  // hold fewer than 2^31 elements.
+  for (int c = 0; c < 6; ++c) {
+    const Dims d = component_dims(c, out->Z, out->Y, out->X);
+    if (static_cast<int64_t>(d.z) * d.y * d.x >= (int64_t{1} << 31)) return false;
+  }
+  return true;
 }
 
 int64_t dims_count(const Dims& d) { return static_cast<int64_t>(d.z) * d.y * d.x; }
@@ -81,18 +85,32 @@ int validate(const FdtdProgram& p) {
   Layout L;
   if (!layout_of(p, &L)) return kInvalid;
   if (p.schedule != FDTD_SCHEDULE_PHASES && p.schedule != FDTD_SCHEDULE_FUSED) return kInvalid;
+  if (p.schedule == FDTD_SCHEDULE_PHASES && p.layout != FDTD_LAYOUT_DENSE) return kInvalid;
   if (p.material_kind != FDTD_MATERIAL_SITE && p.material_kind != FDTD_MATERIAL_VOXEL) return kInvalid;
   if (p.material_kind == FDTD_MATERIAL_VOXEL && p.ndim != 3) return kInvalid;
   if (p.nsteps < 0 || p.source_count < 0 || p.source_count > FDTD_MAX_SOURCES) return kInvalid;
   if (!(p.resolution > 0.0f) || !(p.inv_resolution > 0.0f)) return kInvalid;
   if (p.metallic_edges & ~0x3F) return kInvalid;
+  const bool pitched = p.layout == FDTD_LAYOUT_PITCHED;
+  if (p.layout != FDTD_LAYOUT_DENSE && !pitched) return kInvalid;
+  if (pitched) {
+    // 3D voxel programs with uniform H coefficients; 16-byte-aligned rows.
+    if (p.ndim != 3 || p.material_kind != FDTD_MATERIAL_VOXEL) return kInvalid;
+    if (p.pitch < L.X + 1 || p.pitch % 4 != 0 || p.voxel_pitch < L.X || p.voxel_pitch % 16 != 0) return kInvalid;
+    if (static_cast<int64_t>(L.Z + 1) * (L.Y + 1) * p.pitch >= (int64_t{1} << 31)) return kInvalid;
+  }
+  auto field_ok = [&](const FdtdBuffer& b, int64_t n) {
+    if (!is_f32(b)) return false;
+    if (!pitched) return elements(b) == n && (n == 0 || b.data != nullptr);
+    return b.rank == 3 && b.dims[0] == L.Z + 1 && b.dims[1] == L.Y + 1 && b.dims[2] == p.pitch &&
+           b.data != nullptr && (reinterpret_cast<uintptr_t>(b.data) & 15) == 0;
+  };
   for (int c = 0; c < 6; ++c) {
     if (!((L.active >> c) & 1)) continue;
     const int64_t n = dims_count(component_dims(c, L.Z, L.Y, L.X));
-    if (!is_f32(p.fields[c]) || elements(p.fields[c]) != n || (n > 0 && p.fields[c].data == nullptr)) return kInvalid;
-    if (p.schedule == FDTD_SCHEDULE_FUSED &&
-        (!is_f32(p.fields_alt[c]) || elements(p.fields_alt[c]) != n || (n > 0 && p.fields_alt[c].data == nullptr)))
-      return kInvalid;
+    if (!field_ok(p.fields[c], n)) return kInvalid;
+    if (p.schedule == FDTD_SCHEDULE_FUSED && !field_ok(p.fields_alt[c], n)) return kInvalid;
+    if (pitched && (elements(p.h_decay[c % 3]) != 1 || elements(p.h_source_site[c % 3]) != 1)) return kInvalid;
     if (c < 3) {
       if (p.material_kind == FDTD_MATERIAL_SITE &&
           (!check_coeff(p.e_decay[c], n) || !check_coeff(p.e_source[c], n)))
@@ -102,8 +120,10 @@ int validate(const FdtdProgram& p) {
     }
   }
   if (p.material_kind == FDTD_MATERIAL_VOXEL) {
-    if (p.voxels.element_type != FDTD_U8 || elements(p.voxels) != static_cast<int64_t>(L.Z) * L.Y * L.X ||
-        p.voxels.data == nullptr)
+    if (p.voxels.element_type != FDTD_U8 || p.voxels.data == nullptr) return kInvalid;
+    if (!pitched && elements(p.voxels) != static_cast<int64_t>(L.Z) * L.Y * L.X) return kInvalid;
+    if (pitched && (p.voxels.rank != 3 || p.voxels.dims[0] != L.Z || p.voxels.dims[1] != L.Y ||
+                    p.voxels.dims[2] != p.voxel_pitch || (reinterpret_cast<uintptr_t>(p.voxels.data) & 15) != 0))
       return kInvalid;
     if (!is_f32(p.eps_table) || elements(p.eps_table) != 256 || p.eps_table.data == nullptr) return kInvalid;
   }
@@ -155,6 +175,7 @@ int validate(const FdtdProgram& p) {
   }
   if (p.step_counter.element_type != FDTD_S32 || elements(p.step_counter) < 1 || p.step_counter.data == nullptr)
     return kInvalid;
+  if (p.status.data != nullptr && (p.status.element_type != FDTD_S32 || elements(p.status) < 1)) return kInvalid;
   if (p.dft.monitor_count < 0 || p.dft.monitor_count > FDTD_MAX_MONITORS) return kInvalid;
   if (p.dft.monitor_count > 0) {
     const FdtdDft& d = p.dft;
@@ -251,6 +272,24 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   s.step_counter = static_cast<const int*>(p.step_counter.data);
   s.step_offset = step_offset;
   s.z_chunk = p.z_chunk;
+  s.pitch = static_cast<int>(p.pitch);
+  s.voxel_pitch = p.voxel_pitch;
+  s.status = static_cast<int*>(p.status.data);
+  for (int a = 0; a < 3; ++a) {
+    s.cpml_inner[a][0] = 0;
+    s.cpml_inner[a][1] = 1 << 30;
+  }
+  if (p.cpml) {
+    for (int t = 0; t < 6; ++t) {
+      for (const CpmlTermDev* d : {&s.ht[t], &s.et[t]}) {
+        const int a = (d == &s.ht[t] ? kHTermAxis : kETermAxis)[t];
+        if (d->low + d->high == 0) continue;
+        s.cpml_inner[a][0] = d->low > s.cpml_inner[a][0] ? d->low : s.cpml_inner[a][0];
+        const int hi = d->n_axis - d->high;
+        s.cpml_inner[a][1] = hi < s.cpml_inner[a][1] ? hi : s.cpml_inner[a][1];
+      }
+    }
+  }
   return s;
 }
 
@@ -278,8 +317,11 @@ cudaError_t enqueue_sources(cudaStream_t s, const FdtdProgram& p, const Layout& 
     const FdtdSource& src = p.sources[i];
     if (src.timing != timing) continue;
     const Dims td = component_dims(src.component, L.Z, L.Y, L.X);
-    cudaError_t err = launch_source(s, source_dev(src), static_cast<float*>(bank_fields[src.component].data), td,
-                                    timing, metallic, static_cast<const int*>(p.step_counter.data), step_offset);
+    const bool pitched = p.layout == FDTD_LAYOUT_PITCHED;
+    const int64_t row = pitched ? p.pitch : td.x;
+    const int64_t plane = pitched ? (L.Y + 1) * p.pitch : static_cast<int64_t>(td.y) * td.x;
+    cudaError_t err = launch_source(s, source_dev(src), static_cast<float*>(bank_fields[src.component].data), td, row,
+                                    plane, timing, metallic, static_cast<const int*>(p.step_counter.data), step_offset);
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
@@ -336,7 +378,13 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     if (fused) {
       sp.n_hsrc = n_hsrc;
       for (int i = 0; i < n_hsrc; ++i) sp.hsrc[i] = hsrc[i];
-      err = launch_fused(s, sp, p.material_kind, L.active, p.tile_x, p.tile_y);
+      if (p.layout == FDTD_LAYOUT_PITCHED) {
+        err = launch_fused_tma(s, sp, p.tile_y);
+      } else if (L.active == kActive3D) {
+        err = launch_fused_lean(s, sp, p.material_kind, p.tile_y);
+      } else {
+        err = launch_fused(s, sp, p.material_kind, L.active, p.tile_x, p.tile_y);
+      }
       if (err != cudaSuccess) return err;
     } else {
       err = launch_phase(s, sp, 0, p.material_kind, L.active);
@@ -431,6 +479,7 @@ int fdtd_validate(const FdtdProgram* program) {
 
 int fdtd_launch_phase(void* stream, const FdtdProgram* program, int32_t phase) {
   if (program == nullptr || (phase != 0 && phase != 1)) return fdtd::kInvalid;
+  if (program->layout != FDTD_LAYOUT_DENSE) return fdtd::kInvalid;
   FdtdProgram p = *program;
   p.schedule = FDTD_SCHEDULE_PHASES;
   const int v = fdtd::validate(p);
@@ -474,6 +523,20 @@ int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_o
   if (p.dft.monitor_count == 0) return 0;
   return static_cast<int>(fdtd::launch_dft(static_cast<cudaStream_t>(stream), fdtd::make_dft(p, p.fields),
                                            static_cast<const int*>(p.step_counter.data), step_offset));
+}
+
+int fdtd_copy_component(void* stream, const FdtdBuffer* src, const FdtdBuffer* dst, const int64_t* extent) {
+  if (src == nullptr || dst == nullptr || extent == nullptr) return fdtd::kInvalid;
+  if (src->element_type != FDTD_F32 || dst->element_type != FDTD_F32 || src->rank != 3 || dst->rank != 3)
+    return fdtd::kInvalid;
+  for (int a = 0; a < 3; ++a)
+    if (extent[a] < 0 || extent[a] > src->dims[a] || extent[a] > dst->dims[a]) return fdtd::kInvalid;
+  if (extent[0] * extent[1] * extent[2] == 0) return 0;
+  if (src->data == nullptr || dst->data == nullptr) return fdtd::kInvalid;
+  return static_cast<int>(fdtd::launch_copy3d(static_cast<cudaStream_t>(stream), static_cast<const float*>(src->data),
+                                              src->dims[2], src->dims[1] * src->dims[2],
+                                              static_cast<float*>(dst->data), dst->dims[2],
+                                              dst->dims[1] * dst->dims[2], extent[0], extent[1], extent[2]));
 }
 
 void fdtd_clear_graph_cache(void) {

@@ -63,8 +63,11 @@ class DftArena:
     layout: list  # per monitor: (value_offset, freq_count, point_count, weight_offset)
 
 
-def pack_dft_monitors(monitors, device) -> DftArena | None:
-    """Pad every monitor to a common (P, K, F) and lay out the ragged arena."""
+def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
+    """Pad every monitor to a common (P, K, F) and lay out the ragged arena.
+
+    ``remap(c, flat)`` converts dense flat offsets of component ``c`` into the
+    device layout's offsets (pitched programs)."""
     if not monitors:
         return None
     M = len(monitors)
@@ -86,6 +89,8 @@ def pack_dft_monitors(monitors, device) -> DftArena | None:
         p, nf = mon.points, len(mon.freqs)
         for c in range(6):
             ic, wc = mon.indices[c], mon.weights[c]
+            if remap is not None:
+                ic = remap(c, ic)
             indices[m, c, :p, : ic.shape[1]] = ic
             weights[m, c, :p, : wc.shape[1]] = wc
         freqs[m, :nf] = mon.freqs
@@ -104,8 +109,8 @@ def pack_dft_monitors(monitors, device) -> DftArena | None:
 class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
-    def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=0,
-                 graphs=True):
+    def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 16), z_chunk=32,
+                 graphs=True, layout="auto"):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
         torch = _torch()
@@ -116,6 +121,18 @@ class DeviceProgram:
         self.schedule = {"fused": abi.FDTD_SCHEDULE_FUSED, "phases": abi.FDTD_SCHEDULE_PHASES}[schedule]
         self.shapes = {c: component_shape(c, spec.grid_shape, spec.polarization) for c in COMPONENTS}
         dev = self.device
+        h_uniform = all(np.ndim(d) == 0 and np.ndim(s_) == 0 for d, s_ in spec.h_coefficients().values())
+        pitched_ok = (spec.ndim == 3 and spec.voxel_ids is not None and schedule == "fused" and h_uniform)
+        if layout == "auto":
+            layout = "pitched" if pitched_ok else "dense"
+        if layout == "pitched" and not pitched_ok:
+            raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule and uniform H")
+        self.layout = layout
+        if layout == "pitched":
+            nz, ny, nx = (int(v) for v in spec.grid_shape)
+            self.pitch = -(-(nx + 1) // 4) * 4
+            self.voxel_pitch = -(-nx // 16) * 16
+            self.bank_shape = (nz + 1, ny + 1, self.pitch)
         s = abi.FdtdProgram()
         s.abi_version = abi.FDTD_ABI_VERSION
         s.flags = abi.FDTD_FLAG_GRAPH_CACHE if graphs else 0
@@ -139,6 +156,10 @@ class DeviceProgram:
         s.h_source = f32(float(spec.dt) / MU_0)
         s.tile_x, s.tile_y = int(tile[0]), int(tile[1])
         s.z_chunk = int(z_chunk)
+        if layout == "pitched":
+            s.layout = abi.FDTD_LAYOUT_PITCHED
+            s.pitch = self.pitch
+            s.voxel_pitch = self.voxel_pitch
         self._keep = []  # tensors referenced by the struct
 
         def buf(t):
@@ -148,7 +169,12 @@ class DeviceProgram:
         # Material.
         if spec.voxel_ids is not None:
             s.material_kind = abi.FDTD_MATERIAL_VOXEL
-            self.voxels = torch.as_tensor(np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8), device=dev)
+            ids = np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8)
+            if layout == "pitched":
+                self.voxels = torch.zeros((ids.shape[0], ids.shape[1], self.voxel_pitch), dtype=torch.uint8, device=dev)
+                self.voxels[:, :, : ids.shape[2]].copy_(torch.as_tensor(ids, device=dev))
+            else:
+                self.voxels = torch.as_tensor(ids, device=dev)
             table = np.ones(256, np.float32)
             table[: len(spec.eps_table)] = spec.eps_table
             self.eps_table = _f32(table, dev)
@@ -195,7 +221,7 @@ class DeviceProgram:
             d.coeff = buf(_f32(coeff, dev))
             d.waveform = buf(_f32(np.asarray(src.waveform, np.float32).reshape(-1), dev))
         # Monitors.
-        self.arena = pack_dft_monitors(spec.monitors, dev)
+        self.arena = pack_dft_monitors(spec.monitors, dev, self._remap if layout == "pitched" else None)
         if self.arena is not None:
             a = self.arena
             s.dft.monitor_count = len(spec.monitors)
@@ -203,6 +229,19 @@ class DeviceProgram:
                 setattr(s.dft, name, buf(getattr(a, name)))
         self._times_for(max(int(spec.total_steps), 1))
         self.struct = s
+
+    def _remap(self, c: int, flat: np.ndarray) -> np.ndarray:
+        """Dense flat offsets of component ``c`` -> pitched offsets."""
+        dz, dy, dx = self.shapes[COMPONENTS[c]]
+        k, j, i = np.unravel_index(np.asarray(flat, np.int64), (dz, dy, dx))
+        return ((k * (self.bank_shape[1]) + j) * self.pitch + i).astype(np.int32)
+
+    def view(self, bank_tensor, component: str):
+        """The component's own extent inside a device field tensor."""
+        if self.layout != "pitched":
+            return bank_tensor
+        dz, dy, dx = self.shapes[component]
+        return bank_tensor[:dz, :dy, :dx]
 
     def _times_for(self, nsteps: int):
         have = getattr(self, "_step_time_len", 0)
@@ -242,6 +281,7 @@ class DeviceProgram:
             s.dft.weight_sum = abi.buffer_of(state.dft_w)
         s.step_counter = abi.buffer_of(state.counter)
         s.step_time = abi.buffer_of(self.step_time)
+        s.status = abi.buffer_of(state.status)
         return s
 
 
@@ -256,15 +296,14 @@ class DeviceState:
         empty = torch.zeros(0, dtype=torch.float32, device=dev)
 
         def zeros(c):
-            return torch.zeros(sh[c], dtype=torch.float32, device=dev) if c in program.active else empty
+            if c not in program.active:
+                return empty
+            shape = program.bank_shape if program.layout == "pitched" else sh[c]
+            return torch.zeros(shape, dtype=torch.float32, device=dev)
 
-        if fields is None:
-            self.fields = [zeros(c) for c in COMPONENTS]
-        else:
-            self.fields = [
-                _f32(fields[c], dev).reshape(sh[c]).contiguous() if c in program.active else empty
-                for c in COMPONENTS
-            ]
+        self.fields = [zeros(c) for c in COMPONENTS]
+        if fields is not None:
+            self.set_fields(fields)
         fused = program.schedule == abi.FDTD_SCHEDULE_FUSED
         self.alt = [torch.empty_like(f) for f in self.fields] if fused else None
 
@@ -288,6 +327,7 @@ class DeviceState:
         self.dft_im = torch.zeros(nv, dtype=torch.float32, device=dev)
         self.dft_w = torch.zeros(nw, dtype=torch.float32, device=dev)
         self.counter = torch.full((1,), int(step), dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.step = int(step)
         self.t = program.clock_after(self.step)
 
@@ -296,9 +336,28 @@ class DeviceState:
         if self.psi_h_alt is not None:
             self.psi_h, self.psi_h_alt = self.psi_h_alt, self.psi_h
 
+    def set_fields(self, fields: dict) -> None:
+        """Load host or device arrays (beamz component shapes) into the current bank."""
+        for i, c in enumerate(COMPONENTS):
+            if c in fields and c in self.program.active:
+                src = fields[c]
+                if not isinstance(src, _torch().Tensor):
+                    src = _f32(src, self.program.device)
+                self.program.view(self.fields[i], c).copy_(src.reshape(self.program.shapes[c]))
+
+    def field(self, component: str):
+        """Device view of one component in beamz's shape (may be strided)."""
+        return self.program.view(self.fields[COMPONENT_INDEX[component]], component)
+
+    def check(self) -> None:
+        """Raise if a bounded device wait expired in an earlier launch."""
+        if int(self.status.item()) != 0:
+            raise abi.FdtdError(int(self.status.item()), "device wait expired", "step kernel")
+
     def numpy(self) -> dict:
         """Host copies of every field, memory and accumulator."""
-        out = {c: self.fields[i].cpu().numpy() for i, c in enumerate(COMPONENTS) if c in self.program.active}
+        self.check()
+        out = {c: self.field(c).cpu().numpy() for c in COMPONENTS if c in self.program.active}
         out["psi_h"] = [p.cpu().numpy() for p in self.psi_h]
         out["psi_e"] = [p.cpu().numpy() for p in self.psi_e]
         out["dft_re"] = self.dft_re.cpu().numpy()

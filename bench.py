@@ -41,8 +41,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scene", default="3d_512", choices=["3d_512", "capacity", "2d_400"])
-    ap.add_argument("--tile", default="32x8")
-    ap.add_argument("--z-chunk", type=int, default=0)
+    ap.add_argument("--tile", default="32x16")
+    ap.add_argument("--z-chunk", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel-steps", type=int, default=200)
@@ -246,9 +246,12 @@ def main():
     # ---- end to end through the public API with host buffers ---------------
     e2e = None
     if not args.no_e2e:
-        host = [torch.empty(f.shape, dtype=f.dtype, pin_memory=True) for f in state.fields]
-        for h, f in zip(host, state.fields):
-            h.copy_(f)
+        from beamz_b200.plan import COMPONENTS
+
+        views = [state.field(c) for c in COMPONENTS]
+        host = [torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for v in views]
+        for h, v in zip(host, views):
+            h.copy_(v)
         out_fields = [torch.empty_like(h, pin_memory=True) for h in host]
         out_dft = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in (state.dft_re, state.dft_im, state.dft_w)]
         h2d = sum(h.numel() * 4 for h in host)
@@ -257,11 +260,11 @@ def main():
         barrier()
         torch.cuda.synchronize(dev)
         e0.record(stream)
-        for f, h in zip(state.fields, host):
-            f.copy_(h, non_blocking=True)
+        for c, h in zip(COMPONENTS, host):
+            state.field(c).copy_(h, non_blocking=True)
         R.run_steps(state, prog, args.steps)
-        for h, f in zip(out_fields, state.fields):
-            h.copy_(f, non_blocking=True)
+        for h, c in zip(out_fields, COMPONENTS):
+            h.copy_(state.field(c), non_blocking=True)
         for h, t in zip(out_dft, (state.dft_re, state.dft_im, state.dft_w)):
             h.copy_(t, non_blocking=True)
         e1.record(stream)

@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 1
+#define FDTD_ABI_VERSION 2
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
 enum {
@@ -41,6 +41,20 @@ enum {
 enum {
   FDTD_SCHEDULE_PHASES = 0, /* in place: H kernel, then E kernel (one field bank) */
   FDTD_SCHEDULE_FUSED = 1,  /* one z-marching kernel per step, bank A -> bank B  */
+};
+
+/* Field storage layouts.
+ * DENSE:   each component is its own contiguous (dz, dy, dx) array -- beamz's
+ *          complete Yee supports, exactly as the reference stores them.
+ * PITCHED: each component is a (Z+1, Y+1, pitch) float array, pitch a multiple
+ *          of 4 and >= X+1, holding the component in its (dz, dy, dx) corner;
+ *          the voxel ids are a (Z, Y, voxel_pitch) byte array, voxel_pitch a
+ *          multiple of 16.  All rows are 16-byte aligned, which lets the fused
+ *          3D step stage planes with TMA.  3D, voxel material and uniform H
+ *          coefficients only; fdtd_copy_component converts between layouts. */
+enum {
+  FDTD_LAYOUT_DENSE = 0,
+  FDTD_LAYOUT_PITCHED = 1,
 };
 
 /* Material encodings for the electric update. */
@@ -155,7 +169,9 @@ typedef struct FdtdProgram {
   int32_t tile_x;         /* fused-kernel tile (0 = default) */
   int32_t tile_y;
   int32_t z_chunk;        /* fused-kernel z planes per CTA (0 = whole axis) */
-  int32_t reserved;
+  int32_t layout;         /* FDTD_LAYOUT_* */
+  int64_t pitch;          /* PITCHED: floats per row of every field array */
+  int64_t voxel_pitch;    /* PITCHED: bytes per row of the voxel array */
   FdtdBuffer fields[6];     /* bank A (in/out) */
   FdtdBuffer fields_alt[6]; /* bank B (FDTD_SCHEDULE_FUSED only) */
   /* FDTD_MATERIAL_SITE: e_decay[c], e_source[c] are rank-0 or full E-component
@@ -173,6 +189,7 @@ typedef struct FdtdProgram {
   FdtdDft dft;
   FdtdBuffer step_counter; /* S32 [1]: absolute step of the next step, advanced on device */
   FdtdBuffer step_time;    /* F32 [T]: t + dt after absolute step s (FP32-accumulated clock) */
+  FdtdBuffer status;       /* S32 [1], optional: set nonzero when a bounded device wait expired */
 } FdtdProgram;
 
 /* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */
@@ -207,6 +224,11 @@ int fdtd_apply_sources(void* stream, const FdtdProgram* program, int32_t timing,
 /* Accumulate the DFT monitors once from `program->fields` for absolute step
  * counter[0] + step_offset (beamz: cuda/src/io.cu:381-401). */
 int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_offset);
+
+/* Copy the (extent[0], extent[1], extent[2]) corner block between two rank-3
+ * F32 buffers whose own dims give their row and plane pitches (dense <->
+ * pitched field layouts).  No beamz counterpart: beamz keeps one layout. */
+int fdtd_copy_component(void* stream, const FdtdBuffer* src, const FdtdBuffer* dst, const int64_t* extent);
 
 /* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
 void fdtd_clear_graph_cache(void);

@@ -33,8 +33,7 @@ _lib = None
 def load():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        build()  # make is incremental; rebuilds when fdtd_cpu.c or the ABI header changed
         lib = ctypes.CDLL(LIB)
         lib.fdtd_cpu_run.argtypes = [ctypes.POINTER(abi.FdtdProgram), ctypes.c_int]
         lib.fdtd_cpu_run.restype = ctypes.c_int
