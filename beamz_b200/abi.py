@@ -16,11 +16,11 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 2
+FDTD_ABI_VERSION = 3
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
-FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL = 0, 1
+FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL, FDTD_MATERIAL_CODEBOOK = 0, 1, 2
 FDTD_LAYOUT_DENSE, FDTD_LAYOUT_PITCHED = 0, 1
 FDTD_TIMING_PRE_E, FDTD_TIMING_H, FDTD_TIMING_E = 0, 1, 2
 FDTD_MAX_SOURCES = 16
@@ -132,7 +132,7 @@ class FdtdProgram(ctypes.Structure):
         ("z_chunk", ctypes.c_int32),
         ("layout", ctypes.c_int32),
         ("pitch", ctypes.c_int64),
-        ("voxel_pitch", ctypes.c_int64),
+        ("reserved64", ctypes.c_int64),
         ("fields", FdtdBuffer * 6),
         ("fields_alt", FdtdBuffer * 6),
         ("e_decay", FdtdBuffer * 3),
@@ -141,6 +141,8 @@ class FdtdProgram(ctypes.Structure):
         ("h_source_site", FdtdBuffer * 3),
         ("voxels", FdtdBuffer),
         ("eps_table", FdtdBuffer),
+        ("site_ids", FdtdBuffer),
+        ("site_coef", FdtdBuffer),
         ("h_terms", FdtdCpmlTerm * 6),
         ("e_terms", FdtdCpmlTerm * 6),
         ("sources", FdtdSource * FDTD_MAX_SOURCES),

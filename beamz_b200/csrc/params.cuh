@@ -15,6 +15,10 @@ struct EMaterial {
   // FDTD_MATERIAL_VOXEL: voxel ids [Z, Y, X] and permittivity table [256].
   const uint8_t* voxels;
   const float* eps_table;
+  // FDTD_MATERIAL_CODEBOOK: one word per lattice point (Ex, Ey, Ez ids in
+  // bytes 0-2) on the field pitch, and three 256-entry coefficient tables.
+  const uint32_t* site_ids;
+  const float* site_coef;
 };
 
 // Magnetic update coefficients (uniform or per-site).
@@ -49,9 +53,8 @@ struct Step3D {
   // Per axis (z, y, x): coordinates [lo, hi) where no CPML term of that axis
   // is active for any component; lets tiles and planes skip slot tests.
   int cpml_inner[3][2];
-  // FDTD_LAYOUT_PITCHED: floats per field row, bytes per voxel row.
+  // FDTD_LAYOUT_PITCHED: floats per row of every field and site-id array.
   int pitch;
-  int64_t voxel_pitch;
   int* status;  // optional error word for expired bounded waits
 };
 

@@ -86,7 +86,9 @@ int validate(const FdtdProgram& p) {
   if (!layout_of(p, &L)) return kInvalid;
   if (p.schedule != FDTD_SCHEDULE_PHASES && p.schedule != FDTD_SCHEDULE_FUSED) return kInvalid;
   if (p.schedule == FDTD_SCHEDULE_PHASES && p.layout != FDTD_LAYOUT_DENSE) return kInvalid;
-  if (p.material_kind != FDTD_MATERIAL_SITE && p.material_kind != FDTD_MATERIAL_VOXEL) return kInvalid;
+  if (p.material_kind != FDTD_MATERIAL_SITE && p.material_kind != FDTD_MATERIAL_VOXEL &&
+      p.material_kind != FDTD_MATERIAL_CODEBOOK)
+    return kInvalid;
   if (p.material_kind == FDTD_MATERIAL_VOXEL && p.ndim != 3) return kInvalid;
   if (p.nsteps < 0 || p.source_count < 0 || p.source_count > FDTD_MAX_SOURCES) return kInvalid;
   if (!(p.resolution > 0.0f) || !(p.inv_resolution > 0.0f)) return kInvalid;
@@ -94,10 +96,12 @@ int validate(const FdtdProgram& p) {
   const bool pitched = p.layout == FDTD_LAYOUT_PITCHED;
   if (p.layout != FDTD_LAYOUT_DENSE && !pitched) return kInvalid;
   if (pitched) {
-    // 3D voxel programs with uniform H coefficients; 16-byte-aligned rows.
-    if (p.ndim != 3 || p.material_kind != FDTD_MATERIAL_VOXEL) return kInvalid;
-    if (p.pitch < L.X + 1 || p.pitch % 4 != 0 || p.voxel_pitch < L.X || p.voxel_pitch % 16 != 0) return kInvalid;
+    // 3D codebook programs with uniform H coefficients; 16-byte-aligned rows.
+    if (p.ndim != 3 || p.material_kind != FDTD_MATERIAL_CODEBOOK) return kInvalid;
+    if (p.pitch < L.X + 1 || p.pitch % 4 != 0) return kInvalid;
     if (static_cast<int64_t>(L.Z + 1) * (L.Y + 1) * p.pitch >= (int64_t{1} << 31)) return kInvalid;
+  } else if (p.material_kind == FDTD_MATERIAL_CODEBOOK) {
+    return kInvalid;  // the codebook shares the pitched field layout
   }
   auto field_ok = [&](const FdtdBuffer& b, int64_t n) {
     if (!is_f32(b)) return false;
@@ -121,11 +125,15 @@ int validate(const FdtdProgram& p) {
   }
   if (p.material_kind == FDTD_MATERIAL_VOXEL) {
     if (p.voxels.element_type != FDTD_U8 || p.voxels.data == nullptr) return kInvalid;
-    if (!pitched && elements(p.voxels) != static_cast<int64_t>(L.Z) * L.Y * L.X) return kInvalid;
-    if (pitched && (p.voxels.rank != 3 || p.voxels.dims[0] != L.Z || p.voxels.dims[1] != L.Y ||
-                    p.voxels.dims[2] != p.voxel_pitch || (reinterpret_cast<uintptr_t>(p.voxels.data) & 15) != 0))
-      return kInvalid;
+    if (elements(p.voxels) != static_cast<int64_t>(L.Z) * L.Y * L.X) return kInvalid;
     if (!is_f32(p.eps_table) || elements(p.eps_table) != 256 || p.eps_table.data == nullptr) return kInvalid;
+  }
+  if (p.material_kind == FDTD_MATERIAL_CODEBOOK) {
+    const FdtdBuffer& ids = p.site_ids;
+    if (ids.element_type != FDTD_S32 || ids.rank != 3 || ids.dims[0] != L.Z + 1 || ids.dims[1] != L.Y + 1 ||
+        ids.dims[2] != p.pitch || ids.data == nullptr || (reinterpret_cast<uintptr_t>(ids.data) & 15) != 0)
+      return kInvalid;
+    if (!is_f32(p.site_coef) || elements(p.site_coef) != 3 * 256 || p.site_coef.data == nullptr) return kInvalid;
   }
   if (p.cpml) {
     const int nterms = p.ndim == 3 ? 6 : 2;
@@ -257,6 +265,10 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
     s.em.voxels = static_cast<const uint8_t*>(p.voxels.data);
     s.em.eps_table = static_cast<const float*>(p.eps_table.data);
   }
+  if (p.material_kind == FDTD_MATERIAL_CODEBOOK) {
+    s.em.site_ids = static_cast<const uint32_t*>(p.site_ids.data);
+    s.em.site_coef = static_cast<const float*>(p.site_coef.data);
+  }
   if (p.cpml) {
     const int nterms = p.ndim == 3 ? 6 : 2;
     for (int t = 0; t < nterms; ++t) {
@@ -273,7 +285,6 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   s.step_offset = step_offset;
   s.z_chunk = p.z_chunk;
   s.pitch = static_cast<int>(p.pitch);
-  s.voxel_pitch = p.voxel_pitch;
   s.status = static_cast<int*>(p.status.data);
   for (int a = 0; a < 3; ++a) {
     s.cpml_inner[a][0] = 0;

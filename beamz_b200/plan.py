@@ -233,6 +233,109 @@ def voxel_codebook(eps_grid: np.ndarray):
     return ids.reshape(np.shape(eps_grid)).astype(np.uint8), padded
 
 
+# E-site coefficient codebook (pitched 3D layout).  The E update coefficient at
+# a site is fl(fl(dt)/fl(eps0) * fl(1/eps_site)), with eps_site the centered
+# average 0.5*(0.5*(t0+t1) + 0.5*(t2+t3)) of four voxel samples
+# (beamz/lattice.py:732-786: z, then y, then x, each with clipped indices).
+# On the edge-replicated voxel grid vp (Z+2, Y+2, X+2), vp[k+dk, j+dj, i+di]
+# is voxel (clip(k-1+dk), clip(j-1+dj), clip(i-1+di)); these are the (dk, dj,
+# di) of t0..t3 per component, in averaging order.
+CODEBOOK_TAPS = {
+    "Ex": ((0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 1, 1)),  # average z, then y
+    "Ey": ((0, 1, 0), (1, 1, 0), (0, 1, 1), (1, 1, 1)),  # average z, then x
+    "Ez": ((1, 0, 0), (1, 1, 0), (1, 0, 1), (1, 1, 1)),  # average y, then x
+}
+#: The 4-tuple key space m**4 must stay addressable by int32 keys.
+CODEBOOK_MAX_MATERIALS = 46
+
+
+class CodebookOverflow(ValueError):
+    """The program has more distinct E-site coefficients than a codebook holds."""
+
+
+def codebook_keys(vp, m: int, component: str, k0: int, k1: int):
+    """Tuple keys ((t0*m + t1)*m + t2)*m + t3 of one component's sites on
+    lattice planes [k0, k1) x (Y+1) x (X+1).
+
+    ``vp`` is the edge-replicated grid of compact material indices (0..m-1),
+    as a numpy array or a torch tensor of an integer type wide enough for m**4.
+    """
+    ny, nx = vp.shape[1] - 1, vp.shape[2] - 1
+    t = [vp[k0 + dk:k1 + dk, dj:dj + ny, di:di + nx] for dk, dj, di in CODEBOOK_TAPS[component]]
+    return ((t[0] * m + t[1]) * m + t[2]) * m + t[3]
+
+
+def edge_replicated(compact: np.ndarray) -> np.ndarray:
+    """(Z, Y, X) -> (Z+2, Y+2, X+2) with each face copied outward once."""
+    return np.pad(compact, 1, mode="edge")
+
+
+def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict):
+    """Per-component lookup tables from tuple key to codebook id, and the
+    coefficient tables.
+
+    ``eps_used`` holds the m permittivities in compact-index order and
+    ``present[c]`` flags which of the m**4 keys occur.  Returns ``(luts, coef)``:
+    ``luts[c]`` is a uint8 array of m**4 ids (0 where a key is absent) and
+    ``coef`` the float32 (3, 256) tables.  Raises :class:`CodebookOverflow` when
+    a component has more than 256 distinct coefficients.
+    """
+    f32 = np.float32
+    e = np.asarray(eps_used, f32)
+    half = f32(0.5)
+    a = half * (e[:, None, None, None] + e[None, :, None, None])
+    b = half * (e[None, None, :, None] + e[None, None, None, :])
+    eps_site = (half * (a + b)).reshape(-1)
+    coef_all = f32(dt_over_eps) * (f32(1.0) / eps_site)
+    luts, coef = {}, np.zeros((3, 256), f32)
+    for n, c in enumerate(("Ex", "Ey", "Ez")):
+        mask = np.asarray(present[c], bool)
+        values, inverse = np.unique(coef_all[mask], return_inverse=True)
+        if values.size > 256:
+            raise CodebookOverflow(f"{c}: {values.size} distinct E-site coefficients (> 256)")
+        lut = np.zeros(coef_all.size, np.uint8)
+        lut[mask] = inverse.astype(np.uint8)
+        luts[c] = lut
+        coef[n, : values.size] = values
+    return luts, coef
+
+
+def compact_materials(voxel_ids: np.ndarray, eps_table: np.ndarray):
+    """Compact voxel ids to 0..m-1 over the ids that occur.
+
+    Returns ``(remap, eps_used)``: ``remap`` is a 256-entry int32 table from
+    voxel id to compact index and ``eps_used`` the m permittivities.
+    """
+    used = np.flatnonzero(np.bincount(np.asarray(voxel_ids, np.uint8).reshape(-1), minlength=256))
+    if used.size > CODEBOOK_MAX_MATERIALS:
+        raise CodebookOverflow(f"{used.size} materials (> {CODEBOOK_MAX_MATERIALS}) for the site codebook")
+    remap = np.zeros(256, np.int32)
+    remap[used] = np.arange(used.size, dtype=np.int32)
+    table = np.ones(256, np.float32)
+    table[: len(eps_table)] = np.asarray(eps_table, np.float32)
+    return remap, table[used]
+
+
+def site_codebook(voxel_ids: np.ndarray, eps_table: np.ndarray, dt_over_eps):
+    """Host build of the site-id words and coefficient tables.
+
+    Returns ``(words, coef)``: ``words`` is an int32 (Z+1, Y+1, X+1) array whose
+    bytes 0, 1, 2 are the Ex, Ey, Ez codebook ids at each lattice point, and
+    ``coef`` the float32 (3, 256) coefficient tables.
+    """
+    remap, eps_used = compact_materials(voxel_ids, eps_table)
+    m = eps_used.size
+    vp = edge_replicated(remap[np.asarray(voxel_ids, np.uint8)])
+    nz = vp.shape[0] - 2
+    keys = {c: codebook_keys(vp, m, c, 0, nz + 1) for c in ("Ex", "Ey", "Ez")}
+    present = {c: np.bincount(keys[c].reshape(-1), minlength=m**4) > 0 for c in keys}
+    luts, coef = codebook_tables(eps_used, dt_over_eps, present)
+    words = np.zeros(keys["Ex"].shape, np.int32)
+    for shift, c in ((0, "Ex"), (8, "Ey"), (16, "Ez")):
+        words |= luts[c][keys[c]].astype(np.int32) << shift
+    return words, coef
+
+
 def site_values_2d(eps_grid: np.ndarray, component: str, polarization: str = "tm") -> np.ndarray:
     """2D supports take the owning voxel (beamz/lattice.py:935-972)."""
     ny, nx = eps_grid.shape

@@ -17,7 +17,20 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import abi
-from .plan import COMPONENT_INDEX, COMPONENTS, EPS_0, MU_0, ProgramSpec, active_components, component_shape, step_times
+from .plan import (
+    COMPONENT_INDEX,
+    COMPONENTS,
+    EPS_0,
+    MU_0,
+    CodebookOverflow,
+    ProgramSpec,
+    active_components,
+    codebook_keys,
+    codebook_tables,
+    compact_materials,
+    component_shape,
+    step_times,
+)
 
 #: Steps per native call; beamz replays 256-step CUDA-graph chunks
 #: (beamz/simulation/execute.py:64).
@@ -45,6 +58,45 @@ def _f32(x, device):
 
 def _pad_last(arrays, k):
     return [np.pad(a, ((0, 0), (0, k - a.shape[1]))) for a in arrays]
+
+
+def _replicated_slab(torch, ids, remap, k0: int, k1: int):
+    """Edge-replicated compact material planes for lattice planes [k0, k1):
+    voxel planes clip(k0-1) .. clip(k1), one replicated row/column per side."""
+    nz = ids.shape[0]
+    zi = torch.arange(k0 - 1, k1 + 1, device=ids.device).clamp_(0, nz - 1)
+    slab = remap[ids.index_select(0, zi).long()]
+    slab = torch.cat([slab[:, :1], slab, slab[:, -1:]], dim=1)
+    return torch.cat([slab[:, :, :1], slab, slab[:, :, -1:]], dim=2)
+
+
+def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, z_block: int = 32):
+    """Site-id words (Z+1, Y+1, pitch) int32 and coefficient tables (3, 256) on
+    the device; equal bit for bit to :func:`beamz_b200.plan.site_codebook` (the
+    device part is integer gathers only; coefficients come from the host)."""
+    torch = _torch()
+    remap_np, eps_used = compact_materials(voxel_ids, eps_table)
+    m = int(eps_used.size)
+    ids = torch.as_tensor(np.ascontiguousarray(voxel_ids, np.uint8), device=device)
+    remap = torch.as_tensor(remap_np, device=device)
+    nz, ny, nx = (int(v) for v in ids.shape)
+    blocks = [(k, min(k + z_block, nz + 1)) for k in range(0, nz + 1, z_block)]
+    comps = ("Ex", "Ey", "Ez")
+    present = {c: torch.zeros(m**4, dtype=torch.bool, device=device) for c in comps}
+    for k0, k1 in blocks:
+        vp = _replicated_slab(torch, ids, remap, k0, k1)
+        for c in comps:
+            keys = codebook_keys(vp, m, c, 0, k1 - k0).reshape(-1).long()
+            present[c] |= torch.bincount(keys, minlength=m**4) > 0
+    luts, coef = codebook_tables(eps_used, dt_over_eps, {c: present[c].cpu().numpy() for c in comps})
+    lut = {c: torch.as_tensor(luts[c].astype(np.int32), device=device) for c in comps}
+    words = torch.zeros((nz + 1, ny + 1, pitch), dtype=torch.int32, device=device)
+    for k0, k1 in blocks:
+        vp = _replicated_slab(torch, ids, remap, k0, k1)
+        w = words[k0:k1, :, : nx + 1]
+        for shift, c in ((0, "Ex"), (8, "Ey"), (16, "Ez")):
+            w |= lut[c][codebook_keys(vp, m, c, 0, k1 - k0).long()] << shift
+    return words, torch.as_tensor(coef, device=device)
 
 
 @dataclass
@@ -123,16 +175,26 @@ class DeviceProgram:
         dev = self.device
         h_uniform = all(np.ndim(d) == 0 and np.ndim(s_) == 0 for d, s_ in spec.h_coefficients().values())
         pitched_ok = (spec.ndim == 3 and spec.voxel_ids is not None and schedule == "fused" and h_uniform)
-        if layout == "auto":
-            layout = "pitched" if pitched_ok else "dense"
         if layout == "pitched" and not pitched_ok:
             raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule and uniform H")
-        self.layout = layout
-        if layout == "pitched":
+        f32 = np.float32
+        dt_over_eps = f32(spec.dt) / f32(EPS_0)
+        self.site_ids = self.site_coef = None
+        if layout in ("auto", "pitched") and pitched_ok:
             nz, ny, nx = (int(v) for v in spec.grid_shape)
             self.pitch = -(-(nx + 1) // 4) * 4
-            self.voxel_pitch = -(-nx // 16) * 16
             self.bank_shape = (nz + 1, ny + 1, self.pitch)
+            try:
+                self.site_ids, self.site_coef = device_site_codebook(
+                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev)
+                layout = "pitched"
+            except CodebookOverflow:
+                if layout == "pitched":
+                    raise
+                layout = "dense"
+        elif layout == "auto":
+            layout = "dense"
+        self.layout = layout
         s = abi.FdtdProgram()
         s.abi_version = abi.FDTD_ABI_VERSION
         s.flags = abi.FDTD_FLAG_GRAPH_CACHE if graphs else 0
@@ -147,11 +209,10 @@ class DeviceProgram:
             s.cells[:] = [int(v) for v in spec.grid_shape]
         else:
             s.cells[:] = [1, int(spec.grid_shape[0]), int(spec.grid_shape[1])]
-        f32 = np.float32
         s.dt = f32(spec.dt)
         s.resolution = f32(spec.resolution)
         s.inv_resolution = f32(1.0) / f32(spec.resolution)
-        s.dt_over_eps = f32(spec.dt) / f32(EPS_0)
+        s.dt_over_eps = dt_over_eps
         s.dt_over_mu = f32(spec.dt) / f32(MU_0)
         s.h_source = f32(float(spec.dt) / MU_0)
         s.tile_x, s.tile_y = int(tile[0]), int(tile[1])
@@ -159,7 +220,6 @@ class DeviceProgram:
         if layout == "pitched":
             s.layout = abi.FDTD_LAYOUT_PITCHED
             s.pitch = self.pitch
-            s.voxel_pitch = self.voxel_pitch
         self._keep = []  # tensors referenced by the struct
 
         def buf(t):
@@ -167,14 +227,14 @@ class DeviceProgram:
             return abi.buffer_of(t)
 
         # Material.
-        if spec.voxel_ids is not None:
+        if layout == "pitched":
+            s.material_kind = abi.FDTD_MATERIAL_CODEBOOK
+            s.site_ids = buf(self.site_ids)
+            s.site_coef = buf(self.site_coef)
+        elif spec.voxel_ids is not None:
             s.material_kind = abi.FDTD_MATERIAL_VOXEL
             ids = np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8)
-            if layout == "pitched":
-                self.voxels = torch.zeros((ids.shape[0], ids.shape[1], self.voxel_pitch), dtype=torch.uint8, device=dev)
-                self.voxels[:, :, : ids.shape[2]].copy_(torch.as_tensor(ids, device=dev))
-            else:
-                self.voxels = torch.as_tensor(ids, device=dev)
+            self.voxels = torch.as_tensor(ids, device=dev)
             table = np.ones(256, np.float32)
             table[: len(spec.eps_table)] = spec.eps_table
             self.eps_table = _f32(table, dev)

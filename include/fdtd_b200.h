@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 2
+#define FDTD_ABI_VERSION 3
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
 enum {
@@ -47,10 +47,9 @@ enum {
  * DENSE:   each component is its own contiguous (dz, dy, dx) array -- beamz's
  *          complete Yee supports, exactly as the reference stores them.
  * PITCHED: each component is a (Z+1, Y+1, pitch) float array, pitch a multiple
- *          of 4 and >= X+1, holding the component in its (dz, dy, dx) corner;
- *          the voxel ids are a (Z, Y, voxel_pitch) byte array, voxel_pitch a
- *          multiple of 16.  All rows are 16-byte aligned, which lets the fused
- *          3D step stage planes with TMA.  3D, voxel material and uniform H
+ *          of 4 and >= X+1, holding the component in its (dz, dy, dx) corner.
+ *          All rows are 16-byte aligned, which lets the fused 3D step stage
+ *          planes with TMA.  3D, FDTD_MATERIAL_CODEBOOK and uniform H
  *          coefficients only; fdtd_copy_component converts between layouts. */
 enum {
   FDTD_LAYOUT_DENSE = 0,
@@ -61,6 +60,7 @@ enum {
 enum {
   FDTD_MATERIAL_SITE = 0,  /* per-site (or scalar) decay/source arrays, E = d*E + s*curl      */
   FDTD_MATERIAL_VOXEL = 1, /* uint8 voxel ids + eps table; E-site eps averaged on the fly     */
+  FDTD_MATERIAL_CODEBOOK = 2, /* per-site uint8 ids of E coefficients (pitched layout)        */
 };
 
 /* Source timings (beamz/simulation/execute.py:48-52). */
@@ -171,7 +171,7 @@ typedef struct FdtdProgram {
   int32_t z_chunk;        /* fused-kernel z planes per CTA (0 = whole axis) */
   int32_t layout;         /* FDTD_LAYOUT_* */
   int64_t pitch;          /* PITCHED: floats per row of every field array */
-  int64_t voxel_pitch;    /* PITCHED: bytes per row of the voxel array */
+  int64_t reserved64;
   FdtdBuffer fields[6];     /* bank A (in/out) */
   FdtdBuffer fields_alt[6]; /* bank B (FDTD_SCHEDULE_FUSED only) */
   /* FDTD_MATERIAL_SITE: e_decay[c], e_source[c] are rank-0 or full E-component
@@ -183,6 +183,12 @@ typedef struct FdtdProgram {
   /* FDTD_MATERIAL_VOXEL: U8 [nz, ny, nx] ids and F32 [256] permittivity table. */
   FdtdBuffer voxels;
   FdtdBuffer eps_table;
+  /* FDTD_MATERIAL_CODEBOOK: S32 [Z+1, Y+1, pitch] words whose bytes 0, 1, 2 are
+   * the ids of the Ex, Ey, Ez coefficient fl(fl(dt)/fl(eps0) * fl(1/eps_site))
+   * at that lattice point (beamz: compile.py:146-187 packs its lossless E
+   * material the same way), and the F32 [3, 256] coefficient tables. */
+  FdtdBuffer site_ids;
+  FdtdBuffer site_coef;
   FdtdCpmlTerm h_terms[6]; /* 3D: Hxy Hxz Hyz Hyx Hzx Hzy; 2D: first 2 */
   FdtdCpmlTerm e_terms[6]; /* 3D: Exy Exz Eyz Eyx Ezx Ezy; 2D: first 2 */
   FdtdSource sources[FDTD_MAX_SOURCES];

@@ -133,3 +133,42 @@ def test_runtime_refuses_cpu_devices():
         pytest.skip("a CUDA device is present")
     with pytest.raises(abi.CudaBackendUnavailable):
         runtime.compile_program(scenario_3d(), device="cpu")
+
+
+def _pitched_program():
+    """A 3D fused program on the pitched layout with the site codebook."""
+    Z, Y, X = 4, 5, 6
+    pitch = 8
+    s = _valid_program()
+    s.schedule = abi.FDTD_SCHEDULE_FUSED
+    s.layout = abi.FDTD_LAYOUT_PITCHED
+    s.material_kind = abi.FDTD_MATERIAL_CODEBOOK
+    s.pitch = pitch
+    for c in range(6):
+        s.fields[c] = _fake((Z + 1, Y + 1, pitch), ptr=0x1000 * (c + 1))
+        s.fields_alt[c] = _fake((Z + 1, Y + 1, pitch), ptr=0x10000 * (c + 1))
+    s.voxels = abi.FdtdBuffer()
+    s.eps_table = abi.FdtdBuffer()
+    s.site_ids = _fake((Z + 1, Y + 1, pitch), abi.FDTD_S32, ptr=0x200000)
+    s.site_coef = _fake((3, 256))
+    return s
+
+
+def test_validate_pitched_codebook_program(lib):
+    assert lib.fdtd_validate(ctypes.byref(_pitched_program())) == 0
+
+
+@pytest.mark.parametrize("mutate", [
+    lambda s: setattr(s, "pitch", 6),                                     # < X + 1
+    lambda s: setattr(s, "pitch", 9),                                     # not a multiple of 4
+    lambda s: setattr(s, "site_ids", _fake((5, 6, 8), abi.FDTD_F32)),     # wrong type
+    lambda s: setattr(s, "site_ids", _fake((5, 6, 8), abi.FDTD_S32, ptr=0x1004)),  # misaligned
+    lambda s: setattr(s, "site_coef", _fake((256,))),
+    lambda s: setattr(s, "material_kind", abi.FDTD_MATERIAL_VOXEL),       # pitched needs the codebook
+    lambda s: setattr(s, "layout", abi.FDTD_LAYOUT_DENSE),                # codebook needs pitched
+    lambda s: s.h_decay.__setitem__(0, _fake((4, 5, 7))),                 # non-uniform H
+])
+def test_validate_rejects_inconsistent_pitched_programs(lib, mutate):
+    s = _pitched_program()
+    mutate(s)
+    assert lib.fdtd_validate(ctypes.byref(s)) == 1

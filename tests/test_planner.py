@@ -93,3 +93,47 @@ def test_step_times_accumulate_in_float32():
     times = P.step_times(0.0, float(d["dt"]), int(d["nsteps"]))
     assert times[-1] == d["t"]
     assert times.dtype == np.float32
+
+
+@pytest.mark.parametrize("grid,nmat", [((5, 6, 7), 2), ((4, 9, 3), 5), ((1, 4, 4), 1)])
+def test_site_codebook_matches_oracle_sampling(grid, nmat):
+    """Every E site's codebook coefficient equals fl(dt/eps0 * fl(1/eps_site))
+    with eps_site sampled the oracle's way (clipped centered averages)."""
+    rng = np.random.default_rng(sum(grid) + nmat)
+    table = np.linspace(1.0, 12.25, nmat).astype(np.float32)
+    ids = rng.integers(0, nmat, size=grid).astype(np.uint8)
+    dto = np.float32(2.0e-17) / np.float32(P.EPS_0)
+    words, coef = P.site_codebook(ids, table, dto)
+    assert words.shape == tuple(n + 1 for n in grid)
+    eps_grid = table[ids]
+    for n, c in enumerate(("Ex", "Ey", "Ez")):
+        eps_site = O.sample_e_site_3d(eps_grid, c).astype(np.float32)
+        want = dto * (np.float32(1.0) / eps_site)
+        dz, dy, dx = eps_site.shape
+        got = coef[n][(words[:dz, :dy, :dx] >> (8 * n)) & 0xFF]
+        np.testing.assert_array_equal(got, want)
+
+
+def test_device_codebook_equals_host_build():
+    """The torch (device) builder, run here on CPU tensors, equals the numpy one."""
+    torch = pytest.importorskip("torch")
+    from beamz_b200.runtime import device_site_codebook
+
+    rng = np.random.default_rng(7)
+    grid = (7, 10, 13)
+    table = np.array([1.0, 2.25, 3.5, 12.0], np.float32)
+    ids = rng.integers(0, 4, size=grid).astype(np.uint8)
+    dto = np.float32(1.7e-17) / np.float32(P.EPS_0)
+    words, coef = P.site_codebook(ids, table, dto)
+    pitch = 16
+    dev_words, dev_coef = device_site_codebook(ids, table, dto, pitch, torch.device("cpu"), z_block=3)
+    dev_words = dev_words.numpy()
+    np.testing.assert_array_equal(dev_words[:, :, : grid[2] + 1], words)
+    assert not dev_words[:, :, grid[2] + 1:].any()
+    np.testing.assert_array_equal(dev_coef.numpy(), coef)
+
+
+def test_codebook_overflow_is_reported():
+    ids = np.arange(60, dtype=np.uint8).reshape(3, 4, 5)
+    with pytest.raises(P.CodebookOverflow):
+        P.site_codebook(ids, np.linspace(1, 9, 60).astype(np.float32), np.float32(1.0))
