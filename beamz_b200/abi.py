@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_copy_component",
     "fdtd_clear_graph_cache",
     "fdtd_error_string",
+    "fdtd_registrations",
 )
 
 
@@ -106,6 +107,10 @@ class FdtdDft(ctypes.Structure):
         ("im", FdtdBuffer),
         ("weight_sum", FdtdBuffer),
     ]
+
+
+class FdtdRegistration(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("fn", ctypes.c_void_p)]
 
 
 class FdtdProgram(ctypes.Structure):
@@ -220,6 +225,8 @@ def load_library(path: str | None = None):
         lib.fdtd_clear_graph_cache.restype = None
         lib.fdtd_error_string.argtypes = [ctypes.c_int]
         lib.fdtd_error_string.restype = ctypes.c_char_p
+        lib.fdtd_registrations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+        lib.fdtd_registrations.restype = ctypes.POINTER(FdtdRegistration)
         version = lib.fdtd_abi_version()
         if version != FDTD_ABI_VERSION:
             raise CudaBackendUnavailable(f"ABI mismatch: library {version}, bindings {FDTD_ABI_VERSION}")
@@ -231,6 +238,14 @@ def load_library(path: str | None = None):
         if path is None:
             _LIB = lib
         return lib
+
+
+def registrations(lib=None) -> dict:
+    """Target name -> entry-point address, from the library's own table."""
+    lib = lib or load_library()
+    n = ctypes.c_int32(0)
+    table = lib.fdtd_registrations(ctypes.byref(n))
+    return {table[i].name.decode(): table[i].fn for i in range(n.value)}
 
 
 def check(code: int, where: str) -> None:

@@ -559,4 +559,13 @@ void fdtd_clear_graph_cache(void) {
 
 const char* fdtd_error_string(int code) { return cudaGetErrorString(static_cast<cudaError_t>(code)); }
 
+const FdtdRegistration* fdtd_registrations(int32_t* count) {
+  static const FdtdRegistration table[] = {
+      {"fdtd_phase", reinterpret_cast<void*>(&fdtd_launch_phase)},
+      {"fdtd_program", reinterpret_cast<void*>(&fdtd_launch_program)},
+  };
+  if (count != nullptr) *count = static_cast<int32_t>(sizeof(table) / sizeof(table[0]));
+  return table;
+}
+
 }  // extern "C"

@@ -161,7 +161,7 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
 class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
-    def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 16), z_chunk=32,
+    def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
                  graphs=True, layout="auto"):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)

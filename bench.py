@@ -41,8 +41,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scene", default="3d_512", choices=["3d_512", "capacity", "2d_400"])
-    ap.add_argument("--tile", default="32x16")
-    ap.add_argument("--z-chunk", type=int, default=32)
+    ap.add_argument("--tile", default="32x8")
+    ap.add_argument("--z-chunk", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel-steps", type=int, default=200)
@@ -186,7 +186,8 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     tile = tuple(int(v) for v in args.tile.split("x"))
-    total = args.warmup + args.steps
+    primes = 1 if args.steps % 2 == 0 else 2
+    total = args.warmup + (primes + 2) * args.steps
     shape_kw = {"shape": tuple(int(v) for v in args.shape.split("x"))} if args.shape else {}
     spec = scene_fn(total_steps=total, **shape_kw)
     prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
@@ -197,8 +198,16 @@ def main():
         if world > 1:
             dist.barrier()
 
+    def prime(st, pr, nsteps):
+        """Untimed pass over the exact chunk sequence of a timed run, so every
+        CUDA graph it replays is captured and instantiated before timing (the
+        graph key holds the bank order, hence a second pass for odd counts)."""
+        for _ in range(1 if nsteps % 2 == 0 else 2):
+            R.run_steps(st, pr, nsteps)
+
     # ---- device-resident throughput -----------------------------------------
     R.run_steps(state, prog, args.warmup)
+    prime(state, prog, args.steps)
     torch.cuda.synchronize(dev)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -221,11 +230,12 @@ def main():
     launches = per_step * args.steps + -(-args.steps // R.GRAPH_CHUNK_STEPS)
 
     # ---- dominant kernel alone: the fused step without sources or monitors ---
-    kspec = scene_fn(total_steps=args.kernel_steps + 3, monitors=False, sources=False, **shape_kw) \
+    kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw) \
         if args.scene == "3d_512" else spec
     kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
     kstate = R.initial_state(kprog)
     R.run_steps(kstate, kprog, 3)
+    prime(kstate, kprog, args.kernel_steps)
     torch.cuda.synchronize(dev)
     k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     k0.record(stream)
@@ -238,8 +248,8 @@ def main():
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"fused_step_{args.scene}.json")
-    if os.path.exists(prof):
+    prof = os.path.join(ROOT, "profiles", f"tma_step_{args.scene}.json")
+    if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16:
         with open(prof) as fh:
             traffic = json.load(fh).get("dram_bytes_per_launch")
 
@@ -309,7 +319,7 @@ def main():
                        "l2": "inputs larger than L2 (two field banks of %.1f GB)" % (2 * 4 * 6 * cells / 1e9)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "fused_step_kernel", "kernel_ms": round(kernel_ms, 4),
+                         "kernel": "tma_step_kernel" if prog.layout == "pitched" else "fused step", "kernel_ms": round(kernel_ms, 4),
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
             "gpu_launches": launches,
             "clocks": clocks.summary(),

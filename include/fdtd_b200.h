@@ -242,6 +242,18 @@ void fdtd_clear_graph_cache(void);
 /* Human-readable name of a returned error code. */
 const char* fdtd_error_string(int code);
 
+/* One launch entry point by target name. */
+typedef struct FdtdRegistration {
+  const char* name;
+  void* fn;
+} FdtdRegistration;
+
+/* The launch entry points keyed by target name, as beamz's extension module
+ * lists its FFI targets (beamz: cuda/src/extension.cc:13-21 registrations()):
+ * "fdtd_phase" -> fdtd_launch_phase, "fdtd_program" -> fdtd_launch_program.
+ * Writes the entry count to *count (when non-null); the table is static. */
+const FdtdRegistration* fdtd_registrations(int32_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,7 @@ def lib():
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|void|const char\*)\s+(fdtd_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|void|const char\*|const FdtdRegistration\*)\s+(fdtd_\w+)\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol(lib):
@@ -32,6 +32,13 @@ def test_library_exports_every_declared_symbol(lib):
     assert set(names) == set(abi.EXPORTED_SYMBOLS)
     for name in names:
         assert hasattr(lib, name), name
+
+
+def test_registrations_table(lib):
+    regs = abi.registrations(lib)
+    assert set(regs) == {"fdtd_phase", "fdtd_program"}
+    assert regs["fdtd_phase"] == ctypes.cast(lib.fdtd_launch_phase, ctypes.c_void_p).value
+    assert regs["fdtd_program"] == ctypes.cast(lib.fdtd_launch_program, ctypes.c_void_p).value
 
 
 def test_struct_layout_and_version(lib):
