@@ -34,6 +34,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace fdtd {
@@ -48,7 +50,7 @@ struct TmaTile {
   static constexpr int BX = TX + 8;  // staged row: x from i0-4 to i0+TX+3
   static constexpr int EH = TY + 2;  // E rows j0-1 .. j0+TY
   static constexpr int HH = TY + 1;  // H rows j0-1 .. j0+TY-1
-  static constexpr int HW = TX + 1;  // H-region columns i0-1 .. i0+TX-1
+  static constexpr int HW = TX + 2;  // H-region columns i0-1 .. i0+TX (the last: column X of the last tile)
   static constexpr int EBOX = ((EH * BX + 31) / 32) * 32;  // floats; boxes start on 128 B
   static constexpr int HBOX = ((HH * BX + 31) / 32) * 32;
   static constexpr int IBOX = TY * TX;  // site-id words, rows j0 .. j0+TY-1
@@ -181,6 +183,47 @@ __device__ __forceinline__ float cpml_apply(const CpmlTermDev& t, const CpmlOp& 
   return d * op.c.z + psi;
 }
 
+// CPML halves for the straight-line paths: every term of a cell is fetched
+// (slot, offset, psi) before any is applied, so the loads are in flight
+// together; apply runs psi <- b psi + a d and returns d / kappa + psi with
+// (a, b, 1/kappa) staged in shared memory.
+struct Psi {
+  int slot = -1;
+  int off = 0;
+  float v = 0.0f;
+};
+
+template <int Axis>
+__device__ __forceinline__ int psi_offset(const CpmlTermDev& t, int slot, int k, int j, int i) {
+  const int pk = Axis == 0 ? slot : k;
+  const int pj = Axis == 1 ? slot : j;
+  const int pi = Axis == 2 ? slot : i;
+  return (pk * t.pdy + pj) * t.pdx + pi;
+}
+
+template <int Axis>
+__device__ __forceinline__ Psi psi_fetch(const CpmlTermDev& t, int slot, int k, int j, int i) {
+  Psi q;
+  q.slot = slot;
+  if (slot >= 0) {
+    q.off = psi_offset<Axis>(t, slot, k, j, i);
+    q.v = t.psi_in[q.off];
+  }
+  return q;
+}
+
+__device__ __forceinline__ float psi_apply(const CpmlTermDev& t, const float4* cc, const Psi& q, float d,
+                                           bool write) {
+  if (q.slot < 0) return d;
+  const float4 c = cc[q.slot];
+  const float next = c.y * q.v + c.x * d;
+  if (write) t.psi_out[q.off] = next;
+  return d * c.z + next;
+}
+
+using kOff = std::integral_constant<bool, false>;
+using kOn = std::integral_constant<bool, true>;
+
 __device__ __forceinline__ float h_sources(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
   for (int s = 0; s < p.n_hsrc; ++s) {
     const SourceDev& src = p.hsrc[s];
@@ -270,14 +313,21 @@ __global__ void __launch_bounds__(32 * NW, 1024 / (32 * NW))
   const HFast hf{p.hm.decay[0][0], p.hm.decay[1][0], p.hm.decay[2][0], p.hm.source[0][0], p.hm.source[1][0],
                  p.hm.source[2][0], res, inv_res};
   const int i = i0 + lane;
-  // Interior box: off every domain face and clear of every absorber slab.
-  const int zin0 = Cpml ? max(1, p.cpml_inner[0][0]) : 1, zin1 = Cpml ? min(Z, p.cpml_inner[0][1]) : Z;
-  const int yin0 = Cpml ? max(1, p.cpml_inner[1][0]) : 1, yin1 = Cpml ? min(Y, p.cpml_inner[1][1]) : Y;
-  const int xin0 = Cpml ? max(1, p.cpml_inner[2][0]) : 1, xin1 = Cpml ? min(X, p.cpml_inner[2][1]) : X;
-  // The whole tile, own cells and both halos, inside the interior box.
-  const bool tile_inner = i0 - 1 >= xin0 && i0 + T::TX <= xin1 && j0 - 1 >= yin0 && j0 + T::TY <= yin1;
-  const bool cpml_xy = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + T::TX <= p.cpml_inner[2][1] &&
+  // When X is a multiple of the tile width, the last tile also owns the
+  // face column i = X (Hx, Ey, Ez there), computed by its last warp, so no
+  // CTA is spent on a single column.
+  const bool xcol = X % T::TX == 0 && i0 + T::TX == X;
+  const int xe = xcol ? 1 : 0;
+  const bool cpml_xy = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + T::TX + xe <= p.cpml_inner[2][1] &&
                                  j0 - 1 >= p.cpml_inner[1][0] && j0 + T::TY <= p.cpml_inner[1][1]);
+  // Straight-line tiles: below the y-high face and left of the x-high face
+  // (the low faces x = 0 and y = 0 by per-lane / per-row selects, column X
+  // by the last warp), with every CPML coefficient staged in shared memory.
+  const bool mid_ok = j0 + T::TY <= Y && i0 + T::TX <= X && cc_smem;
+  const bool xface = i0 == 0, yface = j0 == 0;
+  // Axes whose absorber slabs the tile (own cells and halos) touches.
+  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + T::TX + xe <= p.cpml_inner[2][1]);
+  const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + T::TY <= p.cpml_inner[1][1]);
 
   int e0 = kstart % 3, e1 = (kstart + 1) % 3, hs = kstart & 1;
   for (int k = kstart; k < k1; ++k) {
@@ -308,52 +358,191 @@ __global__ void __launch_bounds__(32 * NW, 1024 / (32 * NW))
     const uint32_t* IDS = sm.ids[hs];
     const int hb = k & 1, pb = hb ^ 1;
     const bool src = p.n_hsrc > 0 && sources_hit(p, k, j0 - 1, j0 + T::TY, i0 - 1, i0 + T::TX);
-    const bool fast = tile_inner && k >= zin0 && k < zin1 && !src;
 
-    if (fast) {
-      // ---- straight-line tile: every own and halo cell is interior -------
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int ly = 1 + warp * R + r, lx = 1 + lane, b = ly * BX + lane + 4;
-        const float hx = hf.hx<BX>(E0z, E0y, E1y, HOx, b);
-        const float hy = hf.hy<BX>(E0x, E0z, E1x, HOy, b);
-        const float hz = hf.hz<BX>(E0y, E0x, HOz, b);
-        sm.hn[hb][0][ly][lx] = hx;
-        sm.hn[hb][1][ly][lx] = hy;
-        sm.hn[hb][2][ly][lx] = hz;
-        if (emit) {
-          const int o = k * PL + (j0 + ly - 1) * P + i;
-          p.hout[0][o] = hx;
-          p.hout[1][o] = hy;
-          p.hout[2][o] = hz;
+    if (mid_ok && !src && k >= 1 && k < Z) {
+      // ---- straight-line tile-plane --------------------------------------
+      // Every own and halo cell is a valid site of all six components; the
+      // faces x = 0 (i0 == 0) and y = 0 (j0 == 0) drop their halo and take the
+      // ghost value by select; column X (xcol) is the last warp's extra work.
+      // CPML terms run only for the axes whose slabs the tile-plane touches,
+      // chosen at compile time: AX, AY, AZ.
+      auto body = [&](auto axc, auto ayc, auto azc) {
+        constexpr bool AX = decltype(axc)::value, AY = decltype(ayc)::value, AZ = decltype(azc)::value;
+        int zh1 = -1, zh2 = -1, ze1 = -1, ze2 = -1;  // plane-uniform z slots
+        if constexpr (AZ) {
+          zh1 = cpml_slot(p.ht[1], k);
+          zh2 = cpml_slot(p.ht[2], k);
+          ze1 = cpml_slot(p.et[1], k);
+          ze2 = cpml_slot(p.et[2], k);
         }
-      }
-      if (warp == 0) {  // y-halo row: Hx, Hz
-        const int b = lane + 4;
-        sm.hn[hb][0][0][1 + lane] = hf.hx<BX>(E0z, E0y, E1y, HOx, b);
-        sm.hn[hb][2][0][1 + lane] = hf.hz<BX>(E0y, E0x, HOz, b);
-      } else if (warp == 1 && lane < T::TY) {  // x-halo column: Hy, Hz
-        const int b = (1 + lane) * BX + 3;
-        sm.hn[hb][1][1 + lane][0] = hf.hy<BX>(E0x, E0z, E1x, HOy, b);
-        sm.hn[hb][2][1 + lane][0] = hf.hz<BX>(E0y, E0x, HOz, b);
-      }
-      __syncthreads();
-      if (emit) {
+        // H at box index b, lattice (k, j, ii); W: 1 Hx, 2 Hy, 4 Hz.
+        auto h_cell = [&](auto wc, int b, int j, int ii, bool own, float* hv) {
+          constexpr int W = decltype(wc)::value;
+          Psi q0, q1, q2, q3, q4, q5;
+          if constexpr ((W & 1) && AY) q0 = psi_fetch<1>(p.ht[0], cpml_slot(p.ht[0], j), k, j, ii);
+          if constexpr ((W & 1) && AZ) q1 = psi_fetch<0>(p.ht[1], zh1, k, j, ii);
+          if constexpr ((W & 2) && AZ) q2 = psi_fetch<0>(p.ht[2], zh2, k, j, ii);
+          if constexpr ((W & 2) && AX) q3 = psi_fetch<2>(p.ht[3], cpml_slot(p.ht[3], ii), k, j, ii);
+          if constexpr ((W & 4) && AX) q4 = psi_fetch<2>(p.ht[4], cpml_slot(p.ht[4], ii), k, j, ii);
+          if constexpr ((W & 4) && AY) q5 = psi_fetch<1>(p.ht[5], cpml_slot(p.ht[5], j), k, j, ii);
+          if constexpr ((W & 1) != 0) {  // Hx: dEz/dy - dEy/dz
+            float d0 = div_rn(E0z[b + BX] - E0z[b], res, inv_res);
+            float d1 = div_rn(E1y[b] - E0y[b], res, inv_res);
+            if constexpr (AY) d0 = psi_apply(p.ht[0], sm.cc[0], q0, d0, own);
+            if constexpr (AZ) d1 = psi_apply(p.ht[1], sm.cc[1], q1, d1, own);
+            const float h = hf.dec0 * HOx[b] - hf.src0 * (d0 - d1);
+            hv[0] = ((xface && ii == 0 && wx0) || (ii == X && wx1)) ? 0.0f : h;
+          }
+          if constexpr ((W & 2) != 0) {  // Hy: dEx/dz - dEz/dx
+            float d0 = div_rn(E1x[b] - E0x[b], res, inv_res);
+            float d1 = div_rn(E0z[b + 1] - E0z[b], res, inv_res);
+            if constexpr (AZ) d0 = psi_apply(p.ht[2], sm.cc[2], q2, d0, own);
+            if constexpr (AX) d1 = psi_apply(p.ht[3], sm.cc[3], q3, d1, own);
+            const float h = hf.dec1 * HOy[b] - hf.src1 * (d0 - d1);
+            hv[1] = (yface && j == 0 && wy0) ? 0.0f : h;
+          }
+          if constexpr ((W & 4) != 0) {  // Hz: dEy/dx - dEx/dy
+            float d0 = div_rn(E0y[b + 1] - E0y[b], res, inv_res);
+            float d1 = div_rn(E0x[b + BX] - E0x[b], res, inv_res);
+            if constexpr (AX) d0 = psi_apply(p.ht[4], sm.cc[4], q4, d0, own);
+            if constexpr (AY) d1 = psi_apply(p.ht[5], sm.cc[5], q5, d1, own);
+            hv[2] = hf.dec2 * HOz[b] - hf.src2 * (d0 - d1);
+          }
+        };
+        using W1 = std::integral_constant<int, 1>;
+        using W7 = std::integral_constant<int, 7>;
+        using W5 = std::integral_constant<int, 5>;
+        using W6 = std::integral_constant<int, 6>;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int ly = 1 + warp * R + r, lx = 1 + lane, b = ly * BX + lane + 4;
+          float hv[3];
+          h_cell(W7{}, b, j0 + ly - 1, i, emit, hv);
+          sm.hn[hb][0][ly][lx] = hv[0];
+          sm.hn[hb][1][ly][lx] = hv[1];
+          sm.hn[hb][2][ly][lx] = hv[2];
+          if (emit) {
+            const int o = k * PL + (j0 + ly - 1) * P + i;
+            p.hout[0][o] = hv[0];
+            p.hout[1][o] = hv[1];
+            p.hout[2][o] = hv[2];
+          }
+        }
+        if (warp == 0) {  // y-halo row: Hx, Hz
+          if (!yface) {
+            float hv[3];
+            h_cell(W5{}, lane + 4, j0 - 1, i, false, hv);
+            sm.hn[hb][0][0][1 + lane] = hv[0];
+            sm.hn[hb][2][0][1 + lane] = hv[2];
+          }
+        } else if (warp == 1 && lane < T::TY && !xface) {  // x-halo column: Hy, Hz
+          float hv[3];
+          h_cell(W6{}, (1 + lane) * BX + 3, j0 + lane, i0 - 1, false, hv);
+          sm.hn[hb][1][1 + lane][0] = hv[1];
+          sm.hn[hb][2][1 + lane][0] = hv[2];
+        }
+        if (xcol && warp == NW - 1 && lane <= T::TY && !(yface && lane == 0)) {  // Hx on column X
+          float hv[3];
+          const int j = j0 - 1 + lane;
+          h_cell(W1{}, lane * BX + T::TX + 4, j, X, emit && lane >= 1, hv);
+          sm.hn[hb][0][lane][T::TX + 1] = hv[0];
+          if (emit && lane >= 1) p.hout[0][k * PL + j * P + X] = hv[0];
+        }
+        __syncthreads();
+        if (!emit) return;
+        if (xcol && warp == NW - 1 && lane < T::TY) {  // Ey, Ez on column X
+          const int ly = 1 + lane, j = j0 + lane, b = ly * BX + T::TX + 4;
+          const float hx = sm.hn[hb][0][ly][T::TX + 1], hx_z = sm.hn[pb][0][ly][T::TX + 1];
+          float hx_y = sm.hn[hb][0][ly - 1][T::TX + 1];
+          const float hz_x = sm.hn[hb][2][ly][T::TX], hy_x = sm.hn[hb][1][ly][T::TX];
+          // Ghost beyond x = X: zero on a metallic wall, else the edge value.
+          const float hz = wx1 ? 0.0f : hz_x, hy = wx1 ? 0.0f : hy_x;
+          const bool y0 = yface && j == 0;
+          if (y0) hx_y = wy0 ? 0.0f : hx;
+          Psi q2, q3, q4, q5;
+          if constexpr (AZ) q2 = psi_fetch<0>(p.et[2], ze2, k, j, X);
+          if constexpr (AX) q3 = psi_fetch<2>(p.et[3], cpml_slot(p.et[3], X), k, j, X);
+          if constexpr (AX) q4 = psi_fetch<2>(p.et[4], cpml_slot(p.et[4], X), k, j, X);
+          if constexpr (AY) q5 = psi_fetch<1>(p.et[5], cpml_slot(p.et[5], j), k, j, X);
+          const int o = k * PL + j * P + X;
+          const uint32_t id = p.em.site_ids[o];
+          {  // Ey: dHx/dz - dHz/dx
+            float d0 = div_rn(hx - hx_z, res, inv_res), d1 = div_rn(hz - hz_x, res, inv_res);
+            if constexpr (AZ) d0 = psi_apply(p.et[2], sm.cc[8], q2, d0, true);
+            if constexpr (AX) d1 = psi_apply(p.et[3], sm.cc[9], q3, d1, true);
+            const float e = E0y[b] + sm.coef[1][(id >> 8) & 0xffu] * (d0 - d1);
+            p.eout[1][o] = wx1 ? 0.0f : e;
+          }
+          {  // Ez: dHy/dx - dHx/dy
+            float d0 = div_rn(hy - hy_x, res, inv_res), d1 = div_rn(hx - hx_y, res, inv_res);
+            if constexpr (AX) d0 = psi_apply(p.et[4], sm.cc[10], q4, d0, true);
+            if constexpr (AY) d1 = psi_apply(p.et[5], sm.cc[11], q5, d1, true);
+            const float e = E0z[b] + sm.coef[2][(id >> 16) & 0xffu] * (d0 - d1);
+            p.eout[2][o] = (wx1 || (y0 && wy0)) ? 0.0f : e;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int ly = 1 + warp * R + r, lx = 1 + lane, b = ly * BX + lane + 4;
+          const int j = j0 + ly - 1;
           const float hx = sm.hn[hb][0][ly][lx], hy = sm.hn[hb][1][ly][lx], hz = sm.hn[hb][2][ly][lx];
-          const float cx = div_rn(hz - sm.hn[hb][2][ly - 1][lx], res, inv_res) -
-                           div_rn(hy - sm.hn[pb][1][ly][lx], res, inv_res);
-          const float cy = div_rn(hx - sm.hn[pb][0][ly][lx], res, inv_res) -
-                           div_rn(hz - sm.hn[hb][2][ly][lx - 1], res, inv_res);
-          const float cz = div_rn(hy - sm.hn[hb][1][ly][lx - 1], res, inv_res) -
-                           div_rn(hx - sm.hn[hb][0][ly - 1][lx], res, inv_res);
+          const float hy_z = sm.hn[pb][1][ly][lx], hx_z = sm.hn[pb][0][ly][lx];
+          float hz_x = sm.hn[hb][2][ly][lx - 1], hy_x = sm.hn[hb][1][ly][lx - 1];
+          float hz_y = sm.hn[hb][2][ly - 1][lx], hx_y = sm.hn[hb][0][ly - 1][lx];
+          const bool x0 = xface && i == 0, y0 = yface && j == 0;
+          if (x0) {  // ghost beyond x = 0: zero on a metallic wall, else the edge value
+            hz_x = wx0 ? 0.0f : hz;
+            hy_x = wx0 ? 0.0f : hy;
+          }
+          if (y0) {  // ghost beyond y = 0
+            hz_y = wy0 ? 0.0f : hz;
+            hx_y = wy0 ? 0.0f : hx;
+          }
+          Psi q0, q1, q2, q3, q4, q5;
+          if constexpr (AY) q0 = psi_fetch<1>(p.et[0], cpml_slot(p.et[0], j), k, j, i);
+          if constexpr (AZ) q1 = psi_fetch<0>(p.et[1], ze1, k, j, i);
+          if constexpr (AZ) q2 = psi_fetch<0>(p.et[2], ze2, k, j, i);
+          if constexpr (AX) q3 = psi_fetch<2>(p.et[3], cpml_slot(p.et[3], i), k, j, i);
+          if constexpr (AX) q4 = psi_fetch<2>(p.et[4], cpml_slot(p.et[4], i), k, j, i);
+          if constexpr (AY) q5 = psi_fetch<1>(p.et[5], cpml_slot(p.et[5], j), k, j, i);
           const uint32_t id = IDS[(ly - 1) * T::TX + lane];
-          const int o = k * PL + (j0 + ly - 1) * P + i;
-          p.eout[0][o] = E0x[b] + sm.coef[0][id & 0xffu] * cx;
-          p.eout[1][o] = E0y[b] + sm.coef[1][(id >> 8) & 0xffu] * cy;
-          p.eout[2][o] = E0z[b] + sm.coef[2][(id >> 16) & 0xffu] * cz;
+          const int o = k * PL + j * P + i;
+          {  // Ex: dHz/dy - dHy/dz
+            float d0 = div_rn(hz - hz_y, res, inv_res), d1 = div_rn(hy - hy_z, res, inv_res);
+            if constexpr (AY) d0 = psi_apply(p.et[0], sm.cc[6], q0, d0, true);
+            if constexpr (AZ) d1 = psi_apply(p.et[1], sm.cc[7], q1, d1, true);
+            const float e = E0x[b] + sm.coef[0][id & 0xffu] * (d0 - d1);
+            p.eout[0][o] = (y0 && wy0) ? 0.0f : e;
+          }
+          {  // Ey: dHx/dz - dHz/dx
+            float d0 = div_rn(hx - hx_z, res, inv_res), d1 = div_rn(hz - hz_x, res, inv_res);
+            if constexpr (AZ) d0 = psi_apply(p.et[2], sm.cc[8], q2, d0, true);
+            if constexpr (AX) d1 = psi_apply(p.et[3], sm.cc[9], q3, d1, true);
+            const float e = E0y[b] + sm.coef[1][(id >> 8) & 0xffu] * (d0 - d1);
+            p.eout[1][o] = (x0 && wx0) ? 0.0f : e;
+          }
+          {  // Ez: dHy/dx - dHx/dy
+            float d0 = div_rn(hy - hy_x, res, inv_res), d1 = div_rn(hx - hx_y, res, inv_res);
+            if constexpr (AX) d0 = psi_apply(p.et[4], sm.cc[10], q4, d0, true);
+            if constexpr (AY) d1 = psi_apply(p.et[5], sm.cc[11], q5, d1, true);
+            const float e = E0z[b] + sm.coef[2][(id >> 16) & 0xffu] * (d0 - d1);
+            p.eout[2][o] = ((x0 && wx0) || (y0 && wy0)) ? 0.0f : e;
+          }
+        }
+      };
+      if constexpr (!Cpml) {
+        body(kOff{}, kOff{}, kOff{});
+      } else {
+        const bool az = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
+        switch ((ax ? 4 : 0) | (ay ? 2 : 0) | (az ? 1 : 0)) {
+          case 0: body(kOff{}, kOff{}, kOff{}); break;
+          case 1: body(kOff{}, kOff{}, kOn{}); break;
+          case 2: body(kOff{}, kOn{}, kOff{}); break;
+          case 3: body(kOff{}, kOn{}, kOn{}); break;
+          case 4: body(kOn{}, kOff{}, kOff{}); break;
+          case 5: body(kOn{}, kOff{}, kOn{}); break;
+          case 6: body(kOn{}, kOn{}, kOff{}); break;
+          default: body(kOn{}, kOn{}, kOn{}); break;
         }
       }
     } else {
@@ -418,22 +607,21 @@ __global__ void __launch_bounds__(32 * NW, 1024 / (32 * NW))
       for (int r = 0; r < R; ++r) h_general(1 + warp * R + r, 1 + lane, emit, 7);
       if (warp == 0) h_general(0, 1 + lane, false, 1 | 4);
       if (warp == 1 && lane < T::TY) h_general(1 + lane, 0, false, 2 | 4);
+      if (xcol && warp == NW - 1 && lane <= T::TY) h_general(lane, T::TX + 1, emit && lane >= 1, 1);
       __syncthreads();
-      if (emit) {
+      // E of one cell at region (ly, lx) = lattice (k, j0-1+ly, i0-1+lx).
+      auto e_general = [&](int ly, int lx, bool from_box) {
+        const int j = j0 + ly - 1, i = i0 - 1 + lx, b = ly * BX + lx + 3;
+        if (j > Y || i > X) return;
         const bool zlo = k == 0, zhi = k == Z;
         const bool xlo = i == 0, xhi = i == X;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int ly = 1 + warp * R + r, lx = 1 + lane, b = ly * BX + lane + 4;
-          const int j = j0 + ly - 1;
-          if (j > Y || i > X) continue;
-          const int o = k * PL + j * P + i;
-          const bool ylo = j == 0, yhi = j == Y;
+        const int o = k * PL + j * P + i;
+        const bool ylo = j == 0, yhi = j == Y;
           const float hx = sm.hn[hb][0][ly][lx], hy = sm.hn[hb][1][ly][lx], hz = sm.hn[hb][2][ly][lx];
           const float hz_y = sm.hn[hb][2][ly - 1][lx], hz_x = sm.hn[hb][2][ly][lx - 1];
           const float hy_z = sm.hn[pb][1][ly][lx], hy_x = sm.hn[hb][1][ly][lx - 1];
           const float hx_z = sm.hn[pb][0][ly][lx], hx_y = sm.hn[hb][0][ly - 1][lx];
-          const uint32_t id = IDS[(ly - 1) * T::TX + lane];
+          const uint32_t id = from_box ? IDS[(ly - 1) * T::TX + lx - 1] : p.em.site_ids[o];
           if (i < X) {  // Ex: dHz/dy - dHy/dz
             CpmlOp c0, c1;
             if (cpml) {
@@ -470,7 +658,11 @@ __global__ void __launch_bounds__(32 * NW, 1024 / (32 * NW))
             if ((ylo && wy0) || (yhi && wy1) || (xlo && wx0) || (xhi && wx1)) e = 0.0f;
             p.eout[2][o] = e;
           }
-        }
+      };
+      if (emit) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) e_general(1 + warp * R + r, 1 + lane, true);
+        if (xcol && warp == NW - 1 && lane < T::TY) e_general(1 + lane, T::TX + 1, false);
       }
     }
     e0 = e1;
@@ -492,7 +684,9 @@ cudaError_t launch_tma_t(cudaStream_t s, const TmaMaps& maps, const Step3D& p) {
   }
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
-  const dim3 grid((p.X + 1 + T::TX - 1) / T::TX, (p.Y + 1 + T::TY - 1) / T::TY, (kmax + zc - 1) / zc);
+  // A multiple-of-32 X leaves column X to the last full tile (xcol).
+  const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;
+  const dim3 grid(gx, (p.Y + 1 + T::TY - 1) / T::TY, (kmax + zc - 1) / zc);
   Step3D q = p;
   q.z_chunk = zc;
   kern<<<grid, dim3(32, NW, 1), smem, s>>>(maps, q);

@@ -108,6 +108,7 @@ CASES_3D = [
     dict(grid=(12, 9, 40), metallic=("back", "right", "bottom"), pml_cells=4),
     dict(grid=(6, 8, 37), cpml_edges=(), metallic=("front", "back", "bottom", "top", "left", "right")),
     dict(grid=(10, 35, 9), cpml_edges=("left", "top", "back"), metallic=("right",)),
+    dict(grid=(9, 17, 64), metallic=("right", "bottom")),
 ]
 
 
@@ -136,6 +137,33 @@ def test_fused_tiles_and_z_chunks_are_bitwise_identical(tile, z_chunk):
     out = R.run_steps(R.initial_state(prog, fields=fields), prog, 6).numpy()
     for c in P.COMPONENTS:
         np.testing.assert_array_equal(out[c], ref[c], err_msg=c)
+    np.testing.assert_array_equal(out["dft_re"], ref["dft_re"])
+
+
+# Grids whose x extent is a multiple of the 32-wide tile: the last tile owns the
+# face column x = X; low faces take the straight path with per-lane ghosts.
+FACE_CASES = [
+    dict(grid=(9, 17, 64), metallic=("right", "front")),
+    dict(grid=(7, 24, 32), metallic=("left", "right", "bottom", "top"), pml_cells=5),
+    dict(grid=(13, 16, 96), cpml_edges=("right", "back", "bottom"), metallic=("left",)),
+    dict(grid=(6, 40, 64), cpml_edges=(), metallic=()),
+]
+
+
+@pytest.mark.parametrize("case", range(len(FACE_CASES)))
+@pytest.mark.parametrize("tile_y", [4, 8, 16])
+def test_fused_face_columns_are_bitwise_identical(case, tile_y):
+    spec = scenario_3d(seed=20 + case, nsteps=7, **FACE_CASES[case])
+    fields = random_initial_fields(spec, seed=30 + case)
+    ref_prog = R.compile_program(spec, schedule="phases")
+    ref = R.run_steps(R.initial_state(ref_prog, fields=fields), ref_prog, 7).numpy()
+    prog = R.compile_program(spec, schedule="fused", tile=(32, tile_y), z_chunk=4)
+    assert prog.layout == "pitched"
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, 7).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(out[c], ref[c], err_msg=c)
+    for a, b in zip(out["psi_h"] + out["psi_e"], ref["psi_h"] + ref["psi_e"]):
+        np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(out["dft_re"], ref["dft_re"])
 
 
