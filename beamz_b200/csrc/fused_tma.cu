@@ -264,8 +264,10 @@ struct HFast {
   }
 };
 
+// 8-warp, one-row CTAs are capped at 48 registers (5 resident CTAs, the
+// shared-memory limit too); the CPML body still fits without spills.
 template <int NW, int R, bool Cpml>
-__global__ void __launch_bounds__(32 * NW, 1024 / (32 * NW))
+__global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * NW))
     tma_step_kernel(const __grid_constant__ TmaMaps maps, Step3D p) {
   using T = TmaTile<NW, R>;
   using S = typename T::Smem;
