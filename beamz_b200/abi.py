@@ -39,6 +39,11 @@ EXPORTED_SYMBOLS = (
     "fdtd_apply_sources",
     "fdtd_accumulate_dft",
     "fdtd_copy_component",
+    "fdtd_adjoint_step",
+    "fdtd_adjoint_curl",
+    "fdtd_graph_create",
+    "fdtd_graph_launch",
+    "fdtd_graph_destroy",
     "fdtd_clear_graph_cache",
     "fdtd_error_string",
     "fdtd_registrations",
@@ -106,6 +111,21 @@ class FdtdDft(ctypes.Structure):
         ("re", FdtdBuffer),
         ("im", FdtdBuffer),
         ("weight_sum", FdtdBuffer),
+    ]
+
+
+class FdtdAdjointStep(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("step", ctypes.c_int32),
+        ("scratch_e", FdtdBuffer * 6),
+        ("scratch_h", FdtdBuffer * 6),
+        ("dft_grad_re", FdtdBuffer),
+        ("dft_grad_im", FdtdBuffer),
+        ("curl", FdtdBuffer * 3),
+        ("grad", FdtdBuffer * 3),
+        ("box_lo", ctypes.c_int32 * 3),
+        ("box_hi", ctypes.c_int32 * 3),
     ]
 
 
@@ -222,6 +242,16 @@ def load_library(path: str | None = None):
         lib.fdtd_copy_component.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdBuffer), ctypes.POINTER(FdtdBuffer),
                                             ctypes.POINTER(ctypes.c_int64)]
         lib.fdtd_copy_component.restype = ctypes.c_int
+        lib.fdtd_adjoint_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(FdtdAdjointStep)]
+        lib.fdtd_adjoint_step.restype = ctypes.c_int
+        lib.fdtd_adjoint_curl.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(FdtdAdjointStep)]
+        lib.fdtd_adjoint_curl.restype = ctypes.c_int
+        lib.fdtd_graph_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(ctypes.c_void_p)]
+        lib.fdtd_graph_create.restype = ctypes.c_int
+        lib.fdtd_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.fdtd_graph_launch.restype = ctypes.c_int
+        lib.fdtd_graph_destroy.argtypes = [ctypes.c_void_p]
+        lib.fdtd_graph_destroy.restype = ctypes.c_int
         lib.fdtd_clear_graph_cache.restype = None
         lib.fdtd_error_string.argtypes = [ctypes.c_int]
         lib.fdtd_error_string.restype = ctypes.c_char_p

@@ -100,6 +100,21 @@ struct DftDev;
 cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, int step_offset);
 cudaError_t launch_counter_advance(cudaStream_t s, int* counter, int nsteps);
 
+// Adjoint step buffers (see FdtdAdjointStep in fdtd_b200.h).
+struct AdjDev {
+  float* lam[6];           // adjoint fields, dense component shapes
+  float* scratch_e[6];     // per E term: lam_d at E sites
+  float* scratch_h[6];     // per H term: lam_d at H sites
+  const float* dft_grad_re;
+  const float* dft_grad_im;
+  float* curl[3];          // forward curl over the design box
+  float* grad[3];          // accumulated dJ/dc over the design box
+  int box_lo[3], box_hi[3];
+};
+cudaError_t launch_adjoint_step(cudaStream_t s, const Step3D& p, const DftDev* dft, const AdjDev& a, int active,
+                                int step);
+cudaError_t launch_adjoint_curl(cudaStream_t s, const Step3D& p, const AdjDev& a, int active);
+
 // DFT arena view (see FdtdDft in fdtd_b200.h).
 struct DftDev {
   int monitor_count;

@@ -474,6 +474,22 @@ cudaError_t launch_with_graph(cudaStream_t s, const FdtdProgram& p) {
   return cudaGraphLaunch(it->second, s);
 }
 
+// Capture one program into a caller-owned executable graph.
+cudaError_t capture_program(cudaStream_t s, const FdtdProgram& p, cudaGraphExec_t* out) {
+  cudaError_t err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return err;
+  const cudaError_t enq = enqueue_program(s, p);
+  cudaGraph_t graph = nullptr;
+  err = cudaStreamEndCapture(s, &graph);
+  if (enq != cudaSuccess || err != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return enq != cudaSuccess ? enq : err;
+  }
+  err = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  return err;
+}
+
 }  // namespace
 }  // namespace fdtd
 
@@ -548,6 +564,150 @@ int fdtd_copy_component(void* stream, const FdtdBuffer* src, const FdtdBuffer* d
                                               src->dims[2], src->dims[1] * src->dims[2],
                                               static_cast<float*>(dst->data), dst->dims[2],
                                               dst->dims[1] * dst->dims[2], extent[0], extent[1], extent[2]));
+}
+
+namespace fdtd {
+namespace {
+
+bool f32_sized(const FdtdBuffer& b, int64_t n) { return is_f32(b) && b.data != nullptr && elements(b) == n; }
+
+// Shared checks of an adjoint call: a valid dense phase program and a box
+// whose curl needs no ghost, wall or CPML handling.
+int check_adjoint(const FdtdProgram& p, const FdtdAdjointStep& a, const Layout& L, bool need_box) {
+  if (a.abi_version != FDTD_ABI_VERSION) return kInvalid;
+  if (p.layout != FDTD_LAYOUT_DENSE) return kInvalid;
+  const int64_t bz = a.box_hi[0] - a.box_lo[0], by = a.box_hi[1] - a.box_lo[1], bx = a.box_hi[2] - a.box_lo[2];
+  bool any_box = false;
+  for (int c = 0; c < 3; ++c) any_box = any_box || a.curl[c].data != nullptr || a.grad[c].data != nullptr;
+  if (!any_box) return need_box ? kInvalid : 0;
+  if (bz <= 0 || by <= 0 || bx <= 0) return kInvalid;
+  const int lo[3] = {a.box_lo[0], a.box_lo[1], a.box_lo[2]}, hi[3] = {a.box_hi[0], a.box_hi[1], a.box_hi[2]};
+  const int ext[3] = {L.Z, L.Y, L.X};
+  for (int c = 0; c < 3; ++c) {
+    if (!((L.active >> c) & 1)) {
+      if (a.curl[c].data != nullptr || a.grad[c].data != nullptr) return kInvalid;
+      continue;
+    }
+    if ((a.curl[c].data != nullptr && !f32_sized(a.curl[c], bz * by * bx)) ||
+        (a.grad[c].data != nullptr && !f32_sized(a.grad[c], bz * by * bx)))
+      return kInvalid;
+    if (a.grad[c].data != nullptr && a.curl[c].data == nullptr) return kInvalid;
+    // Axes the component is differentiated along need a lower neighbour and
+    // stay below the H extent; its own axis spans the E extent.
+    for (int ax = 0; ax < 3; ++ax) {
+      const bool derived = ax != 2 - c;
+      const int need_lo = derived ? 1 : 0;
+      const int need_hi = derived ? ext[ax] : ext[ax];
+      if (lo[ax] < need_lo || hi[ax] > need_hi) return kInvalid;
+    }
+    if (p.cpml) {
+      for (int t = 2 * c; t < 2 * c + 2; ++t) {
+        const int ax = kETermAxis[t];
+        for (int s = 0; s < (p.ndim == 3 ? 6 : 2); ++s) {
+          if (term_slot(p.ndim, p.polarization, false, s) != t) continue;
+          const FdtdCpmlTerm& term = p.e_terms[s];
+          const Dims d = component_dims(c, L.Z, L.Y, L.X);
+          const int n = ax == 0 ? d.z : (ax == 1 ? d.y : d.x);
+          if (lo[ax] < term.low || hi[ax] > n - term.high) return kInvalid;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+AdjDev adjoint_dev(const FdtdProgram& p, const FdtdAdjointStep& a) {
+  AdjDev d{};
+  for (int c = 0; c < 6; ++c) d.lam[c] = static_cast<float*>(p.fields[c].data);
+  for (int t = 0; t < 6; ++t) {
+    d.scratch_e[t] = static_cast<float*>(a.scratch_e[t].data);
+    d.scratch_h[t] = static_cast<float*>(a.scratch_h[t].data);
+  }
+  d.dft_grad_re = static_cast<const float*>(a.dft_grad_re.data);
+  d.dft_grad_im = static_cast<const float*>(a.dft_grad_im.data);
+  for (int c = 0; c < 3; ++c) {
+    d.curl[c] = static_cast<float*>(a.curl[c].data);
+    d.grad[c] = static_cast<float*>(a.grad[c].data);
+    d.box_lo[c] = a.box_lo[c];
+    d.box_hi[c] = a.box_hi[c];
+  }
+  return d;
+}
+
+}  // namespace
+}  // namespace fdtd
+
+int fdtd_adjoint_step(void* stream, const FdtdProgram* adjoint, const FdtdAdjointStep* a) {
+  if (adjoint == nullptr || a == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *adjoint;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  if (p.material_kind != FDTD_MATERIAL_SITE) return fdtd::kInvalid;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  const int b = fdtd::check_adjoint(p, *a, L, false);
+  if (b != 0) return b;
+  // Every derivative term between two active components needs its scratch.
+  for (int t = 0; t < 6; ++t) {
+    const int ec = fdtd::kETermComp[t], hsrc = (t == 0 || t == 3) ? 5 : ((t == 1 || t == 4) ? 4 : 3);
+    const bool e_live = ((L.active >> ec) & 1) && ((L.active >> hsrc) & 1);
+    if (e_live ? !fdtd::f32_sized(a->scratch_e[t], fdtd::dims_count(fdtd::component_dims(ec, L.Z, L.Y, L.X)))
+               : a->scratch_e[t].data != nullptr)
+      return fdtd::kInvalid;
+    const int hc = fdtd::kHTermComp[t], esrc = (t == 0 || t == 3) ? 2 : ((t == 1 || t == 4) ? 1 : 0);
+    const bool h_live = ((L.active >> hc) & 1) && ((L.active >> esrc) & 1);
+    if (h_live ? !fdtd::f32_sized(a->scratch_h[t], fdtd::dims_count(fdtd::component_dims(hc, L.Z, L.Y, L.X)))
+               : a->scratch_h[t].data != nullptr)
+      return fdtd::kInvalid;
+  }
+  const bool dft = p.dft.monitor_count > 0 && a->dft_grad_re.data != nullptr;
+  fdtd::DftDev dd{};
+  if (dft) {
+    dd = fdtd::make_dft(p, p.fields);
+    if (!fdtd::f32_sized(a->dft_grad_re, dd.arena_len) || !fdtd::f32_sized(a->dft_grad_im, dd.arena_len))
+      return fdtd::kInvalid;
+  }
+  const fdtd::Step3D sp = fdtd::make_step(p, L, 0, false, 0);
+  return static_cast<int>(fdtd::launch_adjoint_step(static_cast<cudaStream_t>(stream), sp, dft ? &dd : nullptr,
+                                                    fdtd::adjoint_dev(p, *a), L.active, a->step));
+}
+
+int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjointStep* a) {
+  if (forward == nullptr || a == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *forward;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  const int b = fdtd::check_adjoint(p, *a, L, true);
+  if (b != 0) return b;
+  const fdtd::Step3D sp = fdtd::make_step(p, L, 0, false, 0);
+  return static_cast<int>(
+      fdtd::launch_adjoint_curl(static_cast<cudaStream_t>(stream), sp, fdtd::adjoint_dev(p, *a), L.active));
+}
+
+int fdtd_graph_create(void* stream, const FdtdProgram* program, void** graph) {
+  if (program == nullptr || graph == nullptr || stream == nullptr || program->nsteps < 1) return fdtd::kInvalid;
+  *graph = nullptr;
+  const int v = fdtd::validate(*program);
+  if (v != 0) return v;
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t err = fdtd::capture_program(static_cast<cudaStream_t>(stream), *program, &exec);
+  if (err != cudaSuccess) return static_cast<int>(err);
+  *graph = static_cast<void*>(exec);
+  return 0;
+}
+
+int fdtd_graph_launch(void* stream, void* graph) {
+  if (graph == nullptr) return fdtd::kInvalid;
+  return static_cast<int>(cudaGraphLaunch(static_cast<cudaGraphExec_t>(graph), static_cast<cudaStream_t>(stream)));
+}
+
+int fdtd_graph_destroy(void* graph) {
+  if (graph == nullptr) return 0;
+  return static_cast<int>(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph)));
 }
 
 void fdtd_clear_graph_cache(void) {

@@ -221,6 +221,7 @@ class DeviceProgram:
             s.layout = abi.FDTD_LAYOUT_PITCHED
             s.pitch = self.pitch
         self._keep = []  # tensors referenced by the struct
+        self.e_source = {}  # per-site E source coefficients (site material), by component
 
         def buf(t):
             self._keep.append(t)
@@ -248,7 +249,8 @@ class DeviceProgram:
                 dec, src = spec.e_site[c]
                 i = COMPONENT_INDEX[c]
                 s.e_decay[i] = buf(_f32(dec, dev))
-                s.e_source[i] = buf(_f32(src, dev))
+                self.e_source[c] = _f32(src, dev)
+                s.e_source[i] = buf(self.e_source[c])
         for c, (dec, src) in spec.h_coefficients().items():
             if c not in self.active:
                 continue
@@ -428,9 +430,19 @@ class DeviceState:
         return out
 
 
-def compile_program(spec: ProgramSpec, device="cuda", **kwargs) -> DeviceProgram:
-    """Upload a program's static inputs (beamz/simulation/compile.py:796-895 analogue)."""
-    return DeviceProgram(spec, device=device, **kwargs)
+def compile_program(spec: ProgramSpec, device="cuda", tile=(32, 8), z_chunk=16, tune: bool = False,
+                    **kwargs) -> DeviceProgram:
+    """Upload a program's static inputs (beamz/simulation/compile.py:796-895 analogue).
+
+    ``tile="auto"`` / ``z_chunk="auto"`` take the 3D launch shape from the
+    per-shape autotuner (measuring it now when ``tune``)."""
+    if tile == "auto" or z_chunk == "auto":
+        from . import autotune
+
+        ty, zc = autotune.choose(spec, device=device, tune=tune)
+        tile = (32, ty) if tile == "auto" else tile
+        z_chunk = zc if z_chunk == "auto" else z_chunk
+    return DeviceProgram(spec, device=device, tile=tile, z_chunk=z_chunk, **kwargs)
 
 
 def initial_state(program: DeviceProgram, **kwargs) -> DeviceState:

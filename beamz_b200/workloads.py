@@ -40,40 +40,37 @@ def _dipole(component, site, eps_site, dt, total_steps, fwidth, offset, ndim=3):
     return P.SourcePlan(component, "pre_e", tuple(int(v) for v in site), coeff, wave)
 
 
-def _cpml_voxels(eps, pml_cells, dt, polarization="tm", explicit=False):
-    grid = eps.shape
-    h_terms, e_terms = P.plan_cpml(grid, dt, RES, pml_cells=pml_cells, polarization=polarization)
-    eps = P.extend_into_absorber(eps, P.absorber_edge_counts(grid, pml_cells, resolution=RES,
-                                                             explicit_thickness=explicit))
-    return eps, h_terms, e_terms
-
-
-def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, monitors=True, sources=True):
+def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, monitors=True, sources=True,
+                 n_monitors=4, n_freqs=5):
     nz, ny, nx = shape
     rng = np.random.default_rng(seed)
     dt = _dt(3, 0.99)
-    eps = np.full(shape, OXIDE, np.float32)
+    # Voxel ids: 0 = oxide, 1 = Si (the sorted codebook of the two permittivities).
+    ids = np.zeros(shape, np.uint8)
     z0 = nz // 2 - 5
     for _ in range(int(rng.integers(8, 17))):
         sy, sx = (int(v) for v in rng.integers(10, 101, size=2))
         y0 = int(rng.integers(0, max(1, ny - sy)))
         x0 = int(rng.integers(0, max(1, nx - sx)))
-        eps[z0:z0 + 11, y0:y0 + sy, x0:x0 + sx] = SI
-    eps, h_terms, e_terms = _cpml_voxels(eps, pml_cells, dt)
-    ids, table = P.voxel_codebook(eps)
+        ids[z0:z0 + 11, y0:y0 + sy, x0:x0 + sx] = 1
+    h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells)
+    ids = P.extend_into_absorber(ids, P.absorber_edge_counts(shape, pml_cells, resolution=RES))
+    table = np.ones(256, np.float32)
+    table[0], table[1] = OXIDE, SI
     srcs = []
     if sources:
         site = (nz // 2, ny // 2, nx // 2)
         # Ey site permittivity: mean of the voxels sharing the edge.
         k, j, i = site
-        e_site = 0.25 * (eps[k - 1, j, i - 1] + eps[k, j, i - 1] + eps[k - 1, j, i] + eps[k, j, i])
+        eps = table[ids[k - 1:k + 1, j, i - 1:i + 1]]
+        e_site = 0.25 * (eps[0, 0] + eps[1, 0] + eps[0, 1] + eps[1, 1])
         srcs.append(_dipole("Ey", site, float(e_site), dt, total_steps, 0.2 * F0, 0.5))
     mons = []
     if monitors:
         zc = (np.arange(pml_cells, nz - pml_cells) + 0.5) * RES
         yc = (np.arange(pml_cells, ny - pml_cells) + 0.5) * RES
-        freqs = np.linspace(0.9, 1.1, 5) * F0
-        for frac in (0.2, 0.4, 0.6, 0.8):
+        freqs = np.linspace(0.9, 1.1, n_freqs) * F0
+        for frac in (0.2, 0.4, 0.6, 0.8)[:n_monitors]:
             mons.append(P.plane_monitor(shape, RES, "x", frac * nx * RES, zc, yc, freqs,
                                         components=("Ey", "Ez", "Hy", "Hz")))
     return P.ProgramSpec(shape, dt, RES, voxel_ids=ids, eps_table=table, h_terms=h_terms, e_terms=e_terms,
@@ -134,6 +131,70 @@ def scene_2d_400(total_steps=2000, shape=(400, 400), pml_cells=20):
     mon = P.DftMonitorPlan(np.array([0.95, 1.0, 1.05], np.float32) * np.float32(F0), idx, w, mask)
     return P.ProgramSpec(shape, dt, RES, polarization="tm", e_site=e_site, h_terms=h_terms, e_terms=e_terms,
                          sources=[src], monitors=[mon], total_steps=total_steps)
+
+
+def _line_monitor(shape, x_col, ys, freqs):
+    """DFT line monitor along y at column x_col of a 2D TM grid (Ez, Hx, Hy)."""
+    idx, w = [], []
+    for c in P.COMPONENTS:
+        sh = P.component_shape(c, shape, "tm")
+        rows = np.minimum(ys, sh[0] - 1)
+        col = min(x_col, sh[1] - 1)
+        idx.append((rows * sh[1] + col).astype(np.int32)[:, None])
+        w.append(np.ones((ys.size, 1), np.float32))
+    mask = np.array([0, 0, 1, 1, 1, 0], np.float32)
+    return P.DftMonitorPlan(np.asarray(freqs, np.float32), idx, w, mask)
+
+
+def scene_2d(total_steps=2000, seed=0, shape=(512, 512), pml_cells=12, n_monitors=1, n_boxes=(2, 7)):
+    """2D TM request: oxide with seeded random Si boxes, a soft Ez point source
+    (Gaussian pulse at 1.55 um) and 1-4 x-normal DFT lines at 3 frequencies."""
+    ny, nx = shape
+    rng = np.random.default_rng(seed)
+    dt = _dt(2, 0.7)
+    eps = np.full(shape, OXIDE, np.float32)
+    for _ in range(int(rng.integers(*n_boxes))):
+        sy, sx = (int(v) for v in rng.integers(10, max(11, min(ny, nx) // 3), size=2))
+        y0 = int(rng.integers(0, max(1, ny - sy)))
+        x0 = int(rng.integers(0, max(1, nx - sx)))
+        eps[y0:y0 + sy, x0:x0 + sx] = SI
+    h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells, polarization="tm")
+    eps = P.extend_into_absorber(eps, P.absorber_edge_counts(shape, pml_cells, resolution=RES, explicit_thickness=True))
+    e_site = {"Ez": (np.float32(1.0), P.e_source_2d(P.site_values_2d(eps, "Ez", "tm"), dt))}
+    site = (ny // 2, nx // 4)
+    src = _dipole("Ez", site, float(eps[site]), dt, total_steps, 0.1 * F0, 0.5, ndim=2)
+    freqs = np.array([0.95, 1.0, 1.05], np.float32) * np.float32(F0)
+    ys = np.arange(pml_cells, ny - pml_cells)
+    mons = [_line_monitor(shape, int(frac * nx), ys, freqs) for frac in (0.6, 0.7, 0.8, 0.9)[:n_monitors]]
+    return P.ProgramSpec(shape, dt, RES, polarization="tm", e_site=e_site, h_terms=h_terms, e_terms=e_terms,
+                         sources=[src], monitors=mons, total_steps=total_steps)
+
+
+SERVING_3D_SHAPES = ((128, 128, 128), (192, 192, 192), (128, 256, 256))
+
+
+def serving_requests(n=256, rate=50.0, seed=0, steps=(500, 4000), sizes_2d=(256, 1024), shapes_3d=SERVING_3D_SHAPES,
+                     frac_3d=0.5):
+    """Seeded request stream: Poisson arrivals at `rate` per second, half 2D TM
+    grids (square, 256^2-1024^2 in steps of 32) and half 3D grids (128^3,
+    192^3, 256x256x128 in x, y, z), uniform step counts, 1-4 DFT monitors and
+    seeded random Si/oxide boxes.  Returns ``[(arrival_s, spec), ...]``."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for r in range(n):
+        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        nsteps = int(rng.integers(steps[0], steps[1] + 1))
+        nmon = int(rng.integers(1, 5))
+        sub = int(rng.integers(0, 2**31 - 1))
+        if rng.random() < frac_3d:
+            shape = tuple(shapes_3d[int(rng.integers(0, len(shapes_3d)))])
+            spec = scene_3d_512(total_steps=nsteps, seed=sub, shape=shape, n_monitors=nmon, n_freqs=3)
+        else:
+            side = int(rng.integers(sizes_2d[0] // 32, sizes_2d[1] // 32 + 1)) * 32
+            spec = scene_2d(total_steps=nsteps, seed=sub, shape=(side, side), n_monitors=nmon)
+        out.append((t, spec))
+    return out
 
 
 SCENES = {"3d_512": scene_3d_512, "capacity": scene_capacity, "2d_400": scene_2d_400}

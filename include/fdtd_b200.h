@@ -236,6 +236,52 @@ int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_o
  * pitched field layouts).  No beamz counterpart: beamz keeps one layout. */
 int fdtd_copy_component(void* stream, const FdtdBuffer* src, const FdtdBuffer* dst, const int64_t* extent);
 
+/* Capture program->nsteps complete steps, exactly as fdtd_launch_program
+ * enqueues them, into a CUDA graph owned by the caller; *graph receives the
+ * executable graph.  The graph holds every pointer of `program`: each replay
+ * advances that same state by nsteps steps (the step counter and clock live on
+ * the device).  `stream` must be a created stream (capture source).
+ * No beamz counterpart: beamz keeps graphs only in its process-global cache
+ * (cuda/src/graph.cu:84-154); a serving loop that keeps many simulations
+ * resident owns one graph per simulation instead. */
+int fdtd_graph_create(void* stream, const FdtdProgram* program, void** graph);
+
+/* Replay a graph from fdtd_graph_create on `stream`. */
+int fdtd_graph_launch(void* stream, void* graph);
+
+/* Release a graph from fdtd_graph_create (null is a no-op). */
+int fdtd_graph_destroy(void* graph);
+
+/* One adjoint (time-reversed, transposed) step.  No beamz counterpart: beamz
+ * differentiates its JAX path with JAX; this is the hand-written discrete
+ * adjoint of the step fdtd_launch_program runs (dense layout, per-site E
+ * material, phase schedule).  The FdtdProgram passed with it is the ADJOINT
+ * program: the forward program's coefficients, CPML terms, walls and
+ * monitors, with `fields` holding the adjoint fields and each term's `psi`
+ * the adjoint memory. */
+typedef struct FdtdAdjointStep {
+  int32_t abi_version;
+  int32_t step;              /* absolute step n whose transpose is applied */
+  FdtdBuffer scratch_e[6];   /* F32, per E term: that E component's shape */
+  FdtdBuffer scratch_h[6];   /* F32, per H term: that H component's shape */
+  FdtdBuffer dft_grad_re;    /* F32 [arena], optional: dJ/d(dft re) */
+  FdtdBuffer dft_grad_im;    /* F32 [arena], optional: dJ/d(dft im) */
+  FdtdBuffer curl[3];        /* F32 [box], optional: forward curl of Ex/Ey/Ez over the box */
+  FdtdBuffer grad[3];        /* F32 [box], optional: accumulated dJ/dc of Ex/Ey/Ez */
+  int32_t box_lo[3];         /* design box of E sites (z, y, x), interior and */
+  int32_t box_hi[3];         /* clear of every absorber slab */
+} FdtdAdjointStep;
+
+/* Apply the transpose of step `a->step` to the adjoint state in `adjoint`:
+ * the DFT adjoint source of that step's sample (when dft_grad_* are given),
+ * the E update's transpose with gradient accumulation grad += mu * curl over
+ * the box (when grad/curl are given), then the H update's transpose. */
+int fdtd_adjoint_step(void* stream, const FdtdProgram* adjoint, const FdtdAdjointStep* a);
+
+/* Write the forward curl of each active E component over `a`'s box into
+ * a->curl from `forward`'s current H fields (call after a forward step). */
+int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjointStep* a);
+
 /* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
 void fdtd_clear_graph_cache(void);
 
