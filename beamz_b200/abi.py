@@ -25,6 +25,7 @@ FDTD_LAYOUT_DENSE, FDTD_LAYOUT_PITCHED = 0, 1
 FDTD_TIMING_PRE_E, FDTD_TIMING_H, FDTD_TIMING_E = 0, 1, 2
 FDTD_MAX_SOURCES = 16
 FDTD_MAX_MONITORS = 16
+FDTD_ADJOINT_NOALLOC_MAX_FLOATS = 4 * 1024 * 1024
 TIMINGS = {"pre_e": FDTD_TIMING_PRE_E, "h": FDTD_TIMING_H, "e": FDTD_TIMING_E}
 # Wall bits (front, back, bottom, top, left, right), beamz/simulation/cuda/runtime.py:38-40.
 EDGE_BITS = {"front": 0, "back": 1, "bottom": 2, "top": 3, "left": 4, "right": 5}
@@ -41,6 +42,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_copy_component",
     "fdtd_adjoint_step",
     "fdtd_adjoint_curl",
+    "fdtd_adjoint_step_noalloc",
     "fdtd_graph_create",
     "fdtd_graph_launch",
     "fdtd_graph_destroy",
@@ -246,6 +248,9 @@ def load_library(path: str | None = None):
         lib.fdtd_adjoint_step.restype = ctypes.c_int
         lib.fdtd_adjoint_curl.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(FdtdAdjointStep)]
         lib.fdtd_adjoint_curl.restype = ctypes.c_int
+        lib.fdtd_adjoint_step_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram),
+                                                  ctypes.POINTER(FdtdAdjointStep)]
+        lib.fdtd_adjoint_step_noalloc.restype = ctypes.c_int
         lib.fdtd_graph_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(ctypes.c_void_p)]
         lib.fdtd_graph_create.restype = ctypes.c_int
         lib.fdtd_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]

@@ -28,6 +28,8 @@
 // mu * curl'_n per E site over a design box, mu = the masked E adjoint and
 // curl'_n the forward curl recomputed from a checkpoint.
 
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace fdtd {
@@ -303,6 +305,60 @@ cudaError_t launch_adjoint_step(cudaStream_t s, const Step3D& p, const DftDev* d
     adj_egather_kernel<<<blocks_for(static_cast<int64_t>(d.z) * d.y * d.x), kAdjThreads, 0, s>>>(p, a, e);
   }
   return cudaPeekAtLastError();
+}
+
+// ---- adjoint step without caller scratch -----------------------------------
+// The per-term scratch of fdtd_adjoint_step_noalloc lives in this one
+// file-scope device array (FDTD_ADJOINT_NOALLOC_MAX_FLOATS floats, 16 MiB),
+// so that entry point allocates no device memory.  Every call shares it:
+// calls that overlap on the GPU race.  Nothing in it needs clearing: each
+// call writes every scratch element it reads before reading it.
+static __device__ __align__(256) float g_adjoint_scratch[FDTD_ADJOINT_NOALLOC_MAX_FLOATS];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+// Device address of g_adjoint_scratch on the current device, looked up once
+// per device with that device current.
+cudaError_t adjoint_scratch_address(float** out) {
+  static std::mutex mu;
+  static float* addr[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_adjoint_scratch);
+    if (err != cudaSuccess) return err;
+    addr[dev] = static_cast<float*>(p);
+  }
+  *out = addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+int64_t adjoint_noalloc_span(int64_t floats) { return (floats + 63) / 64 * 64; }
+
+cudaError_t launch_adjoint_step_noalloc(cudaStream_t s, const Step3D& p, const DftDev* dft, AdjDev a, int active,
+                                        int step, const int64_t e_len[6], const int64_t h_len[6]) {
+  float* base = nullptr;
+  const cudaError_t err = adjoint_scratch_address(&base);
+  if (err != cudaSuccess) return err;
+  int64_t off = 0;
+  for (int t = 0; t < 6; ++t) {
+    a.scratch_e[t] = e_len[t] > 0 ? base + off : nullptr;
+    off += e_len[t] > 0 ? adjoint_noalloc_span(e_len[t]) : 0;
+  }
+  for (int t = 0; t < 6; ++t) {
+    a.scratch_h[t] = h_len[t] > 0 ? base + off : nullptr;
+    off += h_len[t] > 0 ? adjoint_noalloc_span(h_len[t]) : 0;
+  }
+  if (off > FDTD_ADJOINT_NOALLOC_MAX_FLOATS) return cudaErrorInvalidValue;
+  return launch_adjoint_step(s, p, dft, a, active, step);
 }
 
 cudaError_t launch_adjoint_curl(cudaStream_t s, const Step3D& p, const AdjDev& a, int active) {

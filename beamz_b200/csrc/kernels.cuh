@@ -114,6 +114,9 @@ struct AdjDev {
 cudaError_t launch_adjoint_step(cudaStream_t s, const Step3D& p, const DftDev* dft, const AdjDev& a, int active,
                                 int step);
 cudaError_t launch_adjoint_curl(cudaStream_t s, const Step3D& p, const AdjDev& a, int active);
+int64_t adjoint_noalloc_span(int64_t floats);
+cudaError_t launch_adjoint_step_noalloc(cudaStream_t s, const Step3D& p, const DftDev* dft, AdjDev a, int active,
+                                        int step, const int64_t e_len[6], const int64_t h_len[6]);
 
 // DFT arena view (see FdtdDft in fdtd_b200.h).
 struct DftDev {

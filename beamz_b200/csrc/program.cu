@@ -673,6 +673,42 @@ int fdtd_adjoint_step(void* stream, const FdtdProgram* adjoint, const FdtdAdjoin
                                                     fdtd::adjoint_dev(p, *a), L.active, a->step));
 }
 
+int fdtd_adjoint_step_noalloc(void* stream, const FdtdProgram* adjoint, const FdtdAdjointStep* a) {
+  if (adjoint == nullptr || a == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *adjoint;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  if (p.material_kind != FDTD_MATERIAL_SITE) return fdtd::kInvalid;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  const int b = fdtd::check_adjoint(p, *a, L, false);
+  if (b != 0) return b;
+  int64_t e_len[6] = {}, h_len[6] = {}, total = 0;
+  for (int t = 0; t < 6; ++t) {
+    if (a->scratch_e[t].data != nullptr || a->scratch_h[t].data != nullptr) return fdtd::kInvalid;
+    const int ec = fdtd::kETermComp[t], hsrc = (t == 0 || t == 3) ? 5 : ((t == 1 || t == 4) ? 4 : 3);
+    if (((L.active >> ec) & 1) && ((L.active >> hsrc) & 1))
+      e_len[t] = fdtd::dims_count(fdtd::component_dims(ec, L.Z, L.Y, L.X));
+    const int hc = fdtd::kHTermComp[t], esrc = (t == 0 || t == 3) ? 2 : ((t == 1 || t == 4) ? 1 : 0);
+    if (((L.active >> hc) & 1) && ((L.active >> esrc) & 1))
+      h_len[t] = fdtd::dims_count(fdtd::component_dims(hc, L.Z, L.Y, L.X));
+    total += fdtd::adjoint_noalloc_span(e_len[t]) + fdtd::adjoint_noalloc_span(h_len[t]);
+  }
+  if (total > FDTD_ADJOINT_NOALLOC_MAX_FLOATS) return fdtd::kInvalid;
+  const bool dft = p.dft.monitor_count > 0 && a->dft_grad_re.data != nullptr;
+  fdtd::DftDev dd{};
+  if (dft) {
+    dd = fdtd::make_dft(p, p.fields);
+    if (!fdtd::f32_sized(a->dft_grad_re, dd.arena_len) || !fdtd::f32_sized(a->dft_grad_im, dd.arena_len))
+      return fdtd::kInvalid;
+  }
+  const fdtd::Step3D sp = fdtd::make_step(p, L, 0, false, 0);
+  return static_cast<int>(fdtd::launch_adjoint_step_noalloc(static_cast<cudaStream_t>(stream), sp,
+                                                            dft ? &dd : nullptr, fdtd::adjoint_dev(p, *a), L.active,
+                                                            a->step, e_len, h_len));
+}
+
 int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjointStep* a) {
   if (forward == nullptr || a == nullptr) return fdtd::kInvalid;
   FdtdProgram p = *forward;

@@ -278,6 +278,26 @@ typedef struct FdtdAdjointStep {
  * the box (when grad/curl are given), then the H update's transpose. */
 int fdtd_adjoint_step(void* stream, const FdtdProgram* adjoint, const FdtdAdjointStep* a);
 
+/* Floats in the device scratch array of fdtd_adjoint_step_noalloc (16 MiB). */
+#define FDTD_ADJOINT_NOALLOC_MAX_FLOATS (4 * 1024 * 1024)
+
+/* fdtd_adjoint_step without caller scratch: the per-term scratch arrays are
+ * carved from one device array of FDTD_ADJOINT_NOALLOC_MAX_FLOATS floats
+ * inside this library, so the call allocates no device memory.  It is for
+ * callers that cannot allocate device memory where they step the adjoint: a
+ * host program that links only this C library and owns no device allocator
+ * for temporaries, or one held to a fixed device-memory budget.
+ * No counterpart in the reference (beamz differentiates through JAX).
+ * a->scratch_e and a->scratch_h must be empty.  A program whose live
+ * derivative terms need more scratch than the maximum (each term's array
+ * rounded up to 64 floats; 2D TM up to about 1000 x 1000, 3D up to about
+ * 330 000 lattice points) is rejected with cudaErrorInvalidValue (1) before
+ * any work is enqueued.  Every call shares the one array: calls that overlap
+ * on the GPU (two streams, or two host threads) race and corrupt each
+ * other's results, so serialize them.  Nothing in it needs to start at
+ * zero: each call writes every scratch element it reads first. */
+int fdtd_adjoint_step_noalloc(void* stream, const FdtdProgram* adjoint, const FdtdAdjointStep* a);
+
 /* Write the forward curl of each active E component over `a`'s box into
  * a->curl from `forward`'s current H fields (call after a forward step). */
 int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjointStep* a);
