@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel-steps", type=int, default=200)
     ap.add_argument("--shape", default=None, help="override the scene grid as ZxYxX (profiling runs)")
+    ap.add_argument("--serving", action="store_true", help="config 4: batched serving vs one-at-a-time")
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--adjoint", choices=["2d", "3d"], default=None, help="config 5: forward + adjoint gradient")
     return ap.parse_args()
 
 
@@ -162,6 +166,135 @@ def reference_arm(args, scene_fn, cells_full):
     print(json.dumps(line), flush=True)
 
 
+def serving_arm(args, rank, world):
+    """Config 4: a seeded Poisson stream through the serving engine, then the
+    same requests one at a time through the plain path (rank-local shards)."""
+    import torch
+
+    from beamz_b200 import serve
+    from beamz_b200 import workloads as W
+
+    stream = W.serving_requests(args.requests, rate=args.rate, seed=2024)
+    mine = [(a, s) for i, (a, s) in enumerate(stream) if i % world == rank]
+    reqs = [serve.Request(i, s, s.total_steps, a) for i, (a, s) in enumerate(mine)]
+    warm = [serve.Request(0, W.scene_2d(total_steps=16, shape=(64, 64)), 16, 0.0),
+            serve.Request(1, W.scene_3d_512(total_steps=16, shape=(32, 32, 32), pml_cells=4, n_monitors=1, n_freqs=3),
+                          16, 0.0)]
+    serve.run_sequential(warm)
+    serve.ServingEngine().run(warm)
+    engine = serve.ServingEngine()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        batched = engine.run(reqs)
+        sequential = serve.run_sequential(reqs)
+    b, q = serve.summarize(batched), serve.summarize(sequential)
+    same = all(np.array_equal(x.dft_re, y.dft_re) and np.array_equal(x.dft_im, y.dft_im)
+               for x, y in zip(batched, sequential))
+    line = {"metric": "sims/s (batched serving)", "value": round(b.sims_per_s, 3), "unit": "simulations/s",
+            "n_gpus": world, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+            "data": "synthetic (seeded request stream)",
+            "config": {"workload": "serving: Poisson arrivals, 2D 256^2-1024^2 and 3D 128^3/192^3/256x256x128, "
+                                   "500-4000 steps, 1-4 DFT monitors", "requests": len(reqs), "rate_per_s": args.rate},
+            "batched": {"sims_per_s": round(b.sims_per_s, 3), "p50_s": round(b.p50_s, 3), "p99_s": round(b.p99_s, 3),
+                        "makespan_s": round(b.makespan_s, 2), "peak_resident": engine.peak_active,
+                        "peak_gb": round(engine.peak_bytes / 1e9, 2)},
+            "sequential": {"sims_per_s": round(q.sims_per_s, 3), "p50_s": round(q.p50_s, 3),
+                           "p99_s": round(q.p99_s, 3), "makespan_s": round(q.makespan_s, 2)},
+            "speedup": round(b.sims_per_s / q.sims_per_s, 3), "results_identical": same,
+            "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def adjoint_arm(args):
+    """Config 5: forward with checkpoints every 100 steps plus the adjoint
+    gradient of a port-overlap objective w.r.t. a design density."""
+    import torch
+
+    from beamz_b200 import adjoint as A
+    from beamz_b200 import plan as P
+    from beamz_b200 import workloads as W
+
+    gen = torch.Generator(device="cpu").manual_seed(5)
+    out = {}
+    if args.adjoint == "2d":
+        ny = nx = 600
+        nsteps = 3000
+        spec = W.scene_2d(total_steps=nsteps, seed=5, shape=(ny, nx), pml_cells=20, n_monitors=1)
+        y0, x0 = 200, 200
+        box = ((y0, x0), (y0 + 200, x0 + 200))
+        problem = A.AdjointProblem(spec, nsteps, box, checkpoint_every=100)
+        raw = torch.rand((1, 1, 200, 200), generator=gen)
+        k = torch.exp(-0.5 * (torch.arange(-9, 10, dtype=torch.float32) / 3.0) ** 2)
+        k = (k / k.sum())
+        blur = torch.nn.functional.conv2d(torch.nn.functional.conv2d(raw, k.view(1, 1, 1, -1), padding=(0, 9)),
+                                          k.view(1, 1, -1, 1), padding=(9, 0))[0, 0]
+        rho = blur.cuda().requires_grad_(True)
+        eps_bg = torch.full((ny, nx), W.OXIDE, device="cuda")
+        mon = spec.monitors[0]
+        npts = np.asarray(mon.indices[0]).shape[0]
+        nf = len(mon.freqs)
+        prof = torch.exp(-0.5 * ((torch.arange(npts, dtype=torch.float32) - npts / 2) / (npts / 10)) ** 2).cuda()
+        ez = P.COMPONENT_INDEX["Ez"]
+
+        def objective(r):
+            eps = eps_bg.clone()
+            eps[y0:y0 + 200, x0:x0 + 200] = W.OXIDE + r * (W.SI - W.OXIDE)
+            re, im = A.simulate(problem, [A.eps_to_coefficients_2d(eps, spec.dt, P.EPS_0)])
+            sl = slice((ez * nf + nf // 2) * npts, (ez * nf + nf // 2 + 1) * npts)
+            return (prof * re[sl]).sum() ** 2 + (prof * im[sl]).sum() ** 2
+
+        designs = [rho]
+        cells = ny * nx
+        workload = "2D TM 600x600, 200x200 design, 3000 steps, checkpoints every 100"
+    else:
+        shape = (128, 256, 256)
+        nsteps = 1500
+        spec = W.scene_3d_512(total_steps=nsteps, seed=6, shape=shape, n_monitors=1, n_freqs=3)
+        base = torch.as_tensor(spec.eps_table[spec.voxel_ids], device="cuda")
+        coefs0 = A.eps_to_coefficients_3d(base, spec.dt, P.EPS_0)
+        sspec = A.site_spec(spec, {c: v.cpu().numpy() for c, v in zip(("Ex", "Ey", "Ez"), coefs0)})
+        z0 = shape[0] // 2 - 5
+        box = ((z0, 96, 96), (z0 + 12, 160, 160))
+        problem = A.AdjointProblem(sspec, nsteps, box, checkpoint_every=100)
+        mon = spec.monitors[0]
+        npts = max(np.asarray(ix).shape[0] for ix in mon.indices)
+        nf = len(mon.freqs)
+        w = torch.randn(npts, generator=gen).cuda()
+        ey = P.COMPONENT_INDEX["Ey"]
+
+        def objective(r):
+            eps = base.clone()
+            eps[z0 + 1:z0 + 11, 97:159, 97:159] = W.OXIDE + r * (W.SI - W.OXIDE)
+            re, im = A.simulate(problem, A.eps_to_coefficients_3d(eps, spec.dt, P.EPS_0))
+            sl = slice((ey * nf + nf // 2) * npts, (ey * nf + nf // 2 + 1) * npts)
+            return (w * re[sl]).sum() ** 2 + (w * im[sl]).sum() ** 2
+
+        designs = [torch.rand((10, 62, 62), generator=gen).cuda().requires_grad_(True) for _ in range(8)]
+        cells = int(np.prod(shape))
+        workload = "3D 256x256x128, batch of 8 designs (10x62x62), 1500 steps, checkpoints every 100"
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fwd = bwd = 0.0
+    for r in designs:
+        a = time.perf_counter()
+        val = objective(r)
+        torch.cuda.synchronize()
+        b = time.perf_counter()
+        val.backward()
+        torch.cuda.synchronize()
+        fwd += b - a
+        bwd += time.perf_counter() - b
+    total = time.perf_counter() - t0
+    out = {"metric": "adjoint gradient time", "value": round(total / len(designs), 3), "unit": "s per design",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded density)",
+           "config": {"workload": workload, "designs": len(designs)},
+           "forward_s": round(fwd / len(designs), 3), "backward_s": round(bwd / len(designs), 3),
+           "forward_gcups": round(cells * nsteps / (fwd / len(designs)) / 1e9, 2),
+           "peak_hbm_gb": round(torch.cuda.max_memory_allocated() / 1e9, 2),
+           "grad_norm": float(designs[0].grad.norm())}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     import torch
@@ -172,6 +305,22 @@ def main():
     from beamz_b200 import workloads as W
 
     scene_fn = W.SCENES[args.scene]
+    if args.adjoint:
+        if rank == 0:
+            adjoint_arm(args)
+        return
+    if args.serving and args.impl == "b200":
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", init_method="env://",
+                                    timeout=__import__("datetime").timedelta(seconds=600))
+            torch.cuda.set_device(local)
+        serving_arm(args, rank, world)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         if rank == 0:
             reference_arm(args, W.scene_3d_512, 512 * 512 * 256)
@@ -230,10 +379,13 @@ def main():
     launches = per_step * args.steps + -(-args.steps // R.GRAPH_CHUNK_STEPS)
 
     # ---- dominant kernel alone: the fused step without sources or monitors ---
-    kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw) \
-        if args.scene == "3d_512" else spec
-    kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
-    kstate = R.initial_state(kprog)
+    if args.scene == "3d_512":
+        kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw)
+        kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
+        kstate = R.initial_state(kprog)
+    else:  # other scenes time their own step (a second copy would not fit config 3)
+        kprog, kstate = prog, state
+        kprog._times_for(kstate.step + 3 * args.kernel_steps + 3)
     R.run_steps(kstate, kprog, 3)
     prime(kstate, kprog, args.kernel_steps)
     torch.cuda.synchronize(dev)
@@ -243,6 +395,7 @@ def main():
     k1.record(stream)
     torch.cuda.synchronize(dev)
     kernel_ms = k0.elapsed_time(k1) / args.kernel_steps
+    peak_hbm = torch.cuda.max_memory_allocated(dev)
     del kstate, kprog
     alg_bytes = W.algorithmic_bytes(spec)
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
@@ -321,6 +474,7 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": "tma_step_kernel" if prog.layout == "pitched" else "fused step", "kernel_ms": round(kernel_ms, 4),
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
+            "peak_hbm_gb": round(peak_hbm / 1e9, 2),
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "e2e": e2e,
