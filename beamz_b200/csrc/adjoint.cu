@@ -232,11 +232,12 @@ __global__ void __launch_bounds__(kAdjThreads) adj_dft_kernel(DftDev d, AdjDev a
   }
   g *= s_scale * mask;
   if (g == 0.0f) return;
-  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * d.max_points + pidx) * d.neighbors;
+  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * d.neighbors) * d.max_points + pidx;
   for (int nb = 0; nb < d.neighbors; ++nb) {
-    const float w = d.weights[base + nb];
-    const int idx = d.indices[base + nb];
-    if (w != 0.0f && idx >= 0 && idx < d.field_len[c]) atomicAdd(a.lam[c] + idx, w * g);
+    const float w = d.weights[base + static_cast<int64_t>(nb) * d.max_points];
+    if (w == 0.0f) break;
+    const int idx = d.indices[base + static_cast<int64_t>(nb) * d.max_points];
+    if (idx >= 0 && idx < d.field_len[c]) atomicAdd(a.lam[c] + idx, w * g);
   }
 }
 

@@ -97,14 +97,18 @@ __global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* c
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np || mask == 0.0f) return;
   if (voff < 0 || voff + static_cast<int64_t>(6) * nf * np > d.arena_len) return;
+  // Neighbour-major plan: consecutive points of one neighbour slot are
+  // contiguous; per point the nonzero weights come first, so the gather stops
+  // at the first zero (the same sum, in the same order, as skipping zeros).
   const int K = d.neighbors;
-  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * d.max_points + p) * K;
+  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * K) * d.max_points + p;
   const float* field = d.fields[c];
   float v = 0.0f;
   for (int n = 0; n < K; ++n) {
-    const float w = d.weights[base + n];
-    const int idx = d.indices[base + n];
-    if (w != 0.0f && idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
+    const float w = d.weights[base + static_cast<int64_t>(n) * d.max_points];
+    if (w == 0.0f) break;
+    const int idx = d.indices[base + static_cast<int64_t>(n) * d.max_points];
+    if (idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
   }
   const float sm = s_scale * mask;
   const int64_t out = voff + (static_cast<int64_t>(c) * nf) * np + p;

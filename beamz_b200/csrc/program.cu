@@ -343,8 +343,8 @@ DftDev make_dft(const FdtdProgram& p, const FdtdBuffer* bank_fields) {
   const FdtdDft& m = p.dft;
   d.monitor_count = m.monitor_count;
   if (m.monitor_count == 0) return d;
-  d.max_points = static_cast<int>(m.indices.dims[2]);
-  d.neighbors = static_cast<int>(m.indices.dims[3]);
+  d.max_points = static_cast<int>(m.indices.dims[3]);
+  d.neighbors = static_cast<int>(m.indices.dims[2]);
   d.max_freqs = static_cast<int>(m.freqs.dims[1]);
   d.indices = static_cast<const int*>(m.indices.data);
   d.weights = static_cast<const float*>(m.weights.data);

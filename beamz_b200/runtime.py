@@ -115,6 +115,13 @@ class DftArena:
     layout: list  # per monitor: (value_offset, freq_count, point_count, weight_offset)
 
 
+def nonzero_first(indices: np.ndarray, weights: np.ndarray):
+    """Per point (row), move the nonzero-weight neighbours to the front,
+    keeping their order, so a gather may stop at the first zero weight."""
+    order = np.argsort(weights == 0.0, axis=1, kind="stable")
+    return np.take_along_axis(indices, order, axis=1), np.take_along_axis(weights, order, axis=1)
+
+
 def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
     """Pad every monitor to a common (P, K, F) and lay out the ragged arena.
 
@@ -128,8 +135,8 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
     F = max(len(m.freqs) for m in monitors)
     if F > 64:
         raise ValueError("at most 64 frequencies per monitor")
-    indices = np.zeros((M, 6, P, K), np.int32)
-    weights = np.zeros((M, 6, P, K), np.float32)
+    indices = np.zeros((M, 6, K, P), np.int32)  # neighbour-major (see FdtdDft)
+    weights = np.zeros((M, 6, K, P), np.float32)
     freqs = np.zeros((M, F), np.float32)
     masks = np.zeros((M, 6), np.float32)
     counts = np.zeros((M, 5), np.int32)
@@ -143,8 +150,9 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
             ic, wc = mon.indices[c], mon.weights[c]
             if remap is not None:
                 ic = remap(c, ic)
-            indices[m, c, :p, : ic.shape[1]] = ic
-            weights[m, c, :p, : wc.shape[1]] = wc
+            ic, wc = nonzero_first(np.asarray(ic), np.asarray(wc, np.float32))
+            indices[m, c, : ic.shape[1], :p] = ic.T
+            weights[m, c, : wc.shape[1], :p] = wc.T
         freqs[m, :nf] = mon.freqs
         masks[m] = mon.component_mask
         counts[m] = (nf, p, max(1, int(mon.interval)), voff, woff)

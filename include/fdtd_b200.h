@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 3
+#define FDTD_ABI_VERSION 4
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
 enum {
@@ -122,8 +122,9 @@ typedef struct FdtdSource {
 } FdtdSource;
 
 /* Vector-DFT monitor arena (beamz: cuda/src/launch.h:47-61, observe.py:529-585).
- *  indices  S32 [M, 6, P, K]  flat offsets into each component
- *  weights  F32 [M, 6, P, K]
+ *  indices  S32 [M, 6, K, P]  flat offsets into each component, neighbour-major
+ *  weights  F32 [M, 6, K, P]  (per point, the nonzero weights come first: a
+ *                             zero weight ends that point's gather)
  *  freqs    F32 [M, F]
  *  masks    F32 [M, 6]
  *  counts   S32 [M, 5]: freq_count, point_count, interval, value_offset, weight_offset

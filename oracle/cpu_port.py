@@ -135,8 +135,8 @@ class HostRun:
             M, P = len(mons), max(m.points for m in mons)
             K = max(max(a.shape[1] for a in m.indices) for m in mons)
             F = max(len(m.freqs) for m in mons)
-            idx = np.zeros((M, 6, P, K), np.int32)
-            w = np.zeros((M, 6, P, K), f32)
+            idx = np.zeros((M, 6, K, P), np.int32)  # neighbour-major, as the ABI lays it out
+            w = np.zeros((M, 6, K, P), f32)
             fr = np.zeros((M, F), f32)
             masks = np.zeros((M, 6), f32)
             counts = np.zeros((M, 5), np.int32)
@@ -146,8 +146,8 @@ class HostRun:
             for mi, mon in enumerate(mons):
                 p, nf = mon.points, len(mon.freqs)
                 for c in range(6):
-                    idx[mi, c, :p, : mon.indices[c].shape[1]] = mon.indices[c]
-                    w[mi, c, :p, : mon.weights[c].shape[1]] = mon.weights[c]
+                    idx[mi, c, : mon.indices[c].shape[1], :p] = np.asarray(mon.indices[c]).T
+                    w[mi, c, : mon.weights[c].shape[1], :p] = np.asarray(mon.weights[c]).T
                 fr[mi, :nf] = mon.freqs
                 masks[mi] = mon.component_mask
                 counts[mi] = (nf, p, max(1, mon.interval), vo, wo)

@@ -258,7 +258,7 @@ static void zero_pec(const ctx_t* x, int electric) {
 static void dft(const ctx_t* x, int step) {
   const FdtdDft* m = &x->p->dft;
   if (m->monitor_count <= 0) return;
-  const int P = (int)m->indices.dims[2], K = (int)m->indices.dims[3], F = (int)m->freqs.dims[1];
+  const int K = (int)m->indices.dims[2], P = (int)m->indices.dims[3], F = (int)m->freqs.dims[1];
   const int* counts = (const int*)m->counts.data;
   const int* codes = (const int*)m->codes.data;
   const float* win = (const float*)m->windows.data;
@@ -296,10 +296,10 @@ static void dft(const ctx_t* x, int step) {
       const float sm = scale * mk;
 #pragma omp parallel for schedule(static)
       for (int pp = 0; pp < np; ++pp) {
-        const int64_t base = (((int64_t)mi * 6 + c) * P + pp) * K;
+        const int64_t base = (((int64_t)mi * 6 + c) * K) * P + pp;  /* neighbour-major */
         float v = 0.0f;
         for (int n = 0; n < K; ++n)
-          if (w[base + n] != 0.0f) v = v + x->f[c][idx[base + n]] * w[base + n];
+          if (w[base + (int64_t)n * P] != 0.0f) v = v + x->f[c][idx[base + (int64_t)n * P]] * w[base + (int64_t)n * P];
         const int64_t out = voff + (int64_t)c * nf * np + pp;
         for (int f = 0; f < nf; ++f) {
           ((float*)m->re.data)[out + (int64_t)f * np] += sm * (cs[f] * v);
