@@ -286,8 +286,9 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   s.z_chunk = p.z_chunk;
   s.pitch = static_cast<int>(p.pitch);
   s.status = static_cast<int*>(p.status.data);
+  // An axis without absorber terms has no slab anywhere, the faces included.
   for (int a = 0; a < 3; ++a) {
-    s.cpml_inner[a][0] = 0;
+    s.cpml_inner[a][0] = -(1 << 30);
     s.cpml_inner[a][1] = 1 << 30;
   }
   if (p.cpml) {
@@ -296,6 +297,7 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
         const int a = (d == &s.ht[t] ? kHTermAxis : kETermAxis)[t];
         if (d->low + d->high == 0) continue;
         s.cpml_inner[a][0] = d->low > s.cpml_inner[a][0] ? d->low : s.cpml_inner[a][0];
+        if (s.cpml_inner[a][0] < 0) s.cpml_inner[a][0] = 0;
         const int hi = d->n_axis - d->high;
         s.cpml_inner[a][1] = hi < s.cpml_inner[a][1] ? hi : s.cpml_inner[a][1];
       }
