@@ -31,6 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+from beamz_b200 import replicas  # noqa: E402
+
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -175,7 +177,7 @@ def serving_arm(args, rank, world):
     from beamz_b200 import workloads as W
 
     stream = W.serving_requests(args.requests, rate=args.rate, seed=2024)
-    mine = [(a, s) for i, (a, s) in enumerate(stream) if i % world == rank]
+    mine = replicas.shard(stream, rank, world)
     reqs = [serve.Request(i, s, s.total_steps, a) for i, (a, s) in enumerate(mine)]
     warm = [serve.Request(0, W.scene_2d(total_steps=16, shape=(64, 64)), 16, 0.0),
             serve.Request(1, W.scene_3d_512(total_steps=16, shape=(32, 32, 32), pml_cells=4, n_monitors=1, n_freqs=3),
@@ -367,13 +369,9 @@ def main():
         end.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
-    ms = start.elapsed_time(end)
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = replicas.max_over_ranks(start.elapsed_time(end), device=dev)
     cells = spec.cells
-    value = cells * args.steps * world / (ms / 1e3) / 1e9
+    value = replicas.aggregate_rate(cells * args.steps, ms / 1e3, world) / 1e9
     n_src = len(spec.sources)
     per_step = n_src + 1 + (1 if spec.monitors else 0)
     launches = per_step * args.steps + -(-args.steps // R.GRAPH_CHUNK_STEPS)
@@ -433,10 +431,8 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
-        e2e_ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
-        if world > 1:
-            dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-        e2e_value = cells * args.steps * world / (float(e2e_ms.item()) / 1e3) / 1e9
+        e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1), device=dev)
+        e2e_value = replicas.aggregate_rate(cells * args.steps, e2e_ms / 1e3, world) / 1e9
         e2e = {"value": round(e2e_value, 3), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
                "transfers": "initial fields H2D from pinned host memory, final fields + DFT arena D2H, "
