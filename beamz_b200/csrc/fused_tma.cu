@@ -221,6 +221,54 @@ __device__ __forceinline__ float psi_apply(const CpmlTermDev& t, const float4* c
   return d * c.z + next;
 }
 
+// Paired FP32 arithmetic (sm_100 f32x2 instructions): each lane of the pair is
+// rounded exactly as the scalar operation, so paired and scalar code agree
+// bit for bit; the pair halves the instructions issued.  The operations are
+// PTX with an explicit rounding mode, which the compiler never contracts, and
+// the pairs are packed and unpacked with mov.b64 (no type punning).
+__device__ __forceinline__ unsigned long long f2pack(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};\n" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+
+__device__ __forceinline__ float2 f2unpack(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;\n" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(r);
+}
+
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(r);
+}
+
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(r);
+}
+
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)), "l"(f2pack(c)));
+  return f2unpack(r);
+}
+
+// div_rn on a pair: q = a r, e = fma(q, -b, a), q + e r (fdtd_common.cuh).
+__device__ __forceinline__ float2 f2div(float2 a, float2 r2, float2 nb2) {
+  const float2 q = f2mul(a, r2);
+  const float2 e = f2fma(q, nb2, a);
+  return f2fma(e, r2, q);
+}
+
 using kOff = std::integral_constant<bool, false>;
 using kOn = std::integral_constant<bool, true>;
 
@@ -415,11 +463,24 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
         using W7 = std::integral_constant<int, 7>;
         using W5 = std::integral_constant<int, 5>;
         using W6 = std::integral_constant<int, 6>;
+        const float2 r2 = make_float2(inv_res, inv_res), nb2 = make_float2(-res, -res);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int ly = 1 + warp * R + r, lx = 1 + lane, b = ly * BX + lane + 4;
           float hv[3];
-          h_cell(W7{}, b, j0 + ly - 1, i, emit, hv);
+          if constexpr (!AX && !AY && !AZ) {  // Hx and Hy as a pair, Hz alone
+            const int j = j0 + ly - 1;
+            const float2 d0 = f2div(f2sub(make_float2(E0z[b + BX], E1x[b]), make_float2(E0z[b], E0x[b])), r2, nb2);
+            const float2 d1 = f2div(f2sub(make_float2(E1y[b], E0z[b + 1]), make_float2(E0y[b], E0z[b])), r2, nb2);
+            const float2 h = f2sub(f2mul(make_float2(hf.dec0, hf.dec1), make_float2(HOx[b], HOy[b])),
+                                   f2mul(make_float2(hf.src0, hf.src1), f2sub(d0, d1)));
+            hv[0] = (xface && i == 0 && wx0) ? 0.0f : h.x;
+            hv[1] = (yface && j == 0 && wy0) ? 0.0f : h.y;
+            hv[2] = hf.dec2 * HOz[b] - hf.src2 * (div_rn(E0y[b + 1] - E0y[b], res, inv_res) -
+                                                  div_rn(E0x[b + BX] - E0x[b], res, inv_res));
+          } else {
+            h_cell(W7{}, b, j0 + ly - 1, i, emit, hv);
+          }
           sm.hn[hb][0][ly][lx] = hv[0];
           sm.hn[hb][1][ly][lx] = hv[1];
           sm.hn[hb][2][ly][lx] = hv[2];
@@ -509,6 +570,19 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
           if constexpr (AY) q5 = psi_fetch<1>(p.et[5], cpml_slot(p.et[5], j), k, j, i);
           const uint32_t id = IDS[(ly - 1) * T::TX + lane];
           const int o = k * PL + j * P + i;
+          if constexpr (!AX && !AY && !AZ) {  // Ex and Ey as a pair, Ez alone
+            const float2 d0 = f2div(f2sub(make_float2(hz, hx), make_float2(hz_y, hx_z)), r2, nb2);
+            const float2 d1 = f2div(f2sub(make_float2(hy, hz), make_float2(hy_z, hz_x)), r2, nb2);
+            const float2 cd = f2sub(d0, d1);
+            const float2 e = make_float2(E0x[b] + sm.coef[0][id & 0xffu] * cd.x,
+                                         E0y[b] + sm.coef[1][(id >> 8) & 0xffu] * cd.y);
+            p.eout[0][o] = (y0 && wy0) ? 0.0f : e.x;
+            p.eout[1][o] = (x0 && wx0) ? 0.0f : e.y;
+            const float ez = E0z[b] + sm.coef[2][(id >> 16) & 0xffu] *
+                                          (div_rn(hy - hy_x, res, inv_res) - div_rn(hx - hx_y, res, inv_res));
+            p.eout[2][o] = ((x0 && wx0) || (y0 && wy0)) ? 0.0f : ez;
+            continue;
+          }
           {  // Ex: dHz/dy - dHy/dz
             float d0 = div_rn(hz - hz_y, res, inv_res), d1 = div_rn(hy - hy_z, res, inv_res);
             if constexpr (AY) d0 = psi_apply(p.et[0], sm.cc[6], q0, d0, true);

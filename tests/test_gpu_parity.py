@@ -231,3 +231,29 @@ def test_fp64_error_is_reported_and_small():
     st = O.run(oracle_state(oprog, dtype=np.float64), oprog, 30)
     for c in ("Ex", "Ey", "Ez"):
         assert O.relative_l2(out[c], st.fields[c]) <= 1e-4
+
+
+BITWISE_CASES = {
+    "3d_cpml_sources_pec": lambda: scenario_3d(grid=(9, 12, 40), seed=3, nsteps=4, metallic=("front", "left")),
+    "3d_cpml_face_column": lambda: scenario_3d(grid=(10, 17, 64), seed=5, nsteps=4, metallic=("right",)),
+    "2d_tm": lambda: scenario_2d(grid=(17, 23), polarization="tm", nsteps=4),
+    "2d_te": lambda: scenario_2d(grid=(17, 23), polarization="te", nsteps=4),
+}
+
+
+@pytest.mark.parametrize("case", sorted(BITWISE_CASES))
+@pytest.mark.parametrize("schedule", ["fused", "phases"])
+def test_fields_are_bit_identical_to_the_fp32_oracle(case, schedule):
+    """Every field after 4 steps equals the float32 oracle bit for bit (each
+    product and sum rounded once, in the reference's order); the DFT arena,
+    whose phases come from CUDA's sincosf, stays within its tolerance."""
+    spec = BITWISE_CASES[case]()
+    fields = random_initial_fields(spec, seed=4)
+    prog = R.compile_program(spec, schedule=schedule)
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, 4).numpy()
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog, fields), oprog, 4)
+    for c in P.active_components(spec.ndim, spec.polarization):
+        np.testing.assert_array_equal(out[c], st.fields[c], err_msg=c)
+    for mine, ref in ((out["dft_re"], st.dft_re), (out["dft_im"], st.dft_im)):
+        assert O.relative_l2(mine, ref) <= DFT_TOL
