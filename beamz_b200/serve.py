@@ -157,11 +157,15 @@ class ServingEngine:
 
     ``hbm_budget`` bounds the bytes of all resident simulations (default: 80 %
     of the device memory free at construction); ``max_active`` bounds the
-    number of resident simulations; ``chunk`` is the graph length in steps.
+    number of resident simulations and ``max_active_cells`` their cells (32 Mi
+    by default: a few large grids already fill the SMs, and more resident work
+    only lengthens every request's latency); ``chunk`` is the graph length in
+    steps and ``queue_depth`` the chunks kept queued per stream.
     """
 
     def __init__(self, device="cuda", hbm_budget: int | None = None, max_active: int = 48, chunk: int = 256,
-                 return_fields: bool = False, queue_depth: int = 2, tune: bool = False):
+                 return_fields: bool = False, queue_depth: int = 4, tune: bool = False,
+                 max_active_cells: int | None = 32 * 1024 * 1024):
         import torch
 
         from . import runtime
@@ -179,6 +183,9 @@ class ServingEngine:
         self.return_fields = return_fields
         self.queue_depth = int(queue_depth)
         self.tune = tune
+        # Resident cells beyond a few large grids only share the same SMs:
+        # throughput stays, latency grows.  None disables the bound.
+        self.max_active_cells = max_active_cells
         self.peak_bytes = 0
         self.peak_active = 0
 
@@ -200,6 +207,7 @@ class ServingEngine:
         queue: deque[Request] = deque()
         active: list[_Slot] = []
         used = 0
+        cells = 0
         results = {}
         t0 = clock()
         while pending or queue or active:
@@ -212,9 +220,13 @@ class ServingEngine:
                 need = estimate_bytes(queue[0].spec)
                 if used + need > self.hbm_budget and active:
                     break
+                if (self.max_active_cells is not None and active
+                        and cells + queue[0].spec.cells > self.max_active_cells):
+                    break
                 req = queue.popleft()
                 active.append(self._admit(req, clock() - t0, need))
                 used += need
+                cells += req.spec.cells
                 self.peak_bytes = max(self.peak_bytes, used)
                 self.peak_active = max(self.peak_active, len(active))
                 progressed = True
@@ -234,6 +246,7 @@ class ServingEngine:
                     results[r.rid] = Result(r.rid, r.nsteps, out["dft_re"], out["dft_im"], out["dft_w"], out["fields"],
                                             r.arrival, slot.admitted, finished)
                     used -= slot.nbytes
+                    cells -= slot.req.spec.cells
                     slot.release()
                     progressed = True
                 else:
