@@ -1,13 +1,14 @@
 """Continuous-batching serving loop for FDTD simulation requests.
 
 Requests (a planned :class:`~beamz_b200.plan.ProgramSpec` plus a step count)
-arrive over time.  The engine admits them FIFO as soon as the HBM budget and
-the slot limit allow -- also while others are running -- compiles each onto
-the device once, and keeps its fields, CPML memories and DFT arena resident
-until it finishes.  Every admitted simulation gets its own CUDA stream and its
-own executable graphs of up to ``chunk`` steps (``fdtd_graph_create``); the
-host loop keeps two chunks queued per stream, so the simulations' step kernels
-overlap on the device and small grids fill the GPU together.  Results (the
+arrive over time.  The engine admits them FIFO as soon as the HBM budget, the
+slot limit and the resident-cell bound allow -- also while others are running
+-- compiles each onto the device once, and keeps its fields, CPML memories and
+DFT arena resident until it finishes.  Every admitted simulation gets its own
+CUDA stream and its own executable graphs of up to ``chunk`` steps
+(``fdtd_graph_create``); the host loop keeps up to ``queue_depth`` chunks
+queued per stream, so the simulations' step kernels overlap on the device and
+small grids fill the GPU together.  Results (the
 DFT arena and, optionally, the fields) are copied back when a simulation's
 last chunk completes, and its memory and graphs are released, which admits
 the next request.
