@@ -224,8 +224,10 @@ __device__ __forceinline__ float psi_apply(const CpmlTermDev& t, const float4* c
 // Paired FP32 arithmetic (sm_100 f32x2 instructions): each lane of the pair is
 // rounded exactly as the scalar operation, so paired and scalar code agree
 // bit for bit; the pair halves the instructions issued.  The operations are
-// PTX with an explicit rounding mode, which the compiler never contracts, and
-// the pairs are packed and unpacked with mov.b64 (no type punning).
+// PTX with an explicit rounding mode, and the pairs are packed and unpacked
+// with mov.b64 (no type punning).  A paired add fed by a paired multiply was
+// measured to come out fused into one rounding, so the E update's final
+// multiply-add stays scalar.
 __device__ __forceinline__ unsigned long long f2pack(float2 a) {
   unsigned long long r;
   asm("mov.b64 %0, {%1, %2};\n" : "=l"(r) : "f"(a.x), "f"(a.y));
@@ -247,12 +249,6 @@ __device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
 __device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
   unsigned long long r;
   asm("mul.rn.f32x2 %0, %1, %2;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
-  return f2unpack(r);
-}
-
-__device__ __forceinline__ float2 f2add(float2 a, float2 b) {
-  unsigned long long r;
-  asm("add.rn.f32x2 %0, %1, %2;\n" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
   return f2unpack(r);
 }
 
