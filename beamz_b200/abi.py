@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 4
+FDTD_ABI_VERSION = 5
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
@@ -102,7 +102,7 @@ class FdtdSource(ctypes.Structure):
 class FdtdDft(ctypes.Structure):
     _fields_ = [
         ("monitor_count", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("batch", ctypes.c_int32),
         ("indices", FdtdBuffer),
         ("weights", FdtdBuffer),
         ("freqs", FdtdBuffer),
@@ -113,6 +113,7 @@ class FdtdDft(ctypes.Structure):
         ("re", FdtdBuffer),
         ("im", FdtdBuffer),
         ("weight_sum", FdtdBuffer),
+        ("samples", FdtdBuffer),
     ]
 
 

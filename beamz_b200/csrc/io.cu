@@ -118,6 +118,116 @@ __global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* c
   }
 }
 
+// Step batching: dft_sample_kernel stores one step's gathered sample of every
+// (monitor, component, point) into slot `slot` of a [batch, M, 6, P] buffer;
+// dft_flush_kernel then adds `count` buffered steps to the arena in step
+// order, with the same gate, window, scale and phase per step as dft_kernel,
+// so the arena is bit-identical to per-step accumulation while it is read
+// and written once per batch.
+constexpr int kDftMaxBatch = 16;
+
+__device__ __forceinline__ float dft_gather(const DftDev& d, int m, int c, int p) {
+  const int K = d.neighbors;
+  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * K) * d.max_points + p;
+  const float* field = d.fields[c];
+  float v = 0.0f;
+  for (int n = 0; n < K; ++n) {
+    const float w = d.weights[base + static_cast<int64_t>(n) * d.max_points];
+    if (w == 0.0f) break;
+    const int idx = d.indices[base + static_cast<int64_t>(n) * d.max_points];
+    if (idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kDftThreads) dft_sample_kernel(DftDev d, float* samples, int slot) {
+  const int mc = blockIdx.y;
+  const int m = mc / 6, c = mc % 6;
+  const int np = min(max(d.counts[5 * m + 1], 0), d.max_points);
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || d.masks[m * 6 + c] == 0.0f) return;
+  samples[((static_cast<int64_t>(slot) * d.monitor_count + m) * 6 + c) * d.max_points + p] = dft_gather(d, m, c, p);
+}
+
+__global__ void __launch_bounds__(kDftThreads) dft_flush_kernel(DftDev d, const float* samples, const int* counter,
+                                                                int first, int count) {
+  const int mc = blockIdx.y;
+  const int m = mc / 6, c = mc % 6;
+  const int* cnt = d.counts + 5 * m;
+  const int nf = min(max(cnt[0], 0), d.max_freqs);
+  const int np = min(max(cnt[1], 0), d.max_points);
+  const int interval = cnt[2] > 0 ? cnt[2] : 1;
+  const int voff = cnt[3], woff = cnt[4];
+  const float t0 = d.windows[3 * m], t1 = d.windows[3 * m + 1], unit = d.windows[3 * m + 2];
+  __shared__ float s_cos[kDftMaxBatch][kDftMaxFreqs];
+  __shared__ float s_sin[kDftMaxBatch][kDftMaxFreqs];
+  __shared__ float s_scale[kDftMaxBatch];
+  __shared__ float s_window[kDftMaxBatch];
+  __shared__ float s_time[kDftMaxBatch];
+  __shared__ int s_on[kDftMaxBatch];
+  for (int s = threadIdx.x; s < count; s += blockDim.x) {
+    const int step = counter[0] + first + s;
+    int ti = step < 0 ? 0 : step;
+    ti = ti >= d.step_time_len ? d.step_time_len - 1 : ti;
+    const float t = d.step_time[ti];
+    const bool on = step % interval == 0 && t >= t0 && t <= t1;
+    float window = 1.0f;
+    if (on && d.codes[2 * m] == 1 && isfinite(t1) && t1 > t0) {
+      const float span = fmaxf(t1 - t0, 1e-30f);
+      const float tau = fminf(fmaxf((t - t0) / span, 0.0f), 1.0f);
+      window = 0.5f * (1.0f - cosf(6.2831855f * tau));
+    }
+    float scale = fmaxf(window, 0.0f);
+    if (d.codes[2 * m + 1] == 1) {
+      const float phys = ((d.dt * static_cast<float>(interval)) * 299792458.0f) / unit;
+      scale = scale * (phys / sqrtf(6.2831855f));
+    }
+    s_on[s] = on ? 1 : 0;
+    s_scale[s] = scale;
+    s_window[s] = window;
+    s_time[s] = t;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < count * nf; e += blockDim.x) {
+    const int s = e / nf, f = e % nf;
+    const float theta = (6.2831855f * d.freqs[m * d.max_freqs + f]) * s_time[s];
+    float sn, cs;
+    sincosf(theta, &sn, &cs);
+    s_cos[s][f] = cs;
+    s_sin[s][f] = sn;
+  }
+  __syncthreads();
+  if (c == 0 && blockIdx.x == 0) {
+    for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+      if (woff < 0 || woff + f >= d.weight_len) continue;
+      float ws = d.weight_sum[woff + f];
+      for (int s = 0; s < count; ++s)
+        if (s_on[s]) ws += s_window[s];
+      d.weight_sum[woff + f] = ws;
+    }
+  }
+  const float mask = d.masks[m * 6 + c];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || mask == 0.0f) return;
+  if (voff < 0 || voff + static_cast<int64_t>(6) * nf * np > d.arena_len) return;
+  const int64_t out = voff + (static_cast<int64_t>(c) * nf) * np + p;
+  const int64_t stride = static_cast<int64_t>(d.monitor_count) * 6 * d.max_points;
+  const float* v = samples + (static_cast<int64_t>(m) * 6 + c) * d.max_points + p;
+  for (int f = 0; f < nf; ++f) {
+    float re = d.re[out + static_cast<int64_t>(f) * np];
+    float im = d.im[out + static_cast<int64_t>(f) * np];
+    for (int s = 0; s < count; ++s) {
+      if (!s_on[s]) continue;
+      const float sm = s_scale[s] * mask;
+      const float vs = v[s * stride];
+      re += sm * (s_cos[s][f] * vs);
+      im += sm * (s_sin[s][f] * vs);
+    }
+    d.re[out + static_cast<int64_t>(f) * np] = re;
+    d.im[out + static_cast<int64_t>(f) * np] = im;
+  }
+}
+
 __global__ void counter_kernel(int* counter, int nsteps) { counter[0] += nsteps; }
 
 }  // namespace
@@ -148,6 +258,22 @@ cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, in
   if (dft.max_freqs > kDftMaxFreqs) return cudaErrorInvalidValue;
   const dim3 grid((dft.max_points + kDftThreads - 1) / kDftThreads, dft.monitor_count * 6, 1);
   dft_kernel<<<grid, kDftThreads, 0, s>>>(dft, counter, step_offset);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_dft_sample(cudaStream_t s, const DftDev& dft, float* samples, int slot) {
+  if (dft.monitor_count <= 0 || dft.max_points <= 0) return cudaSuccess;
+  const dim3 grid((dft.max_points + kDftThreads - 1) / kDftThreads, dft.monitor_count * 6, 1);
+  dft_sample_kernel<<<grid, kDftThreads, 0, s>>>(dft, samples, slot);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_dft_flush(cudaStream_t s, const DftDev& dft, const float* samples, const int* counter, int first,
+                             int count) {
+  if (dft.monitor_count <= 0 || dft.max_points <= 0 || count <= 0) return cudaSuccess;
+  if (dft.max_freqs > kDftMaxFreqs || count > kDftMaxBatch) return cudaErrorInvalidValue;
+  const dim3 grid((dft.max_points + kDftThreads - 1) / kDftThreads, dft.monitor_count * 6, 1);
+  dft_flush_kernel<<<grid, kDftThreads, 0, s>>>(dft, samples, counter, first, count);
   return cudaPeekAtLastError();
 }
 

@@ -99,6 +99,9 @@ cudaError_t launch_copy3d(cudaStream_t s, const float* src, int64_t src_row, int
 struct DftDev;
 cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, int step_offset);
 cudaError_t launch_counter_advance(cudaStream_t s, int* counter, int nsteps);
+cudaError_t launch_dft_sample(cudaStream_t s, const DftDev& dft, float* samples, int slot);
+cudaError_t launch_dft_flush(cudaStream_t s, const DftDev& dft, const float* samples, const int* counter, int first,
+                             int count);
 
 // Adjoint step buffers (see FdtdAdjointStep in fdtd_b200.h).
 struct AdjDev {

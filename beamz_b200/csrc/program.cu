@@ -203,6 +203,10 @@ int validate(const FdtdProgram& p) {
     for (const FdtdBuffer* b : {&d.indices, &d.weights, &d.freqs, &d.masks, &d.counts, &d.codes, &d.windows, &d.re,
                                 &d.im, &d.weight_sum})
       if (b->data == nullptr && elements(*b) > 0) return kInvalid;
+    if (d.batch < 0 || d.batch > 16) return kInvalid;
+    if (d.samples.data != nullptr &&
+        (!is_f32(d.samples) || elements(d.samples) != static_cast<int64_t>(d.batch) * M * 6 * d.indices.dims[3]))
+      return kInvalid;
   }
   return 0;
 }
@@ -381,6 +385,10 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
   SourceDev hsrc[kMaxFusedSources];
   for (int i = 0; i < p.source_count; ++i)
     if (p.sources[i].timing == FDTD_TIMING_H) hsrc[n_hsrc++] = source_dev(p.sources[i]);
+  // DFT step batching (validated: batch <= 16, samples sized [batch, M, 6, P]).
+  const bool batched = p.dft.monitor_count > 0 && p.dft.batch > 1 && p.dft.samples.data != nullptr;
+  float* samples = static_cast<float*>(p.dft.samples.data);
+  int batch_start = 0;
   for (int step = 0; step < p.nsteps; ++step) {
     const int bank = fused ? (step & 1) : 0;
     const FdtdBuffer* a = bank == 0 ? p.fields : p.fields_alt;
@@ -409,7 +417,16 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     }
     err = enqueue_sources(s, p, L, b, FDTD_TIMING_E, step);
     if (err != cudaSuccess) return err;
-    if (p.dft.monitor_count > 0) {
+    if (p.dft.monitor_count > 0 && batched) {
+      const DftDev dd = make_dft(p, b);
+      err = launch_dft_sample(s, dd, samples, step - batch_start);
+      if (err != cudaSuccess) return err;
+      if (step - batch_start + 1 == p.dft.batch || step == p.nsteps - 1) {
+        err = launch_dft_flush(s, dd, samples, counter, batch_start, step - batch_start + 1);
+        if (err != cudaSuccess) return err;
+        batch_start = step + 1;
+      }
+    } else if (p.dft.monitor_count > 0) {
       err = launch_dft(s, make_dft(p, b), counter, step);
       if (err != cudaSuccess) return err;
     }

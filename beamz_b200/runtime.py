@@ -170,7 +170,7 @@ class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
     def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
-                 graphs=True, layout="auto"):
+                 graphs=True, layout="auto", dft_batch: int = 8):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
         torch = _torch()
@@ -229,6 +229,9 @@ class DeviceProgram:
             s.layout = abi.FDTD_LAYOUT_PITCHED
             s.pitch = self.pitch
         self._keep = []  # tensors referenced by the struct
+        # DFT samples are buffered and added to the arena every `dft_batch` steps
+        # (bit-identical to per-step accumulation; 1 disables the buffer).
+        self.dft_batch = max(1, min(16, int(dft_batch)))
         self.e_source = {}  # per-site E source coefficients (site material), by component
 
         def buf(t):
@@ -349,6 +352,9 @@ class DeviceProgram:
             s.dft.re = abi.buffer_of(state.dft_re)
             s.dft.im = abi.buffer_of(state.dft_im)
             s.dft.weight_sum = abi.buffer_of(state.dft_w)
+            if state.dft_samples is not None:
+                s.dft.batch = self.dft_batch
+                s.dft.samples = abi.buffer_of(state.dft_samples)
         s.step_counter = abi.buffer_of(state.counter)
         s.step_time = abi.buffer_of(self.step_time)
         s.status = abi.buffer_of(state.status)
@@ -396,6 +402,10 @@ class DeviceState:
         self.dft_re = torch.zeros(nv, dtype=torch.float32, device=dev)
         self.dft_im = torch.zeros(nv, dtype=torch.float32, device=dev)
         self.dft_w = torch.zeros(nw, dtype=torch.float32, device=dev)
+        self.dft_samples = None
+        if a is not None and program.dft_batch > 1:
+            M, P = len(a.layout), int(a.indices.shape[3])
+            self.dft_samples = torch.empty((program.dft_batch, M, 6, P), dtype=torch.float32, device=dev)
         self.counter = torch.full((1,), int(step), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.step = int(step)

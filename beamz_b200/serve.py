@@ -76,7 +76,7 @@ def estimate_bytes(spec: ProgramSpec, schedule: str = "fused") -> int:
     dft = 0
     for m in spec.monitors:
         points = max(int(np.asarray(ix).shape[0]) for ix in m.indices)
-        dft += 6 * len(m.freqs) * points * 8 * 2 + 6 * points * 8 * 8
+        dft += 6 * len(m.freqs) * points * 8 * 2 + 6 * points * 8 * 8 + 8 * 6 * points * 4  # + sample batch
     return banks * field_bytes + material + psi + dft + 4 * max(int(spec.total_steps), 1) + (1 << 20)
 
 

@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 4
+#define FDTD_ABI_VERSION 5
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
 enum {
@@ -131,10 +131,11 @@ typedef struct FdtdSource {
  *  codes    S32 [M, 2]: window code (1 = Hann), normalization code (1 = physical)
  *  windows  F32 [M, 3]: t_start, t_end, length_unit
  *  re, im   F32 arena, accumulated at value_offset + (c * F + f) * P + p
- *  weight_sum F32 arena, accumulated at weight_offset + f                       */
+ *  weight_sum F32 arena, accumulated at weight_offset + f
+ *  samples  F32 [batch, M, 6, P] (optional step batching)                      */
 typedef struct FdtdDft {
   int32_t monitor_count;
-  int32_t reserved;
+  int32_t batch;           /* > 1 with `samples`: accumulate every `batch` steps (below) */
   FdtdBuffer indices;
   FdtdBuffer weights;
   FdtdBuffer freqs;
@@ -145,6 +146,12 @@ typedef struct FdtdDft {
   FdtdBuffer re;
   FdtdBuffer im;
   FdtdBuffer weight_sum;
+  /* F32 [batch, M, 6, P], optional.  With it, fdtd_launch_program stores each
+   * step's gathered samples and adds a batch of them to re/im/weight_sum in
+   * one pass every `batch` steps and at the end of the call -- in step order,
+   * so the arena is bit-identical to per-step accumulation, with the arena
+   * read and written once per batch instead of once per step. */
+  FdtdBuffer samples;
 } FdtdDft;
 
 /* A complete step program (replaces BeamzLaunch + BeamzProgramLaunch,

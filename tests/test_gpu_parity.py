@@ -257,3 +257,22 @@ def test_fields_are_bit_identical_to_the_fp32_oracle(case, schedule):
         np.testing.assert_array_equal(out[c], st.fields[c], err_msg=c)
     for mine, ref in ((out["dft_re"], st.dft_re), (out["dft_im"], st.dft_im)):
         assert O.relative_l2(mine, ref) <= DFT_TOL
+
+
+@pytest.mark.parametrize("dims", [3, 2])
+def test_dft_step_batching_is_bit_identical(dims):
+    """Samples buffered and flushed every few steps (and at every call's end)
+    give the same arena, bit for bit, as per-step accumulation."""
+    spec = (scenario_3d(grid=(9, 12, 40), seed=8, nsteps=37) if dims == 3
+            else scenario_2d(grid=(17, 23), polarization="tm", nsteps=37))
+    fields = random_initial_fields(spec, seed=2)
+    outs = []
+    for batch in (1, 8, 5):
+        prog = R.compile_program(spec, dft_batch=batch)
+        st = R.initial_state(prog, fields=fields)
+        R.run_steps(st, prog, 20)
+        R.run_steps(st, prog, 17)
+        outs.append(st.numpy())
+    for out in outs[1:]:
+        for key in ("dft_re", "dft_im", "dft_w"):
+            np.testing.assert_array_equal(out[key], outs[0][key], err_msg=key)
