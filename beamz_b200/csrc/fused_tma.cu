@@ -225,9 +225,10 @@ __device__ __forceinline__ float psi_apply(const CpmlTermDev& t, const float4* c
 // rounded exactly as the scalar operation, so paired and scalar code agree
 // bit for bit; the pair halves the instructions issued.  The operations are
 // PTX with an explicit rounding mode, and the pairs are packed and unpacked
-// with mov.b64 (no type punning).  A paired add fed by a paired multiply was
-// measured to come out fused into one rounding, so the E update's final
-// multiply-add stays scalar.
+// with mov.b64 (no type punning).  A paired add or subtract fed by a paired
+// multiply was measured to come out fused into one rounding (about a fifth of
+// the lanes differ), so the final multiply-adds of the H and E updates stay
+// scalar.
 __device__ __forceinline__ unsigned long long f2pack(float2 a) {
   unsigned long long r;
   asm("mov.b64 %0, {%1, %2};\n" : "=l"(r) : "f"(a.x), "f"(a.y));
@@ -468,10 +469,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
             const int j = j0 + ly - 1;
             const float2 d0 = f2div(f2sub(make_float2(E0z[b + BX], E1x[b]), make_float2(E0z[b], E0x[b])), r2, nb2);
             const float2 d1 = f2div(f2sub(make_float2(E1y[b], E0z[b + 1]), make_float2(E0y[b], E0z[b])), r2, nb2);
-            const float2 h = f2sub(f2mul(make_float2(hf.dec0, hf.dec1), make_float2(HOx[b], HOy[b])),
-                                   f2mul(make_float2(hf.src0, hf.src1), f2sub(d0, d1)));
-            hv[0] = (xface && i == 0 && wx0) ? 0.0f : h.x;
-            hv[1] = (yface && j == 0 && wy0) ? 0.0f : h.y;
+            const float2 cd = f2sub(d0, d1);
+            const float hx = hf.dec0 * HOx[b] - hf.src0 * cd.x, hy = hf.dec1 * HOy[b] - hf.src1 * cd.y;
+            hv[0] = (xface && i == 0 && wx0) ? 0.0f : hx;
+            hv[1] = (yface && j == 0 && wy0) ? 0.0f : hy;
             hv[2] = hf.dec2 * HOz[b] - hf.src2 * (div_rn(E0y[b + 1] - E0y[b], res, inv_res) -
                                                   div_rn(E0x[b + BX] - E0x[b], res, inv_res));
           } else {

@@ -140,6 +140,26 @@ def test_fused_tiles_and_z_chunks_are_bitwise_identical(tile, z_chunk):
     np.testing.assert_array_equal(out["dft_re"], ref["dft_re"])
 
 
+def test_lossy_uniform_h_matches_the_scalar_schedule():
+    """A uniform H decay below one (magnetic loss) through the pitched
+    straight path, whose interior tiles pair two components per instruction:
+    every field equals the dense scalar schedule's bit for bit (each product
+    and difference rounded on its own, none fused)."""
+    import dataclasses
+
+    spec = scenario_3d(grid=(24, 24, 192), seed=6, nsteps=6, metallic=("front",))
+    loss = np.float32(0.9996)
+    site = {c: (np.float32(0.9993), np.float32(np.float32(s) * loss)) for c, (_d, s) in spec.h_coefficients().items()}
+    spec = dataclasses.replace(spec, h_site=site)
+    fields = random_initial_fields(spec, seed=7)
+    ref_prog = R.compile_program(spec, schedule="phases")
+    ref = R.run_steps(R.initial_state(ref_prog, fields=fields), ref_prog, 6).numpy()
+    prog = R.compile_program(spec, schedule="fused", layout="pitched", tile=(32, 8), z_chunk=8)
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, 6).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(out[c], ref[c], err_msg=c)
+
+
 # Grids whose x extent is a multiple of the 32-wide tile: the last tile owns the
 # face column x = X; low faces take the straight path with per-lane ghosts.
 FACE_CASES = [
