@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 FDTD_ABI_VERSION = 5
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
+FDTD_FLAG_DFT_OVERLAP = 1 << 16
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
 FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL, FDTD_MATERIAL_CODEBOOK = 0, 1, 2
 FDTD_LAYOUT_DENSE, FDTD_LAYOUT_PITCHED = 0, 1

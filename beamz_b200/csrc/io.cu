@@ -41,6 +41,45 @@ __global__ void copy3d_kernel(const float* src, int64_t sr, int64_t sp, float* d
 constexpr int kDftThreads = 256;
 constexpr int kDftMaxFreqs = 64;
 
+// Interpolated sample of one (monitor, component, point).  Neighbour-major
+// plan: consecutive points of one neighbour slot are contiguous, and per point
+// the nonzero weights come first, so the sum runs over the slots before the
+// first zero weight, in slot order (the same sum as skipping zeros).  The
+// first kGatherSlots slots' weights and indices are loaded together, then
+// their field values together: two dependent memory round trips per point
+// instead of one per slot (plane monitors interpolate over at most four).
+constexpr int kGatherSlots = 4;
+
+__device__ __forceinline__ float dft_gather(const DftDev& d, int m, int c, int p) {
+  const int K = d.neighbors;
+  const int64_t stride = d.max_points;
+  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * K) * stride + p;
+  const float* field = d.fields[c];
+  const int64_t len = d.field_len[c];
+  float w[kGatherSlots], f[kGatherSlots];
+  int idx[kGatherSlots];
+#pragma unroll
+  for (int n = 0; n < kGatherSlots; ++n) {
+    w[n] = n < K ? d.weights[base + n * stride] : 0.0f;
+    idx[n] = n < K ? d.indices[base + n * stride] : -1;
+  }
+#pragma unroll
+  for (int n = 0; n < kGatherSlots; ++n) f[n] = (w[n] != 0.0f && idx[n] >= 0 && idx[n] < len) ? field[idx[n]] : 0.0f;
+  float v = 0.0f;
+#pragma unroll
+  for (int n = 0; n < kGatherSlots; ++n) {
+    if (w[n] == 0.0f) return v;
+    if (idx[n] >= 0 && idx[n] < len) v = v + f[n] * w[n];
+  }
+  for (int n = kGatherSlots; n < K; ++n) {
+    const float wn = d.weights[base + n * stride];
+    if (wn == 0.0f) break;
+    const int i = d.indices[base + n * stride];
+    if (i >= 0 && i < len) v = v + field[i] * wn;
+  }
+  return v;
+}
+
 __global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* counter, int step_offset) {
   const int mc = blockIdx.y;
   const int m = mc / 6;
@@ -97,19 +136,7 @@ __global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* c
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np || mask == 0.0f) return;
   if (voff < 0 || voff + static_cast<int64_t>(6) * nf * np > d.arena_len) return;
-  // Neighbour-major plan: consecutive points of one neighbour slot are
-  // contiguous; per point the nonzero weights come first, so the gather stops
-  // at the first zero (the same sum, in the same order, as skipping zeros).
-  const int K = d.neighbors;
-  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * K) * d.max_points + p;
-  const float* field = d.fields[c];
-  float v = 0.0f;
-  for (int n = 0; n < K; ++n) {
-    const float w = d.weights[base + static_cast<int64_t>(n) * d.max_points];
-    if (w == 0.0f) break;
-    const int idx = d.indices[base + static_cast<int64_t>(n) * d.max_points];
-    if (idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
-  }
+  const float v = dft_gather(d, m, c, p);
   const float sm = s_scale * mask;
   const int64_t out = voff + (static_cast<int64_t>(c) * nf) * np + p;
   for (int f = 0; f < nf; ++f) {
@@ -126,21 +153,11 @@ __global__ void __launch_bounds__(kDftThreads) dft_kernel(DftDev d, const int* c
 // and written once per batch.
 constexpr int kDftMaxBatch = 16;
 
-__device__ __forceinline__ float dft_gather(const DftDev& d, int m, int c, int p) {
-  const int K = d.neighbors;
-  const int64_t base = ((static_cast<int64_t>(m) * 6 + c) * K) * d.max_points + p;
-  const float* field = d.fields[c];
-  float v = 0.0f;
-  for (int n = 0; n < K; ++n) {
-    const float w = d.weights[base + static_cast<int64_t>(n) * d.max_points];
-    if (w == 0.0f) break;
-    const int idx = d.indices[base + static_cast<int64_t>(n) * d.max_points];
-    if (idx >= 0 && idx < d.field_len[c]) v = v + field[idx] * w;
-  }
-  return v;
-}
+// 128-thread blocks at 32 registers: one fits on an SM beside five resident
+// step CTAs, so sampling on a side stream overlaps the next step.
+constexpr int kDftSampleThreads = 128;
 
-__global__ void __launch_bounds__(kDftThreads) dft_sample_kernel(DftDev d, float* samples, int slot) {
+__global__ void __launch_bounds__(kDftSampleThreads, 16) dft_sample_kernel(DftDev d, float* samples, int slot) {
   const int mc = blockIdx.y;
   const int m = mc / 6, c = mc % 6;
   const int np = min(max(d.counts[5 * m + 1], 0), d.max_points);
@@ -213,18 +230,37 @@ __global__ void __launch_bounds__(kDftThreads) dft_flush_kernel(DftDev d, const 
   const int64_t out = voff + (static_cast<int64_t>(c) * nf) * np + p;
   const int64_t stride = static_cast<int64_t>(d.monitor_count) * 6 * d.max_points;
   const float* v = samples + (static_cast<int64_t>(m) * 6 + c) * d.max_points + p;
-  for (int f = 0; f < nf; ++f) {
-    float re = d.re[out + static_cast<int64_t>(f) * np];
-    float im = d.im[out + static_cast<int64_t>(f) * np];
-    for (int s = 0; s < count; ++s) {
-      if (!s_on[s]) continue;
-      const float sm = s_scale[s] * mask;
-      const float vs = v[s * stride];
-      re += sm * (s_cos[s][f] * vs);
-      im += sm * (s_sin[s][f] * vs);
+  // The point's buffered samples are loaded once, and the arena words of
+  // kFlushFreqs frequencies together, so a flush costs a few memory round
+  // trips per point; each arena word still adds the steps in step order.
+  constexpr int kFlushFreqs = 4;
+  float vs[kDftMaxBatch];
+#pragma unroll
+  for (int s = 0; s < kDftMaxBatch; ++s) vs[s] = s < count && s_on[s] ? v[s * stride] : 0.0f;
+  for (int f0 = 0; f0 < nf; f0 += kFlushFreqs) {
+    float re[kFlushFreqs], im[kFlushFreqs];
+#pragma unroll
+    for (int q = 0; q < kFlushFreqs; ++q) {
+      const int64_t o = out + static_cast<int64_t>(f0 + q) * np;
+      re[q] = f0 + q < nf ? d.re[o] : 0.0f;
+      im[q] = f0 + q < nf ? d.im[o] : 0.0f;
     }
-    d.re[out + static_cast<int64_t>(f) * np] = re;
-    d.im[out + static_cast<int64_t>(f) * np] = im;
+#pragma unroll
+    for (int q = 0; q < kFlushFreqs; ++q) {
+      const int f = f0 + q;
+      if (f >= nf) break;
+#pragma unroll
+      for (int s = 0; s < kDftMaxBatch; ++s) {
+        if (s >= count) break;
+        if (!s_on[s]) continue;
+        const float sm = s_scale[s] * mask;
+        re[q] += sm * (s_cos[s][f] * vs[s]);
+        im[q] += sm * (s_sin[s][f] * vs[s]);
+      }
+      const int64_t o = out + static_cast<int64_t>(f) * np;
+      d.re[o] = re[q];
+      d.im[o] = im[q];
+    }
   }
 }
 
@@ -263,8 +299,8 @@ cudaError_t launch_dft(cudaStream_t s, const DftDev& dft, const int* counter, in
 
 cudaError_t launch_dft_sample(cudaStream_t s, const DftDev& dft, float* samples, int slot) {
   if (dft.monitor_count <= 0 || dft.max_points <= 0) return cudaSuccess;
-  const dim3 grid((dft.max_points + kDftThreads - 1) / kDftThreads, dft.monitor_count * 6, 1);
-  dft_sample_kernel<<<grid, kDftThreads, 0, s>>>(dft, samples, slot);
+  const dim3 grid((dft.max_points + kDftSampleThreads - 1) / kDftSampleThreads, dft.monitor_count * 6, 1);
+  dft_sample_kernel<<<grid, kDftSampleThreads, 0, s>>>(dft, samples, slot);
   return cudaPeekAtLastError();
 }
 

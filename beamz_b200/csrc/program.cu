@@ -5,9 +5,11 @@
 // cache in cuda/src/graph.cu (11-154).
 
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <utility>
 
 #include "kernels.cuh"
 
@@ -374,6 +376,68 @@ DftDev make_dft(const FdtdProgram& p, const FdtdBuffer* bank_fields) {
   return d;
 }
 
+// ---- DFT sampling beside the next step --------------------------------------
+// With FDTD_FLAG_DFT_OVERLAP, step n's sample runs on a side stream while step
+// n+1 (which only reads that bank) runs on the caller's stream; step n+2, which
+// overwrites the bank, waits for it, and every call joins the side stream
+// before the step counter advances.  One side stream (higher priority, so its
+// small blocks take the SM room the step kernel leaves) and its events per
+// (device, caller stream), created outside any capture and kept until exit.
+struct SideStream {
+  cudaStream_t side = nullptr;
+  cudaEvent_t step_done = nullptr;
+  cudaEvent_t sample_done[2] = {nullptr, nullptr};
+  cudaEvent_t joined = nullptr;
+};
+
+std::mutex& side_mutex() {
+  static std::mutex* m = new std::mutex();
+  return *m;
+}
+
+std::map<std::pair<int, cudaStream_t>, SideStream>& side_table() {
+  static auto* t = new std::map<std::pair<int, cudaStream_t>, SideStream>();
+  return *t;
+}
+
+// The side stream of `s`, created when `create` (never while `s` captures);
+// nullptr when absent.
+cudaError_t side_stream_of(cudaStream_t s, bool create, SideStream** out) {
+  *out = nullptr;
+  int device = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err != cudaSuccess) return err;
+  std::lock_guard<std::mutex> lock(side_mutex());
+  auto& table = side_table();
+  const auto key = std::make_pair(device, s);
+  auto it = table.find(key);
+  if (it != table.end()) {
+    *out = &it->second;
+    return cudaSuccess;
+  }
+  if (!create) return cudaSuccess;
+  SideStream ss;
+  int least = 0, greatest = 0;
+  err = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&ss.side, cudaStreamNonBlocking, greatest);
+  cudaEvent_t* events[4] = {&ss.step_done, &ss.sample_done[0], &ss.sample_done[1], &ss.joined};
+  for (cudaEvent_t* e : events)
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+  if (err != cudaSuccess) {
+    for (cudaEvent_t* e : events)
+      if (*e) cudaEventDestroy(*e);
+    if (ss.side) cudaStreamDestroy(ss.side);
+    return err;
+  }
+  *out = &table.emplace(key, ss).first->second;
+  return cudaSuccess;
+}
+
+bool wants_side_stream(const FdtdProgram& p) {
+  return (p.flags & FDTD_FLAG_DFT_OVERLAP) != 0 && p.schedule == FDTD_SCHEDULE_FUSED && p.dft.monitor_count > 0 &&
+         p.dft.batch > 1 && p.dft.samples.data != nullptr;
+}
+
 // Enqueue `nsteps` steps.  Under the fused schedule step s reads bank (s & 1).
 cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
   Layout L;
@@ -389,6 +453,17 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
   const bool batched = p.dft.monitor_count > 0 && p.dft.batch > 1 && p.dft.samples.data != nullptr;
   float* samples = static_cast<float*>(p.dft.samples.data);
   int batch_start = 0;
+  // Side stream for the samples (FDTD_FLAG_DFT_OVERLAP); while `s` captures, an
+  // absent one is not created and the samples stay on `s`.
+  SideStream* ss = nullptr;
+  if (wants_side_stream(p)) {
+    cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(s, &status);
+    if (err != cudaSuccess) return err;
+    err = side_stream_of(s, status == cudaStreamCaptureStatusNone, &ss);
+    if (err != cudaSuccess) return err;
+  }
+  const cudaStream_t ds = ss ? ss->side : s;
   for (int step = 0; step < p.nsteps; ++step) {
     const int bank = fused ? (step & 1) : 0;
     const FdtdBuffer* a = bank == 0 ? p.fields : p.fields_alt;
@@ -396,6 +471,10 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     cudaError_t err = enqueue_sources(s, p, L, a, FDTD_TIMING_PRE_E, step);
     if (err != cudaSuccess) return err;
     Step3D sp = make_step(p, L, bank, fused, step);
+    if (ss && step >= 2) {  // step `step` overwrites the bank that sample step-2 reads
+      err = cudaStreamWaitEvent(s, ss->sample_done[step & 1], 0);
+      if (err != cudaSuccess) return err;
+    }
     if (fused) {
       sp.n_hsrc = n_hsrc;
       for (int i = 0; i < n_hsrc; ++i) sp.hsrc[i] = hsrc[i];
@@ -419,10 +498,19 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     if (err != cudaSuccess) return err;
     if (p.dft.monitor_count > 0 && batched) {
       const DftDev dd = make_dft(p, b);
-      err = launch_dft_sample(s, dd, samples, step - batch_start);
+      if (ss) {
+        err = cudaEventRecord(ss->step_done, s);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(ds, ss->step_done, 0);
+        if (err != cudaSuccess) return err;
+      }
+      err = launch_dft_sample(ds, dd, samples, step - batch_start);
       if (err != cudaSuccess) return err;
+      if (ss) {
+        err = cudaEventRecord(ss->sample_done[step & 1], ds);
+        if (err != cudaSuccess) return err;
+      }
       if (step - batch_start + 1 == p.dft.batch || step == p.nsteps - 1) {
-        err = launch_dft_flush(s, dd, samples, counter, batch_start, step - batch_start + 1);
+        err = launch_dft_flush(ds, dd, samples, counter, batch_start, step - batch_start + 1);
         if (err != cudaSuccess) return err;
         batch_start = step + 1;
       }
@@ -430,6 +518,11 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
       err = launch_dft(s, make_dft(p, b), counter, step);
       if (err != cudaSuccess) return err;
     }
+  }
+  if (ss) {  // join: the flush reads the step counter, and callers read the arena
+    cudaError_t err = cudaEventRecord(ss->joined, ds);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(s, ss->joined, 0);
+    if (err != cudaSuccess) return err;
   }
   if (p.nsteps > 0) return launch_counter_advance(s, static_cast<int*>(p.step_counter.data), p.nsteps);
   return cudaSuccess;
@@ -462,6 +555,11 @@ cudaError_t launch_with_graph(cudaStream_t s, const FdtdProgram& p) {
   cudaError_t err = cudaStreamIsCapturing(s, &status);
   if (err != cudaSuccess) return err;
   if (status != cudaStreamCaptureStatusNone || s == nullptr) return enqueue_program(s, p);
+  if (wants_side_stream(p)) {
+    SideStream* ss = nullptr;
+    err = side_stream_of(s, true, &ss);
+    if (err != cudaSuccess) return err;
+  }
   const std::string key = graph_key(p, s);
   GraphCache& gc = cache();
   std::lock_guard<std::mutex> lock(gc.mu);
@@ -495,6 +593,11 @@ cudaError_t launch_with_graph(cudaStream_t s, const FdtdProgram& p) {
 
 // Capture one program into a caller-owned executable graph.
 cudaError_t capture_program(cudaStream_t s, const FdtdProgram& p, cudaGraphExec_t* out) {
+  if (wants_side_stream(p)) {
+    SideStream* ss = nullptr;
+    const cudaError_t e = side_stream_of(s, true, &ss);
+    if (e != cudaSuccess) return e;
+  }
   cudaError_t err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (err != cudaSuccess) return err;
   const cudaError_t enq = enqueue_program(s, p);

@@ -476,6 +476,38 @@ def plane_monitor(grid_shape, resolution, normal_axis, position, coords_a, coord
     return DftMonitorPlan(np.asarray(freqs, np.float32), idx, w, mask, **kwargs)
 
 
+def sources_clear_of_monitors(spec) -> bool:
+    """True when no pre-E source cell is read by a DFT monitor's gather (same
+    component, nonzero weight, component not masked off).
+
+    A pre-E source writes the bank that the previous step's DFT sample reads,
+    so only then may that sample run beside the next step."""
+    boxes: dict = {}
+    for src in spec.sources:
+        if src.timing != "pre_e":
+            continue
+        ext = (1,) * (len(spec.grid_shape) - np.ndim(src.coeff)) + tuple(np.shape(src.coeff))
+        boxes.setdefault(src.component, []).append((tuple(int(v) for v in src.start), ext))
+    if not boxes:
+        return True
+    for mon in spec.monitors:
+        for ci, c in enumerate(COMPONENTS):
+            if c not in boxes or float(mon.component_mask[ci]) == 0.0:
+                continue
+            idx = np.asarray(mon.indices[ci])
+            flat = idx[np.asarray(mon.weights[ci]) != 0]
+            if flat.size == 0:
+                continue
+            coords = np.unravel_index(flat.astype(np.int64), component_shape(c, spec.grid_shape, spec.polarization))
+            for start, ext in boxes[c]:
+                inside = np.ones(flat.shape, bool)
+                for a, (lo, n) in enumerate(zip(start, ext)):
+                    inside &= (coords[a] >= lo) & (coords[a] < lo + n)
+                if inside.any():
+                    return False
+    return True
+
+
 def step_times(t0: float, dt: float, nsteps: int) -> np.ndarray:
     """t + dt after each step, accumulated in float32 like beamz's clock
     (beamz/simulation/execute.py:524-541)."""

@@ -29,6 +29,7 @@ from .plan import (
     codebook_tables,
     compact_materials,
     component_shape,
+    sources_clear_of_monitors,
     step_times,
 )
 
@@ -170,7 +171,7 @@ class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
     def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
-                 graphs=True, layout="auto", dft_batch: int = 8):
+                 graphs=True, layout="auto", dft_batch: int = 8, dft_overlap: bool = True):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
         torch = _torch()
@@ -232,6 +233,9 @@ class DeviceProgram:
         # DFT samples are buffered and added to the arena every `dft_batch` steps
         # (bit-identical to per-step accumulation; 1 disables the buffer).
         self.dft_batch = max(1, min(16, int(dft_batch)))
+        # ... and the sample of step n runs on a side stream beside step n+1
+        # when no pre-E source writes a gathered cell (bit-identical either way).
+        self.dft_overlap = bool(dft_overlap) and schedule == "fused" and sources_clear_of_monitors(spec)
         self.e_source = {}  # per-site E source coefficients (site material), by component
 
         def buf(t):
@@ -355,6 +359,8 @@ class DeviceProgram:
             if state.dft_samples is not None:
                 s.dft.batch = self.dft_batch
                 s.dft.samples = abi.buffer_of(state.dft_samples)
+                if self.dft_overlap:
+                    s.flags |= abi.FDTD_FLAG_DFT_OVERLAP
         s.step_counter = abi.buffer_of(state.counter)
         s.step_time = abi.buffer_of(self.step_time)
         s.status = abi.buffer_of(state.status)

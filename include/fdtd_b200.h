@@ -36,6 +36,11 @@ enum {
 
 /* Flags (beamz: abi_layout.json "flags"; bit 7 keeps its meaning). */
 #define FDTD_FLAG_GRAPH_CACHE (1 << 7) /* capture multi-step programs into CUDA graphs */
+/* Batched DFT sampling of step n runs on a side stream, beside step n+1 (no
+ * counterpart in beamz).  Set it only when no pre-E source cell is gathered by
+ * a monitor: a pre-E source writes the bank that the previous step's sample
+ * reads.  One host thread per caller stream. */
+#define FDTD_FLAG_DFT_OVERLAP (1 << 16)
 
 /* Step schedules. */
 enum {

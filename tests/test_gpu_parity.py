@@ -279,6 +279,27 @@ def test_fields_are_bit_identical_to_the_fp32_oracle(case, schedule):
         assert O.relative_l2(mine, ref) <= DFT_TOL
 
 
+@pytest.mark.parametrize("graphs", [True, False])
+def test_dft_sampling_beside_the_next_step_is_bit_identical(graphs):
+    """Samples taken on a side stream while the next step runs give the same
+    arena and fields, bit for bit, as samples taken in line, over two calls."""
+    from beamz_b200 import workloads as W
+
+    spec = W.scene_3d_512(total_steps=60, shape=(40, 48, 96), pml_cells=6)
+    outs = []
+    for overlap in (False, True):
+        prog = R.compile_program(spec, dft_overlap=overlap, graphs=graphs)
+        assert prog.dft_overlap == overlap
+        st = R.initial_state(prog)
+        R.run_steps(st, prog, 23)
+        R.run_steps(st, prog, 18)
+        st.check()
+        outs.append(st.numpy())
+    for key in ("dft_re", "dft_im", "dft_w", "Ey", "Hz"):
+        np.testing.assert_array_equal(outs[1][key], outs[0][key], err_msg=key)
+    assert np.abs(outs[1]["dft_re"]).max() > 0
+
+
 @pytest.mark.parametrize("dims", [3, 2])
 def test_dft_step_batching_is_bit_identical(dims):
     """Samples buffered and flushed every few steps (and at every call's end)

@@ -137,3 +137,26 @@ def test_codebook_overflow_is_reported():
     ids = np.arange(60, dtype=np.uint8).reshape(3, 4, 5)
     with pytest.raises(P.CodebookOverflow):
         P.site_codebook(ids, np.linspace(1, 9, 60).astype(np.float32), np.float32(1.0))
+
+
+def test_sources_clear_of_monitors():
+    """The DFT sample of a step may run beside the next step only when no
+    pre-E source writes a cell that a monitor gathers."""
+    import dataclasses
+
+    from beamz_b200 import workloads as W
+
+    spec = W.scene_3d_512(total_steps=10, shape=(24, 32, 40), pml_cells=3)
+    assert P.sources_clear_of_monitors(spec)
+    mon = spec.monitors[0]
+    ci = P.COMPONENTS.index("Ey")
+    flat = int(np.asarray(mon.indices[ci])[np.asarray(mon.weights[ci]) != 0][0])
+    cell = tuple(int(v) for v in np.unravel_index(flat, P.component_shape("Ey", spec.grid_shape)))
+
+    def with_source(component, timing):
+        src = P.SourcePlan(component, timing, cell, np.ones((1, 1, 1), np.float32), np.zeros(4, np.float32))
+        return dataclasses.replace(spec, sources=list(spec.sources) + [src])
+
+    assert not P.sources_clear_of_monitors(with_source("Ey", "pre_e"))
+    assert P.sources_clear_of_monitors(with_source("Ey", "e"))  # written before the sample is taken
+    assert P.sources_clear_of_monitors(with_source("Ex", "pre_e"))  # Ex is masked off on these planes
