@@ -20,9 +20,10 @@
 //      on another; barrier;
 //   4. E(k) on the own cells from H(k) and H(k-1) (double-buffered in shared
 //      memory).
-// A tile-plane clear of every domain face, absorber slab and H source runs a
-// straight-line body; all others run the general one (ghost planes, PEC, CPML
-// with both operands of a component fetched before use, H sources, validity).
+// A tile-plane clear of the high domain faces and of H sources runs one of six
+// straight-line bodies (by the absorber axes it touches); all others run the
+// general one (ghost planes, PEC, CPML with both operands of a component
+// fetched before use, H sources, validity).
 // TMA zero-fills outside each array's extent.  Fields and the H-term CPML
 // memories are double-banked (read A, write B); E-term memories stay in
 // place.  Every mbarrier wait is bounded: on expiry the kernel records an
@@ -413,8 +414,11 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
       // ghost value by select; column X (xcol) is the last warp's extra work.
       // CPML terms run only for the axes whose slabs the tile-plane touches,
       // chosen at compile time: AX, AY, AZ.
-      auto body = [&](auto axc, auto ayc, auto azc) {
+      auto body = [&](auto axc, auto ayc, auto azc, auto fc) {
         constexpr bool AX = decltype(axc)::value, AY = decltype(ayc)::value, AZ = decltype(azc)::value;
+        // FC: the tile may touch the faces x = 0 / y = 0 (else their selects drop).
+        constexpr bool FC = decltype(fc)::value;
+        const bool at_x0 = FC && xface, at_y0 = FC && yface;
         int zh1 = -1, zh2 = -1, ze1 = -1, ze2 = -1;  // plane-uniform z slots
         if constexpr (AZ) {
           zh1 = cpml_slot(p.ht[1], k);
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
             if constexpr (AY) d0 = psi_apply(p.ht[0], sm.cc[0], q0, d0, own);
             if constexpr (AZ) d1 = psi_apply(p.ht[1], sm.cc[1], q1, d1, own);
             const float h = hf.dec0 * HOx[b] - hf.src0 * (d0 - d1);
-            hv[0] = ((xface && ii == 0 && wx0) || (ii == X && wx1)) ? 0.0f : h;
+            hv[0] = ((at_x0 && ii == 0 && wx0) || (ii == X && wx1)) ? 0.0f : h;
           }
           if constexpr ((W & 2) != 0) {  // Hy: dEx/dz - dEz/dx
             float d0 = div_rn(E1x[b] - E0x[b], res, inv_res);
@@ -446,7 +450,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
             if constexpr (AZ) d0 = psi_apply(p.ht[2], sm.cc[2], q2, d0, own);
             if constexpr (AX) d1 = psi_apply(p.ht[3], sm.cc[3], q3, d1, own);
             const float h = hf.dec1 * HOy[b] - hf.src1 * (d0 - d1);
-            hv[1] = (yface && j == 0 && wy0) ? 0.0f : h;
+            hv[1] = (at_y0 && j == 0 && wy0) ? 0.0f : h;
           }
           if constexpr ((W & 4) != 0) {  // Hz: dEy/dx - dEx/dy
             float d0 = div_rn(E0y[b + 1] - E0y[b], res, inv_res);
@@ -471,8 +475,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
             const float2 d1 = f2div(f2sub(make_float2(E1y[b], E0z[b + 1]), make_float2(E0y[b], E0z[b])), r2, nb2);
             const float2 cd = f2sub(d0, d1);
             const float hx = hf.dec0 * HOx[b] - hf.src0 * cd.x, hy = hf.dec1 * HOy[b] - hf.src1 * cd.y;
-            hv[0] = (xface && i == 0 && wx0) ? 0.0f : hx;
-            hv[1] = (yface && j == 0 && wy0) ? 0.0f : hy;
+            hv[0] = (at_x0 && i == 0 && wx0) ? 0.0f : hx;
+            hv[1] = (at_y0 && j == 0 && wy0) ? 0.0f : hy;
             hv[2] = hf.dec2 * HOz[b] - hf.src2 * (div_rn(E0y[b + 1] - E0y[b], res, inv_res) -
                                                   div_rn(E0x[b + BX] - E0x[b], res, inv_res));
           } else {
@@ -489,19 +493,19 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
           }
         }
         if (warp == 0) {  // y-halo row: Hx, Hz
-          if (!yface) {
+          if (!at_y0) {
             float hv[3];
             h_cell(W5{}, lane + 4, j0 - 1, i, false, hv);
             sm.hn[hb][0][0][1 + lane] = hv[0];
             sm.hn[hb][2][0][1 + lane] = hv[2];
           }
-        } else if (warp == 1 && lane < T::TY && !xface) {  // x-halo column: Hy, Hz
+        } else if (warp == 1 && lane < T::TY && !at_x0) {  // x-halo column: Hy, Hz
           float hv[3];
           h_cell(W6{}, (1 + lane) * BX + 3, j0 + lane, i0 - 1, false, hv);
           sm.hn[hb][1][1 + lane][0] = hv[1];
           sm.hn[hb][2][1 + lane][0] = hv[2];
         }
-        if (xcol && warp == NW - 1 && lane <= T::TY && !(yface && lane == 0)) {  // Hx on column X
+        if (xcol && warp == NW - 1 && lane <= T::TY && !(at_y0 && lane == 0)) {  // Hx on column X
           float hv[3];
           const int j = j0 - 1 + lane;
           h_cell(W1{}, lane * BX + T::TX + 4, j, X, emit && lane >= 1, hv);
@@ -517,7 +521,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
           const float hz_x = sm.hn[hb][2][ly][T::TX], hy_x = sm.hn[hb][1][ly][T::TX];
           // Ghost beyond x = X: zero on a metallic wall, else the edge value.
           const float hz = wx1 ? 0.0f : hz_x, hy = wx1 ? 0.0f : hy_x;
-          const bool y0 = yface && j == 0;
+          const bool y0 = at_y0 && j == 0;
           if (y0) hx_y = wy0 ? 0.0f : hx;
           Psi q2, q3, q4, q5;
           if constexpr (AZ) q2 = psi_fetch<0>(p.et[2], ze2, k, j, X);
@@ -549,7 +553,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
           const float hy_z = sm.hn[pb][1][ly][lx], hx_z = sm.hn[pb][0][ly][lx];
           float hz_x = sm.hn[hb][2][ly][lx - 1], hy_x = sm.hn[hb][1][ly][lx - 1];
           float hz_y = sm.hn[hb][2][ly - 1][lx], hx_y = sm.hn[hb][0][ly - 1][lx];
-          const bool x0 = xface && i == 0, y0 = yface && j == 0;
+          const bool x0 = at_x0 && i == 0, y0 = at_y0 && j == 0;
           if (x0) {  // ghost beyond x = 0: zero on a metallic wall, else the edge value
             hz_x = wx0 ? 0.0f : hz;
             hy_x = wx0 ? 0.0f : hy;
@@ -603,19 +607,24 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
           }
         }
       };
+      // Six straight variants, each inlined once: the interior with and
+      // without the low faces, one absorbing axis (x, y or z), and every
+      // tile-plane whose slabs span two or three axes (rare: edges and
+      // corners) through the all-axes body; fewer bodies keep the hot code
+      // small for the instruction cache.
       if constexpr (!Cpml) {
-        body(kOff{}, kOff{}, kOff{});
+        if (xface || yface) body(kOff{}, kOff{}, kOff{}, kOn{});
+        else body(kOff{}, kOff{}, kOff{}, kOff{});
       } else {
         const bool az = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
-        switch ((ax ? 4 : 0) | (ay ? 2 : 0) | (az ? 1 : 0)) {
-          case 0: body(kOff{}, kOff{}, kOff{}); break;
-          case 1: body(kOff{}, kOff{}, kOn{}); break;
-          case 2: body(kOff{}, kOn{}, kOff{}); break;
-          case 3: body(kOff{}, kOn{}, kOn{}); break;
-          case 4: body(kOn{}, kOff{}, kOff{}); break;
-          case 5: body(kOn{}, kOff{}, kOn{}); break;
-          case 6: body(kOn{}, kOn{}, kOff{}); break;
-          default: body(kOn{}, kOn{}, kOn{}); break;
+        const int v = (ax ? 4 : 0) | (ay ? 2 : 0) | (az ? 1 : 0);
+        switch (v == 3 || v == 5 || v == 6 ? 7 : (v == 0 && !(xface || yface) ? 8 : v)) {
+          case 8: body(kOff{}, kOff{}, kOff{}, kOff{}); break;
+          case 0: body(kOff{}, kOff{}, kOff{}, kOn{}); break;
+          case 1: body(kOff{}, kOff{}, kOn{}, kOn{}); break;
+          case 2: body(kOff{}, kOn{}, kOff{}, kOn{}); break;
+          case 4: body(kOn{}, kOff{}, kOff{}, kOn{}); break;
+          default: body(kOn{}, kOn{}, kOn{}, kOn{}); break;
         }
       }
     } else {
