@@ -16,8 +16,8 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 5
-FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8 = 0, 1, 2, 3
+FDTD_ABI_VERSION = 6
+FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
@@ -27,6 +27,7 @@ FDTD_TIMING_PRE_E, FDTD_TIMING_H, FDTD_TIMING_E = 0, 1, 2
 FDTD_MAX_SOURCES = 16
 FDTD_MAX_MONITORS = 16
 FDTD_ADJOINT_NOALLOC_MAX_FLOATS = 4 * 1024 * 1024
+FDTD_DIAG_BLOCKS = 592
 TIMINGS = {"pre_e": FDTD_TIMING_PRE_E, "h": FDTD_TIMING_H, "e": FDTD_TIMING_E}
 # Wall bits (front, back, bottom, top, left, right), beamz/simulation/cuda/runtime.py:38-40.
 EDGE_BITS = {"front": 0, "back": 1, "bottom": 2, "top": 3, "left": 4, "right": 5}
@@ -43,6 +44,8 @@ EXPORTED_SYMBOLS = (
     "fdtd_copy_component",
     "fdtd_adjoint_step",
     "fdtd_adjoint_curl",
+    "fdtd_field_diagnostics",
+    "fdtd_dft_change",
     "fdtd_adjoint_step_noalloc",
     "fdtd_graph_create",
     "fdtd_graph_launch",
@@ -133,6 +136,19 @@ class FdtdAdjointStep(ctypes.Structure):
     ]
 
 
+class FdtdDiagnostics(ctypes.Structure):
+    _fields_ = [
+        ("site_eps_table", FdtdBuffer),
+        ("site_eps", FdtdBuffer * 3),
+        ("partials", FdtdBuffer),
+        ("out", FdtdBuffer),
+    ]
+
+
+class FdtdDftChange(ctypes.Structure):
+    _fields_ = [("prev_re", FdtdBuffer), ("prev_im", FdtdBuffer), ("out", FdtdBuffer)]
+
+
 class FdtdRegistration(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char_p), ("fn", ctypes.c_void_p)]
 
@@ -192,7 +208,7 @@ def buffer_of(tensor) -> FdtdBuffer:
 
     if _TORCH_DTYPES is None:
         _TORCH_DTYPES = {torch.float32: FDTD_F32, torch.int32: FDTD_S32, torch.bfloat16: FDTD_BF16,
-                         torch.uint8: FDTD_U8}
+                         torch.uint8: FDTD_U8, torch.float64: FDTD_F64}
     buf = FdtdBuffer()
     if tensor is None:
         return buf
@@ -253,6 +269,11 @@ def load_library(path: str | None = None):
         lib.fdtd_adjoint_step_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram),
                                                   ctypes.POINTER(FdtdAdjointStep)]
         lib.fdtd_adjoint_step_noalloc.restype = ctypes.c_int
+        lib.fdtd_field_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram),
+                                               ctypes.POINTER(FdtdDiagnostics)]
+        lib.fdtd_field_diagnostics.restype = ctypes.c_int
+        lib.fdtd_dft_change.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(FdtdDftChange)]
+        lib.fdtd_dft_change.restype = ctypes.c_int
         lib.fdtd_graph_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(ctypes.c_void_p)]
         lib.fdtd_graph_create.restype = ctypes.c_int
         lib.fdtd_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]

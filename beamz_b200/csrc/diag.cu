@@ -1,0 +1,175 @@
+// Device reductions behind automatic termination: field diagnostics
+// (integrated energy, largest |field|, non-finite count) and the change of
+// each DFT monitor vector between checks.
+//
+// beamz evaluates both between run chunks with jnp reductions
+// (beamz/simulation/execute.py:184-222 _field_diagnostics, 294-316
+// _relative_monitor_change, driven by run_until_terminated 1312-1484).  Here
+// each is a bandwidth-bound read of the fields or the arena: coalesced row
+// sweeps, per-thread double accumulators, warp-shuffle and shared-memory
+// block reductions, and a fixed partition and summation order, so a result
+// is identical from run to run.
+
+#include "kernels.cuh"
+
+namespace fdtd {
+
+namespace {
+
+constexpr int kDiagThreads = 256;
+constexpr int kDiagWarps = kDiagThreads / 32;
+
+__device__ __forceinline__ void warp_reduce(double& s, float& m, unsigned& n) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+    n += __shfl_down_sync(0xffffffffu, n, o);
+  }
+}
+
+// Block reduction of (sum, max, count); the result is valid in thread 0.
+__device__ __forceinline__ void block_reduce(double& s, float& m, unsigned& n) {
+  __shared__ double ss[kDiagWarps];
+  __shared__ float sm[kDiagWarps];
+  __shared__ unsigned sn[kDiagWarps];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  warp_reduce(s, m, n);
+  if (l == 0) {
+    ss[w] = s;
+    sm[w] = m;
+    sn[w] = n;
+  }
+  __syncthreads();
+  if (w == 0) {
+    s = l < kDiagWarps ? ss[l] : 0.0;
+    m = l < kDiagWarps ? sm[l] : 0.0f;
+    n = l < kDiagWarps ? sn[l] : 0u;
+    warp_reduce(s, m, n);
+  }
+}
+
+// Block b of component c sweeps rows (k, j) = b, b + gridDim.x, ... of the
+// component's stored extents, threads striding along x.
+__global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(DiagArgs a) {
+  const int c = blockIdx.y;
+  double s = 0.0;
+  float mx = 0.0f;
+  unsigned bad = 0;
+  if ((a.active >> c) & 1) {
+    const DiagComp& q = a.comp[c];
+    const int64_t rows = static_cast<int64_t>(q.d.z) * q.d.y;
+    for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+      const int k = static_cast<int>(r / q.d.y), j = static_cast<int>(r % q.d.y);
+      double hzy = 1.0;
+      if (q.integrate_z && q.edge_z && (k == 0 || k == q.d.z - 1)) hzy *= 0.5;
+      if (q.edge_y && (j == 0 || j == q.d.y - 1)) hzy *= 0.5;
+      const float* row = q.field + k * q.plane + j * q.row;
+      const uint32_t* ids = q.ids ? q.ids + k * q.plane + j * q.row : nullptr;
+      const float* eps = q.eps ? q.eps + (static_cast<int64_t>(k) * q.d.y + j) * q.d.x : nullptr;
+      for (int i = threadIdx.x; i < q.d.x; i += kDiagThreads) {
+        const float v = row[i];
+        if (!isfinite(v)) {
+          ++bad;
+          continue;
+        }
+        mx = fmaxf(mx, fabsf(v));
+        double e = 1.0;
+        if (ids) e = q.table[(ids[i] >> q.shift) & 0xffu];
+        else if (eps) e = eps[i];
+        const double h = q.edge_x && (i == 0 || i == q.d.x - 1) ? 0.5 * hzy : hzy;
+        const double dv = v;
+        s += e * dv * dv * h;
+      }
+    }
+  }
+  block_reduce(s, mx, bad);
+  if (threadIdx.x == 0) {
+    double* o = a.partials + (static_cast<int64_t>(c) * gridDim.x + blockIdx.x) * 3;
+    o[0] = s;
+    o[1] = mx;
+    o[2] = bad;
+  }
+}
+
+// One block per component: the partials in block order.
+__global__ void __launch_bounds__(kDiagThreads) diag_final_kernel(const double* partials, int blocks, double* out) {
+  const int c = blockIdx.x;
+  double s = 0.0;
+  float mx = 0.0f;
+  unsigned bad = 0;
+  for (int b = threadIdx.x; b < blocks; b += kDiagThreads) {
+    const double* o = partials + (static_cast<int64_t>(c) * blocks + b) * 3;
+    s += o[0];
+    mx = fmaxf(mx, static_cast<float>(o[1]));
+    bad += static_cast<unsigned>(o[2]);
+  }
+  block_reduce(s, mx, bad);
+  if (threadIdx.x == 0) {
+    out[c * 3 + 0] = s;
+    out[c * 3 + 1] = mx;
+    out[c * 3 + 2] = bad;
+  }
+}
+
+// One block per (monitor, component, frequency): squared norms of the change,
+// the current and the previous vector, then prev <- current.
+__global__ void __launch_bounds__(kDiagThreads) dft_change_kernel(DftDev d, float* prev_re, float* prev_im,
+                                                                  double* out) {
+  const int key = blockIdx.x;
+  const int f = key % d.max_freqs, mc = key / d.max_freqs;
+  const int m = mc / 6, c = mc % 6;
+  const int* cnt = d.counts + 5 * m;
+  const int nf = min(max(cnt[0], 0), d.max_freqs);
+  const int np = min(max(cnt[1], 0), d.max_points);
+  const int voff = cnt[3];
+  double dd = 0.0, cc = 0.0, pp = 0.0;
+  const bool on = d.masks[m * 6 + c] != 0.0f && f < nf && voff >= 0 &&
+                  voff + static_cast<int64_t>(6) * nf * np <= d.arena_len;
+  if (on) {
+    const int64_t base = voff + (static_cast<int64_t>(c) * nf + f) * np;
+    for (int p = threadIdx.x; p < np; p += kDiagThreads) {
+      const float re = d.re[base + p], im = d.im[base + p];
+      const double dr = static_cast<double>(re) - prev_re[base + p], di = static_cast<double>(im) - prev_im[base + p];
+      const double pr = prev_re[base + p], pi = prev_im[base + p];
+      dd += dr * dr + di * di;
+      cc += static_cast<double>(re) * re + static_cast<double>(im) * im;
+      pp += pr * pr + pi * pi;
+      prev_re[base + p] = re;
+      prev_im[base + p] = im;
+    }
+  }
+  // Three block sums in sequence; each total lands in thread 0's variable and
+  // stays there through the later reductions.
+  float unused = 0.0f;
+  unsigned none = 0;
+  block_reduce(dd, unused, none);
+  __syncthreads();
+  block_reduce(cc, unused, none);
+  __syncthreads();
+  block_reduce(pp, unused, none);
+  if (threadIdx.x == 0) {
+    out[key * 3 + 0] = dd;
+    out[key * 3 + 1] = cc;
+    out[key * 3 + 2] = pp;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_field_diagnostics(cudaStream_t s, const DiagArgs& a, double* out) {
+  diag_partial_kernel<<<dim3(FDTD_DIAG_BLOCKS, 6, 1), kDiagThreads, 0, s>>>(a);
+  cudaError_t err = cudaPeekAtLastError();
+  if (err != cudaSuccess) return err;
+  diag_final_kernel<<<6, kDiagThreads, 0, s>>>(a.partials, FDTD_DIAG_BLOCKS, out);
+  return cudaPeekAtLastError();
+}
+
+cudaError_t launch_dft_change(cudaStream_t s, const DftDev& d, float* prev_re, float* prev_im, double* out) {
+  const int keys = d.monitor_count * 6 * d.max_freqs;
+  if (keys <= 0) return cudaSuccess;
+  dft_change_kernel<<<keys, kDiagThreads, 0, s>>>(d, prev_re, prev_im, out);
+  return cudaPeekAtLastError();
+}
+
+}  // namespace fdtd

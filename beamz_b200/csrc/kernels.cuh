@@ -144,4 +144,26 @@ struct DftDev {
   float dt;
 };
 
+// Field diagnostics (diag.cu): one component's view.
+struct DiagComp {
+  const float* field = nullptr;   // stored array (dense, or pitched rows)
+  Dims d{};                       // stored extents (z, y, x)
+  int64_t row = 0, plane = 0;     // element strides of the field and of ids
+  int edge_z = 0, edge_y = 0, edge_x = 0;  // axis extent n + 1: its end sites weigh 1/2
+  int integrate_z = 0;            // 3D: the z axis is integrated
+  const uint32_t* ids = nullptr;  // codebook words (pitched); id byte at `shift`
+  int shift = 0;
+  const float* table = nullptr;   // 256 relative permittivities of the ids
+  const float* eps = nullptr;     // per-site relative permittivity, dense over d
+};
+
+struct DiagArgs {
+  DiagComp comp[6];
+  int active = 0;                 // bit c: component c is reduced
+  double* partials = nullptr;     // [6][FDTD_DIAG_BLOCKS][3]
+};
+
+cudaError_t launch_field_diagnostics(cudaStream_t s, const DiagArgs& a, double* out);
+cudaError_t launch_dft_change(cudaStream_t s, const DftDev& d, float* prev_re, float* prev_im, double* out);
+
 }  // namespace fdtd

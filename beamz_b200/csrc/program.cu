@@ -846,6 +846,72 @@ int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjoin
       fdtd::launch_adjoint_curl(static_cast<cudaStream_t>(stream), sp, fdtd::adjoint_dev(p, *a), L.active));
 }
 
+int fdtd_field_diagnostics(void* stream, const FdtdProgram* program, const FdtdDiagnostics* d) {
+  if (program == nullptr || d == nullptr) return fdtd::kInvalid;
+  const FdtdProgram& p = *program;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  auto f64_at_least = [](const FdtdBuffer& b, int64_t n) {
+    return b.element_type == FDTD_F64 && b.data != nullptr && fdtd::elements(b) >= n;
+  };
+  if (!f64_at_least(d->partials, int64_t{6} * FDTD_DIAG_BLOCKS * 3) || !f64_at_least(d->out, 18))
+    return fdtd::kInvalid;
+  const bool pitched = p.layout == FDTD_LAYOUT_PITCHED;
+  const bool codebook = p.material_kind == FDTD_MATERIAL_CODEBOOK;
+  if (codebook && (!fdtd::is_f32(d->site_eps_table) || d->site_eps_table.data == nullptr ||
+                   fdtd::elements(d->site_eps_table) != 3 * 256))
+    return fdtd::kInvalid;
+  fdtd::DiagArgs a;
+  a.active = L.active;
+  a.partials = static_cast<double*>(d->partials.data);
+  for (int c = 0; c < 6; ++c) {
+    if (!((L.active >> c) & 1)) continue;
+    fdtd::DiagComp& q = a.comp[c];
+    q.field = static_cast<const float*>(p.fields[c].data);
+    q.d = fdtd::component_dims(c, L.Z, L.Y, L.X);
+    q.row = pitched ? p.pitch : q.d.x;
+    q.plane = pitched ? static_cast<int64_t>(L.Y + 1) * p.pitch : static_cast<int64_t>(q.d.y) * q.d.x;
+    q.integrate_z = p.ndim == 3 ? 1 : 0;
+    q.edge_z = q.d.z == L.Z + 1 ? 1 : 0;
+    q.edge_y = q.d.y == L.Y + 1 ? 1 : 0;
+    q.edge_x = q.d.x == L.X + 1 ? 1 : 0;
+    if (c >= 3) continue;  // non-magnetic: mu_r = 1
+    if (codebook) {
+      q.ids = static_cast<const uint32_t*>(p.site_ids.data);
+      q.shift = 8 * c;
+      q.table = static_cast<const float*>(d->site_eps_table.data) + 256 * c;
+    } else if (d->site_eps[c].data != nullptr) {
+      const int64_t n = static_cast<int64_t>(q.d.z) * q.d.y * q.d.x;
+      if (!fdtd::is_f32(d->site_eps[c]) || d->site_eps[c].data == nullptr || fdtd::elements(d->site_eps[c]) != n)
+        return fdtd::kInvalid;
+      q.eps = static_cast<const float*>(d->site_eps[c].data);
+    }
+  }
+  return static_cast<int>(
+      fdtd::launch_field_diagnostics(static_cast<cudaStream_t>(stream), a, static_cast<double*>(d->out.data)));
+}
+
+int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChange* c) {
+  if (program == nullptr || c == nullptr) return fdtd::kInvalid;
+  const FdtdProgram& p = *program;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  if (p.dft.monitor_count <= 0) return fdtd::kInvalid;
+  const int64_t arena = fdtd::elements(p.dft.re);
+  for (const FdtdBuffer* b : {&c->prev_re, &c->prev_im})
+    if (!fdtd::is_f32(*b) || b->data == nullptr || fdtd::elements(*b) != arena) return fdtd::kInvalid;
+  const fdtd::DftDev dd = fdtd::make_dft(p, p.fields);
+  const int64_t keys = static_cast<int64_t>(dd.monitor_count) * 6 * dd.max_freqs;
+  if (c->out.element_type != FDTD_F64 || c->out.data == nullptr || fdtd::elements(c->out) < keys * 3)
+    return fdtd::kInvalid;
+  return static_cast<int>(fdtd::launch_dft_change(static_cast<cudaStream_t>(stream), dd,
+                                                  static_cast<float*>(c->prev_re.data),
+                                                  static_cast<float*>(c->prev_im.data),
+                                                  static_cast<double*>(c->out.data)));
+}
+
 int fdtd_graph_create(void* stream, const FdtdProgram* program, void** graph) {
   if (program == nullptr || graph == nullptr || stream == nullptr || program->nsteps < 1) return fdtd::kInvalid;
   *graph = nullptr;

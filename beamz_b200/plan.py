@@ -270,7 +270,7 @@ def edge_replicated(compact: np.ndarray) -> np.ndarray:
     return np.pad(compact, 1, mode="edge")
 
 
-def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict):
+def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict, with_eps: bool = False):
     """Per-component lookup tables from tuple key to codebook id, and the
     coefficient tables.
 
@@ -278,7 +278,9 @@ def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict):
     ``present[c]`` flags which of the m**4 keys occur.  Returns ``(luts, coef)``:
     ``luts[c]`` is a uint8 array of m**4 ids (0 where a key is absent) and
     ``coef`` the float32 (3, 256) tables.  Raises :class:`CodebookOverflow` when
-    a component has more than 256 distinct coefficients.
+    a component has more than 256 distinct coefficients.  With ``with_eps``
+    also returns the float32 (3, 256) site permittivities of the ids (an id's
+    sites share one coefficient; the table keeps one of their permittivities).
     """
     f32 = np.float32
     e = np.asarray(eps_used, f32)
@@ -287,7 +289,7 @@ def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict):
     b = half * (e[None, None, :, None] + e[None, None, None, :])
     eps_site = (half * (a + b)).reshape(-1)
     coef_all = f32(dt_over_eps) * (f32(1.0) / eps_site)
-    luts, coef = {}, np.zeros((3, 256), f32)
+    luts, coef, eps = {}, np.zeros((3, 256), f32), np.ones((3, 256), f32)
     for n, c in enumerate(("Ex", "Ey", "Ez")):
         mask = np.asarray(present[c], bool)
         values, inverse = np.unique(coef_all[mask], return_inverse=True)
@@ -297,7 +299,8 @@ def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict):
         lut[mask] = inverse.astype(np.uint8)
         luts[c] = lut
         coef[n, : values.size] = values
-    return luts, coef
+        eps[n, inverse] = eps_site[mask]
+    return (luts, coef, eps) if with_eps else (luts, coef)
 
 
 def compact_materials(voxel_ids: np.ndarray, eps_table: np.ndarray):
@@ -334,6 +337,21 @@ def site_codebook(voxel_ids: np.ndarray, eps_table: np.ndarray, dt_over_eps):
     for shift, c in ((0, "Ex"), (8, "Ey"), (16, "Ez")):
         words |= luts[c][keys[c]].astype(np.int32) << shift
     return words, coef
+
+
+def site_eps_3d(voxel_ids: np.ndarray, eps_table: np.ndarray, component: str) -> np.ndarray:
+    """float32 E-site permittivity of one component over its stored shape: the
+    same four-voxel average as the codebook (beamz/lattice.py:732-786)."""
+    f32 = np.float32
+    table = np.ones(256, f32)
+    table[: len(eps_table)] = np.asarray(eps_table, f32)
+    vp = edge_replicated(table[np.asarray(voxel_ids, np.uint8)])
+    nz, ny, nx = (int(v) for v in np.shape(voxel_ids))
+    t = [vp[dk:dk + nz + 1, dj:dj + ny + 1, di:di + nx + 1] for dk, dj, di in CODEBOOK_TAPS[component]]
+    half = f32(0.5)
+    site = half * (half * (t[0] + t[1]) + half * (t[2] + t[3]))
+    dz, dy, dx = component_shape(component, (nz, ny, nx))
+    return np.ascontiguousarray(site[:dz, :dy, :dx], dtype=f32)
 
 
 def site_values_2d(eps_grid: np.ndarray, component: str, polarization: str = "tm") -> np.ndarray:
@@ -539,6 +557,9 @@ class ProgramSpec:
     # Per-site material: component -> (decay, source), scalars or full arrays.
     e_site: dict | None = None
     h_site: dict | None = None
+    # Relative permittivity per E site (component -> array over its stored
+    # shape), for energy diagnostics of per-site programs; optional.
+    e_site_eps: dict | None = None
     h_terms: list = field(default_factory=list)
     e_terms: list = field(default_factory=list)
     metallic_edges: frozenset = frozenset()

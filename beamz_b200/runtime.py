@@ -29,6 +29,7 @@ from .plan import (
     codebook_tables,
     compact_materials,
     component_shape,
+    site_eps_3d,
     sources_clear_of_monitors,
     step_times,
 )
@@ -71,10 +72,12 @@ def _replicated_slab(torch, ids, remap, k0: int, k1: int):
     return torch.cat([slab[:, :, :1], slab, slab[:, :, -1:]], dim=2)
 
 
-def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, z_block: int = 32):
+def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, z_block: int = 32,
+                         with_eps: bool = False):
     """Site-id words (Z+1, Y+1, pitch) int32 and coefficient tables (3, 256) on
     the device; equal bit for bit to :func:`beamz_b200.plan.site_codebook` (the
-    device part is integer gathers only; coefficients come from the host)."""
+    device part is integer gathers only; coefficients come from the host).
+    With ``with_eps`` also the (3, 256) site permittivities of the ids."""
     torch = _torch()
     remap_np, eps_used = compact_materials(voxel_ids, eps_table)
     m = int(eps_used.size)
@@ -89,7 +92,8 @@ def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, 
         for c in comps:
             keys = codebook_keys(vp, m, c, 0, k1 - k0).reshape(-1).long()
             present[c] |= torch.bincount(keys, minlength=m**4) > 0
-    luts, coef = codebook_tables(eps_used, dt_over_eps, {c: present[c].cpu().numpy() for c in comps})
+    luts, coef, eps = codebook_tables(eps_used, dt_over_eps, {c: present[c].cpu().numpy() for c in comps},
+                                      with_eps=True)
     lut = {c: torch.as_tensor(luts[c].astype(np.int32), device=device) for c in comps}
     words = torch.zeros((nz + 1, ny + 1, pitch), dtype=torch.int32, device=device)
     for k0, k1 in blocks:
@@ -97,6 +101,8 @@ def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, 
         w = words[k0:k1, :, : nx + 1]
         for shift, c in ((0, "Ex"), (8, "Ey"), (16, "Ez")):
             w |= lut[c][codebook_keys(vp, m, c, 0, k1 - k0).long()] << shift
+    if with_eps:
+        return words, torch.as_tensor(coef, device=device), torch.as_tensor(eps, device=device)
     return words, torch.as_tensor(coef, device=device)
 
 
@@ -188,14 +194,15 @@ class DeviceProgram:
             raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule and uniform H")
         f32 = np.float32
         dt_over_eps = f32(spec.dt) / f32(EPS_0)
-        self.site_ids = self.site_coef = None
+        self.site_ids = self.site_coef = self.site_eps_table = None
+        self._diag_eps = None
         if layout in ("auto", "pitched") and pitched_ok:
             nz, ny, nx = (int(v) for v in spec.grid_shape)
             self.pitch = -(-(nx + 1) // 4) * 4
             self.bank_shape = (nz + 1, ny + 1, self.pitch)
             try:
-                self.site_ids, self.site_coef = device_site_codebook(
-                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev)
+                self.site_ids, self.site_coef, self.site_eps_table = device_site_codebook(
+                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev, with_eps=True)
                 layout = "pitched"
             except CodebookOverflow:
                 if layout == "pitched":
@@ -312,6 +319,31 @@ class DeviceProgram:
         dz, dy, dx = self.shapes[COMPONENTS[c]]
         k, j, i = np.unravel_index(np.asarray(flat, np.int64), (dz, dy, dx))
         return ((k * (self.bank_shape[1]) + j) * self.pitch + i).astype(np.int32)
+
+    def diag_site_eps(self, component: str):
+        """Device relative permittivity of one E component over its stored
+        shape, for energy diagnostics of dense programs: the spec's
+        ``e_site_eps``, else the voxel sampling of the update (3D voxel
+        material), else dt / (eps0 * source) of lossless per-site material."""
+        if self._diag_eps is None:
+            self._diag_eps = {}
+        if component in self._diag_eps:
+            return self._diag_eps[component]
+        spec = self.spec
+        if spec.e_site_eps is not None and component in spec.e_site_eps:
+            eps = np.asarray(spec.e_site_eps[component], np.float32)
+        elif spec.ndim == 3 and spec.voxel_ids is not None:
+            eps = site_eps_3d(spec.voxel_ids, spec.eps_table, component)
+        elif spec.e_site is not None and component in spec.e_site:
+            decay, src = (np.asarray(v, np.float64) for v in spec.e_site[component])
+            if np.any(decay != 1.0):
+                raise ValueError(f"{component}: lossy per-site material needs e_site_eps for energy diagnostics")
+            eps = (float(spec.dt) / (EPS_0 * src)).astype(np.float32)
+        else:
+            eps = np.ones(1, np.float32)
+        eps = np.broadcast_to(eps, self.shapes[component]).astype(np.float32)
+        self._diag_eps[component] = _f32(eps, self.device)
+        return self._diag_eps[component]
 
     def view(self, bank_tensor, component: str):
         """The component's own extent inside a device field tensor."""
@@ -540,3 +572,82 @@ def run_steps(state: DeviceState, program: DeviceProgram, nsteps: int, chunk: in
 
 
 run_program_steps = run_steps
+
+
+@dataclass
+class FieldDiagnostics:
+    """Integrated electromagnetic energy (J; per metre of depth in 2D), largest
+    |field| and finiteness of a state's fields."""
+
+    energy: float
+    max_field: float
+    finite: bool
+    nonfinite: int
+
+
+def field_diagnostics(state: DeviceState, program: DeviceProgram) -> FieldDiagnostics:
+    """beamz/simulation/execute.py:184-222 (_field_diagnostics) as one device
+    reduction (fdtd_field_diagnostics): sum over components of
+    0.5 * const * sum(eps_r * v^2 * control volume), const = eps0 for E and mu0
+    for H.  Non-finite values are counted, and left out of the sum and max."""
+    torch = _torch()
+    dev = program.device
+    if getattr(state, "_diag_scratch", None) is None:
+        state._diag_scratch = (torch.empty(6 * abi.FDTD_DIAG_BLOCKS * 3, dtype=torch.float64, device=dev),
+                               torch.empty(18, dtype=torch.float64, device=dev))
+    partials, out = state._diag_scratch
+    d = abi.FdtdDiagnostics()
+    if program.layout == "pitched":
+        d.site_eps_table = abi.buffer_of(program.site_eps_table)
+    else:
+        for i, c in enumerate(("Ex", "Ey", "Ez")):
+            if c in program.active:
+                d.site_eps[i] = abi.buffer_of(program.diag_site_eps(c))
+    d.partials = abi.buffer_of(partials)
+    d.out = abi.buffer_of(out)
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_field_diagnostics(_stream(program), ctypes.byref(s), ctypes.byref(d)),
+              "fdtd_field_diagnostics")
+    r = out.cpu().numpy().reshape(6, 3)
+    volume = float(program.spec.resolution) ** program.ndim
+    energy = sum(0.5 * (EPS_0 if i < 3 else MU_0) * float(r[i, 0]) * volume
+                 for i, c in enumerate(COMPONENTS) if c in program.active)
+    nonfinite = int(r[:, 2].sum())
+    return FieldDiagnostics(float(energy), float(r[:, 1].max()), nonfinite == 0 and np.isfinite(energy), nonfinite)
+
+
+def dft_change(state: DeviceState, program: DeviceProgram, monitors=None):
+    """Largest relative change of any (monitor, component, frequency) DFT vector
+    since the previous call, and whether every monitor value is finite
+    (beamz/simulation/execute.py:294-316, _relative_monitor_change): per vector
+    |cur - prev| / max(|cur|, |prev|), 0 when both norms vanish.  The first
+    call only records the arena and returns (None, finite).  ``monitors``
+    selects monitor indices (default: every monitor)."""
+    torch = _torch()
+    if program.arena is None:
+        return None, True
+    first = getattr(state, "_dft_prev", None) is None
+    if first:
+        F = int(program.arena.freqs.shape[1])
+        state._dft_prev = (torch.zeros_like(state.dft_re), torch.zeros_like(state.dft_im),
+                           torch.empty(len(program.arena.layout) * 6 * F * 3, dtype=torch.float64,
+                                       device=program.device))
+    prev_re, prev_im, out = state._dft_prev
+    c = abi.FdtdDftChange(abi.buffer_of(prev_re), abi.buffer_of(prev_im), abi.buffer_of(out))
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_dft_change(_stream(program), ctypes.byref(s), ctypes.byref(c)), "fdtd_dft_change")
+    M = len(program.arena.layout)
+    r = out.cpu().numpy().reshape(M, 6, -1, 3)
+    chosen = range(M) if monitors is None else monitors
+    keys = [(m, ci, f) for m in chosen for ci in range(6) if program.spec.monitors[m].component_mask[ci] > 0
+            for f in range(program.arena.layout[m][1])]
+    finite = all(np.isfinite(r[k][1]) for k in keys)
+    if first:
+        return None, finite
+    tiny = np.finfo(float).tiny
+    changes = []
+    for k in keys:
+        num = float(np.sqrt(r[k][0]))
+        den = max(float(np.sqrt(r[k][1])), float(np.sqrt(r[k][2])))
+        changes.append(0.0 if den <= tiny and num <= tiny else num / den)
+    return max(changes, default=0.0), finite

@@ -24,14 +24,16 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 5
+#define FDTD_ABI_VERSION 6
 
-/* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids). */
+/* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
+ * for reduction results). */
 enum {
   FDTD_F32 = 0,
   FDTD_S32 = 1,
   FDTD_BF16 = 2,
   FDTD_U8 = 3,
+  FDTD_F64 = 4,
 };
 
 /* Flags (beamz: abi_layout.json "flags"; bit 7 keeps its meaning). */
@@ -314,6 +316,47 @@ int fdtd_adjoint_step_noalloc(void* stream, const FdtdProgram* adjoint, const Fd
 /* Write the forward curl of each active E component over `a`'s box into
  * a->curl from `forward`'s current H fields (call after a forward step). */
 int fdtd_adjoint_curl(void* stream, const FdtdProgram* forward, const FdtdAdjointStep* a);
+
+/* ---- Field diagnostics and monitor change (automatic termination) ---------
+ * beamz checks a chunked run for convergence, divergence and non-finite
+ * fields between chunks (beamz/simulation/execute.py:1312-1484): integrated
+ * electromagnetic energy, the largest |field| and finiteness of every active
+ * component (_field_diagnostics, execute.py:184-222) and the relative change
+ * of each monitor's DFT vectors (_relative_monitor_change, 294-316).  beamz
+ * reduces with jnp; these two entry points are the device reductions, each
+ * deterministic (fixed block partition, fixed summation order). */
+
+/* Reduction blocks per component of fdtd_field_diagnostics. */
+#define FDTD_DIAG_BLOCKS 592
+
+typedef struct FdtdDiagnostics {
+  FdtdBuffer site_eps_table; /* F32 [3, 256]: relative permittivity per codebook id (codebook programs) */
+  FdtdBuffer site_eps[3];    /* F32 per E component over its stored shape (other programs); empty = 1 */
+  FdtdBuffer partials;       /* F64 scratch of >= 6 * FDTD_DIAG_BLOCKS * 3 elements */
+  FdtdBuffer out;            /* F64 [6, 3]: per component sum(eps * v^2 * h), max |v|, non-finite count */
+} FdtdDiagnostics;
+
+/* Reduce the program's current fields (`fields`).  For every active component
+ * c: S_c = sum over its stored sites of eps_r * v^2 * h, where h is the
+ * product over the integrated axes (x, y and, in 3D, z) of 1/2 at the two ends
+ * of an edge-aligned axis (extent n + 1) and 1 elsewhere: beamz's control
+ * volumes (_axis_integration_weights, execute.py:75-92) divided by the cell
+ * size.  eps_r is 1 for H components.  Non-finite values are counted and left
+ * out of the sum and the maximum.  The caller forms the energy
+ * sum_c 0.5 * const_c * S_c * res^ndim (const = eps0 for E, mu0 for H). */
+int fdtd_field_diagnostics(void* stream, const FdtdProgram* program, const FdtdDiagnostics* d);
+
+typedef struct FdtdDftChange {
+  FdtdBuffer prev_re;  /* F32 [arena]: the arena at the previous check (updated to the current one) */
+  FdtdBuffer prev_im;
+  FdtdBuffer out;      /* F64 [M, 6, F, 3]: |cur - prev|^2, |cur|^2, |prev|^2 per (monitor, component, frequency) */
+} FdtdDftChange;
+
+/* Squared norms of each (monitor, component, frequency) DFT vector's change
+ * since the previous check, of the vector and of its previous value; then
+ * copies the arena into prev_re / prev_im.  Masked-off components and
+ * frequencies beyond a monitor's count report zeros. */
+int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChange* c);
 
 /* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
 void fdtd_clear_graph_cache(void);

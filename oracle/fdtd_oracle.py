@@ -996,3 +996,83 @@ def relative_l2(actual, expected) -> float:
     den = float(np.linalg.norm(e))
     num = float(np.linalg.norm(a - e))
     return 0.0 if den == 0.0 and num == 0.0 else num / max(den, 1e-300)
+
+
+# ---------------------------------------------------------------------------
+# Field diagnostics for automatic termination
+# ---------------------------------------------------------------------------
+
+# beamz/lattice.py:14-21: Yee offsets (z, y, x) in cells; 2D (y, x) from
+# beamz/simulation/execute.py:66-73.
+COMPONENT_OFFSETS_3D = {
+    "Ex": (0.0, 0.0, 0.5), "Ey": (0.0, 0.5, 0.0), "Ez": (0.5, 0.0, 0.0),
+    "Hx": (0.5, 0.5, 0.0), "Hy": (0.5, 0.0, 0.5), "Hz": (0.0, 0.5, 0.5),
+}
+COMPONENT_OFFSETS_2D = {
+    "Ex": (0.0, 0.5), "Ey": (0.5, 0.0), "Ez": (0.0, 0.0),
+    "Hx": (0.5, 0.0), "Hy": (0.0, 0.5), "Hz": (0.5, 0.5),
+}
+
+
+def axis_integration_weights(edges, offset: float, count: int) -> np.ndarray:
+    """Control-volume widths along one axis (beamz/simulation/execute.py:77-93):
+    cell widths for a centre-aligned support; half cells at the two ends and
+    averages of neighbouring cells inside for an edge-aligned one."""
+    edges = np.asarray(edges, dtype=np.float64)
+    widths = np.diff(edges)
+    if offset == 0.5:
+        return widths
+    out = np.empty(int(count), dtype=np.float64)
+    out[0] = 0.5 * widths[0]
+    out[-1] = 0.5 * widths[-1]
+    if count > 2:
+        out[1:-1] = 0.5 * (widths[:-1] + widths[1:])
+    return out
+
+
+def component_integration_weights(component: str, grid_shape, resolution: float) -> np.ndarray:
+    """Physical integration weights of one component on a uniform grid
+    (beamz/simulation/execute.py:95-111)."""
+    offsets = COMPONENT_OFFSETS_3D[component] if len(grid_shape) == 3 else COMPONENT_OFFSETS_2D[component]
+    axes = []
+    for n, off in zip(grid_shape, offsets):
+        edges = np.arange(int(n) + 1, dtype=np.float64) * float(resolution)
+        axes.append(axis_integration_weights(edges, off, int(n) + (1 if off == 0.0 else 0)))
+    w = axes[0]
+    for a in axes[1:]:
+        w = np.multiply.outer(w, a)
+    return w
+
+
+def field_diagnostics(fields: dict, eps_sites: dict, grid_shape, resolution: float):
+    """(energy, max |field|, all finite) of scalar-material fields
+    (beamz/simulation/execute.py:127-222, _energy_terms / _field_diagnostics
+    without the full-tensor cross terms), in float64: energy =
+    sum_c 0.5 * const_c * sum(material * v^2 * weights), const = eps0 for E,
+    mu0 for H; H material is mu_r = 1."""
+    energy, max_field, finite = 0.0, 0.0, True
+    for c, v in fields.items():
+        v = np.asarray(v, dtype=np.float64)
+        finite = finite and bool(np.all(np.isfinite(v)))
+        max_field = max(max_field, float(np.max(np.abs(v), initial=0.0)))
+        mat = np.asarray(eps_sites.get(c, 1.0), dtype=np.float64) if c[0] == "E" else 1.0
+        const = EPS_0 if c[0] == "E" else MU_0
+        w = component_integration_weights(c, grid_shape, resolution)
+        energy += 0.5 * const * float(np.sum(mat * v * v * w))
+    return energy, max_field, finite
+
+
+def relative_monitor_change(current: dict, previous: dict | None):
+    """Largest |cur - prev| / max(|cur|, |prev|) over the monitor vectors, 0 for
+    a pair of vanishing vectors, None without a previous check
+    (beamz/simulation/execute.py:292-316)."""
+    if previous is None:
+        return None
+    tiny = np.finfo(float).tiny
+    changes = []
+    for key, cur in current.items():
+        prev = previous[key]
+        num = float(np.linalg.norm(cur - prev))
+        den = max(float(np.linalg.norm(cur)), float(np.linalg.norm(prev)))
+        changes.append(0.0 if den <= tiny and num <= tiny else num / den)
+    return max(changes, default=0.0)

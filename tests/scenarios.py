@@ -100,7 +100,8 @@ def scenario_2d(grid=(13, 15), polarization="tm", seed=0, pml_cells=3, metallic=
     eps[grid[0] // 3: 2 * grid[0] // 3, :] = 12.11
     h_terms, e_terms = P.plan_cpml(grid, dt, res, pml_cells=pml_cells, polarization=polarization) if cpml else ([], [])
     e_comps = ("Ez",) if polarization == "tm" else ("Ex", "Ey")
-    e_site = {c: (np.float32(1.0), P.e_source_2d(P.site_values_2d(eps, c, polarization), dt)) for c in e_comps}
+    site_eps = {c: P.site_values_2d(eps, c, polarization) for c in e_comps}
+    e_site = {c: (np.float32(1.0), P.e_source_2d(site_eps[c], dt)) for c in e_comps}
     f0 = P.LIGHT_SPEED / 1.55e-6
     wave = P.gaussian_pulse((np.arange(nsteps) + 0.5) * dt, f0, 0.5 * f0, offset=0.3)
     comp = "Ez" if polarization == "tm" else "Ey"
@@ -120,9 +121,9 @@ def scenario_2d(grid=(13, 15), polarization="tm", seed=0, pml_cells=3, metallic=
         w.append(np.ones((P_, 1), np.float32))
     mask = np.array([1.0 if c in P.active_components(2, polarization) else 0.0 for c in P.COMPONENTS], np.float32)
     mons = [P.DftMonitorPlan(np.array([0.95 * f0, f0, 1.05 * f0], np.float32), idx, w, mask)]
-    return P.ProgramSpec(tuple(grid), dt, res, polarization=polarization, e_site=e_site, h_terms=h_terms,
-                         e_terms=e_terms, metallic_edges=frozenset(metallic), sources=srcs, monitors=mons,
-                         total_steps=nsteps)
+    return P.ProgramSpec(tuple(grid), dt, res, polarization=polarization, e_site=e_site, e_site_eps=site_eps,
+                         h_terms=h_terms, e_terms=e_terms, metallic_edges=frozenset(metallic), sources=srcs,
+                         monitors=mons, total_steps=nsteps)
 
 
 def random_initial_fields(spec: P.ProgramSpec, seed=1, scale=1.0):
