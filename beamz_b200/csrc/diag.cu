@@ -6,9 +6,9 @@
 // (beamz/simulation/execute.py:184-222 _field_diagnostics, 294-316
 // _relative_monitor_change, driven by run_until_terminated 1312-1484).  Here
 // each is a bandwidth-bound read of the fields or the arena: coalesced row
-// sweeps, per-thread double accumulators, warp-shuffle and shared-memory
-// block reductions, and a fixed partition and summation order, so a result
-// is identical from run to run.
+// sweeps, float products with double accumulation across rows, warp-shuffle
+// and shared-memory block reductions, and a fixed partition and summation
+// order, so a result is identical from run to run.
 
 #include "kernels.cuh"
 
@@ -49,8 +49,45 @@ __device__ __forceinline__ void block_reduce(double& s, float& m, unsigned& n) {
   }
 }
 
-// Block b of component c sweeps rows (k, j) = b, b + gridDim.x, ... of the
-// component's stored extents, threads striding along x.
+// Rows (k, j) of one component, one warp per row: warp w of block b sweeps
+// rows b * warps_per_block + w, then + all warps of the grid; its lanes stride
+// along x, eight loads in flight each.  A lane forms each product eps * v^2 in
+// float and sums its products of a row in float; each row then enters the
+// double accumulator once, weighted by its y/z factor, with the two end sites
+// of an edge-aligned x axis taken at half weight.  MAT: 0 eps_r = 1, 1
+// codebook ids and table, 2 per-site array.
+template <int MAT>
+__device__ __forceinline__ void diag_rows(const DiagComp& q, double& s, float& mx, unsigned& bad) {
+  const int rows = q.d.z * q.d.y;  // < 2^31: component arrays are validated below 2^31 elements
+  const int lane = threadIdx.x & 31;
+  const int step = gridDim.x * kDiagWarps;
+  for (int r = blockIdx.x * kDiagWarps + (threadIdx.x >> 5); r < rows; r += step) {
+    const int k = r / q.d.y, j = r - k * q.d.y;
+    const int64_t base = k * q.plane + j * q.row;
+    const float* f = q.field + base;
+    float acc = 0.0f, ends = 0.0f;
+#pragma unroll 8
+    for (int i = lane; i < q.d.x; i += 32) {
+      const float x = f[i];
+      float e = 1.0f;
+      if constexpr (MAT == 1) e = q.table[(q.ids[base + i] >> q.shift) & 0xffu];
+      if constexpr (MAT == 2) e = q.eps[static_cast<int64_t>(r) * q.d.x + i];
+      if (!isfinite(x)) {
+        ++bad;
+        continue;
+      }
+      mx = fmaxf(mx, fabsf(x));
+      const float prod = e * x * x;
+      acc += prod;
+      if (i == 0 || i == q.d.x - 1) ends += prod;
+    }
+    double h = 1.0;
+    if (q.integrate_z && q.edge_z && (k == 0 || k == q.d.z - 1)) h *= 0.5;
+    if (q.edge_y && (j == 0 || j == q.d.y - 1)) h *= 0.5;
+    s += h * (static_cast<double>(acc) - (q.edge_x ? 0.5 * static_cast<double>(ends) : 0.0));
+  }
+}
+
 __global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(DiagArgs a) {
   const int c = blockIdx.y;
   double s = 0.0;
@@ -58,30 +95,9 @@ __global__ void __launch_bounds__(kDiagThreads) diag_partial_kernel(DiagArgs a) 
   unsigned bad = 0;
   if ((a.active >> c) & 1) {
     const DiagComp& q = a.comp[c];
-    const int64_t rows = static_cast<int64_t>(q.d.z) * q.d.y;
-    for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
-      const int k = static_cast<int>(r / q.d.y), j = static_cast<int>(r % q.d.y);
-      double hzy = 1.0;
-      if (q.integrate_z && q.edge_z && (k == 0 || k == q.d.z - 1)) hzy *= 0.5;
-      if (q.edge_y && (j == 0 || j == q.d.y - 1)) hzy *= 0.5;
-      const float* row = q.field + k * q.plane + j * q.row;
-      const uint32_t* ids = q.ids ? q.ids + k * q.plane + j * q.row : nullptr;
-      const float* eps = q.eps ? q.eps + (static_cast<int64_t>(k) * q.d.y + j) * q.d.x : nullptr;
-      for (int i = threadIdx.x; i < q.d.x; i += kDiagThreads) {
-        const float v = row[i];
-        if (!isfinite(v)) {
-          ++bad;
-          continue;
-        }
-        mx = fmaxf(mx, fabsf(v));
-        double e = 1.0;
-        if (ids) e = q.table[(ids[i] >> q.shift) & 0xffu];
-        else if (eps) e = eps[i];
-        const double h = q.edge_x && (i == 0 || i == q.d.x - 1) ? 0.5 * hzy : hzy;
-        const double dv = v;
-        s += e * dv * dv * h;
-      }
-    }
+    if (q.ids) diag_rows<1>(q, s, mx, bad);
+    else if (q.eps) diag_rows<2>(q, s, mx, bad);
+    else diag_rows<0>(q, s, mx, bad);
   }
   block_reduce(s, mx, bad);
   if (threadIdx.x == 0) {

@@ -45,7 +45,8 @@ def test_device_diagnostics_match_the_oracle(case):
     got = R.field_diagnostics(st, prog)
     energy, max_field, finite = O.field_diagnostics(fields, _site_eps(spec), spec.grid_shape, spec.resolution)
     assert got.finite and finite and got.nonfinite == 0
-    assert got.energy == pytest.approx(energy, rel=1e-9)
+    # float products, double sums across rows (the reference sums in float32)
+    assert got.energy == pytest.approx(energy, rel=1e-6)
     assert np.float32(got.max_field) == np.float32(max_field)
     again = R.field_diagnostics(st, prog)
     assert again.energy == got.energy  # fixed partition and order: identical
@@ -63,7 +64,7 @@ def test_nonfinite_values_are_counted_and_left_out():
     assert not got.finite and got.nonfinite == 3
     clean = {k: np.where(np.isfinite(v), v, 0.0).astype(np.float32) for k, v in planted.items()}
     energy, max_field, _ = O.field_diagnostics(clean, _site_eps(spec), spec.grid_shape, spec.resolution)
-    assert got.energy == pytest.approx(energy, rel=1e-9)
+    assert got.energy == pytest.approx(energy, rel=1e-6)
     assert np.float32(got.max_field) == np.float32(max_field)
 
 
