@@ -339,19 +339,72 @@ def site_codebook(voxel_ids: np.ndarray, eps_table: np.ndarray, dt_over_eps):
     return words, coef
 
 
-def site_eps_3d(voxel_ids: np.ndarray, eps_table: np.ndarray, component: str) -> np.ndarray:
-    """float32 E-site permittivity of one component over its stored shape: the
-    same four-voxel average as the codebook (beamz/lattice.py:732-786)."""
+def e_site_average_3d(grid: np.ndarray, component: str) -> np.ndarray:
+    """float32 E-site sample of a cell-centred float grid over the component's
+    stored shape: the four-voxel average 0.5*(0.5*(t0+t1) + 0.5*(t2+t3)) with
+    clipped indices (beamz/lattice.py:732-786), as the codebook uses."""
     f32 = np.float32
-    table = np.ones(256, f32)
-    table[: len(eps_table)] = np.asarray(eps_table, f32)
-    vp = edge_replicated(table[np.asarray(voxel_ids, np.uint8)])
-    nz, ny, nx = (int(v) for v in np.shape(voxel_ids))
+    g = np.asarray(grid, f32)
+    vp = edge_replicated(g)
+    nz, ny, nx = g.shape
     t = [vp[dk:dk + nz + 1, dj:dj + ny + 1, di:di + nx + 1] for dk, dj, di in CODEBOOK_TAPS[component]]
     half = f32(0.5)
     site = half * (half * (t[0] + t[1]) + half * (t[2] + t[3]))
     dz, dy, dx = component_shape(component, (nz, ny, nx))
     return np.ascontiguousarray(site[:dz, :dy, :dx], dtype=f32)
+
+
+def site_eps_3d(voxel_ids: np.ndarray, eps_table: np.ndarray, component: str) -> np.ndarray:
+    """float32 E-site permittivity of one component over its stored shape
+    (voxel ids and a permittivity table)."""
+    table = np.ones(256, np.float32)
+    table[: len(eps_table)] = np.asarray(eps_table, np.float32)
+    return e_site_average_3d(table[np.asarray(voxel_ids, np.uint8)], component)
+
+
+# Yee offsets (z, y, x) in cells, beamz/lattice.py:14-21.
+_OFFSETS_3D = {"Ex": (0.0, 0.0, 0.5), "Ey": (0.0, 0.5, 0.0), "Ez": (0.5, 0.0, 0.0),
+               "Hx": (0.5, 0.5, 0.0), "Hy": (0.5, 0.0, 0.5), "Hz": (0.0, 0.5, 0.5)}
+
+
+def h_site_sample_3d(grid: np.ndarray, component: str) -> np.ndarray:
+    """Sample of a cell-centred grid at an H component's sites: the owning
+    voxel floor(index + offset), clipped (beamz/lattice.py:670-729)."""
+    g = np.asarray(grid)
+    shape = component_shape(component, g.shape)
+    idx = [np.clip(np.floor(np.arange(n, dtype=np.float64) + off).astype(np.int64), 0, m - 1)
+           for n, off, m in zip(shape, _OFFSETS_3D[component], g.shape)]
+    return np.ascontiguousarray(g[np.ix_(*idx)])
+
+
+def lossy_site_coefficients_3d(eps_grid: np.ndarray, sigma_grid: np.ndarray, dt: float):
+    """Per-site update coefficients of a conductive, non-magnetic 3D material,
+    as beamz's CUDA path receives them (beamz/simulation/compile.py:563-640):
+    sigma sampled at E sites like eps (lattice.py:1031-1044), the matched
+    magnetic conductivity sigma * MU_0 / EPS_0 at the H sites' owning voxels
+    (lattice.py:1046-1068), then decay and source by
+    precompute_e/h_update_coefficients (kernels.py:704-728), float32 throughout.
+    Returns ``(e_site, h_site, e_site_eps)`` for a :class:`ProgramSpec`."""
+    f32 = np.float32
+    dt = float(dt)  # a Python float: float32 arithmetic, as in beamz (JAX weak typing)
+    eps = np.asarray(eps_grid, f32)
+    sig = np.asarray(sigma_grid, f32)
+    e_site, h_site, e_eps = {}, {}, {}
+    for c in ("Ex", "Ey", "Ez"):
+        ep = e_site_average_3d(eps, c)
+        sg = e_site_average_3d(sig, c)
+        denom = 1.0 + sg * dt / (2.0 * EPS_0 * ep)
+        decay = ((1.0 - sg * dt / (2.0 * EPS_0 * ep)) / denom).astype(f32)
+        source = ((dt / (EPS_0 * ep)) / denom).astype(f32)
+        e_site[c], e_eps[c] = (decay, source), ep
+    base = sig * f32(1.0) * MU_0 / EPS_0
+    for c in ("Hx", "Hy", "Hz"):
+        sm = h_site_sample_3d(base, c)
+        denom = 1.0 + sm * dt / (2.0 * MU_0)
+        decay = ((1.0 - sm * dt / (2.0 * MU_0)) / denom).astype(f32)
+        source = ((dt / MU_0) / denom).astype(f32)
+        h_site[c] = (decay, source)
+    return e_site, h_site, e_eps
 
 
 def site_values_2d(eps_grid: np.ndarray, component: str, polarization: str = "tm") -> np.ndarray:

@@ -511,9 +511,14 @@ def material_from_voxels(voxel_eps: np.ndarray, voxel_sigma=None, dtype=np.float
     return Material3D(eps, tuple(sample_e_site_3d(s, c) for c in ("Ex", "Ey", "Ez")))
 
 
-def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0)):
+def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0), coeffs=None):
     """beamz/simulation/kernels.py:458-503 (``h_terms`` empty => kernels.py:267-290
-    without CPML).  Returns (hx, hy, hz, psi_h)."""
+    without CPML).  Returns (hx, hy, hz, psi_h).
+
+    ``coeffs`` (component -> (decay, source) arrays) selects the form of
+    beamz's CUDA path instead, which receives precomputed coefficients:
+    H <- decay * H - source * curl with the same (CPML-corrected) curl
+    (cuda/src/update.cu:392-410 and 585-597)."""
     ex, ey, ez, hx, hy, hz = (fields[c] for c in COMPONENTS)
     dtype = hx.dtype
     f = dtype.type
@@ -537,12 +542,22 @@ def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0))
             new_psi[i] = p
         curls = tuple(corrected[i] + corrected[i + 1] for i in (0, 2, 4))
         out = []
+        if coeffs is not None:
+            for c, fld, curl in zip(("Hx", "Hy", "Hz"), (hx, hy, hz), curls):
+                decay, source = (np.asarray(v, dtype) for v in coeffs[c])
+                out.append(decay * fld - source * curl)
+            return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
         for fld, curl, sm in zip((hx, hy, hz), curls, sigma_m):
             alpha = np.asarray(sm, dtype) * (f(0.5) * dt_over_mu)
             out.append(((one - alpha) * fld - dt_over_mu * curl) / (one + alpha))
     else:
         curls = (derivs[0] - derivs[1], derivs[2] - derivs[3], derivs[4] - derivs[5])
         out = []
+        if coeffs is not None:
+            for c, fld, curl in zip(("Hx", "Hy", "Hz"), (hx, hy, hz), curls):
+                decay, source = (np.asarray(v, dtype) for v in coeffs[c])
+                out.append(decay * fld - source * curl)
+            return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
         for fld, curl, sm in zip((hx, hy, hz), curls, sigma_m):
             alpha = np.asarray(sm, dtype) * (f(0.5) * dt_over_mu)
             denom = one + alpha
@@ -550,7 +565,7 @@ def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0))
     return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
 
 
-def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, metallic_edges=()):
+def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, metallic_edges=(), coeffs=None):
     """beamz/simulation/kernels.py:554-626 (``e_terms`` empty =>
     kernels.py:326-388).  Returns (ex, ey, ez, psi_e)."""
     ex, ey, ez, hx, hy, hz = (fields[c] for c in COMPONENTS)
@@ -585,12 +600,22 @@ def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, me
             new_psi[i] = p
         curls = tuple(corrected[i] + corrected[i + 1] for i in (0, 2, 4))
         out = []
+        if coeffs is not None:  # beamz's CUDA path: cuda/src/update.cu:644-652
+            for c, fld, curl in zip(("Ex", "Ey", "Ez"), (ex, ey, ez), curls):
+                decay, source = (np.asarray(v, dtype) for v in coeffs[c])
+                out.append(decay * fld + source * curl)
+            return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
         for fld, curl, cond, iv in zip((ex, ey, ez), curls, material.sigma, inv):
             beta = np.asarray(cond, dtype) * (f(0.5) * dt_over_eps) * iv
             out.append(((one - beta) * fld + dt_over_eps * iv * curl) / (one + beta))
     else:
         curls = (derivs[0] - derivs[1], derivs[2] - derivs[3], derivs[4] - derivs[5])
         out = []
+        if coeffs is not None:  # cuda/src/update.cu:392-410
+            for c, fld, curl in zip(("Ex", "Ey", "Ez"), (ex, ey, ez), curls):
+                decay, source = (np.asarray(v, dtype) for v in coeffs[c])
+                out.append(decay * fld + source * curl)
+            return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
         for fld, curl, cond, iv in zip((ex, ey, ez), curls, material.sigma, inv):
             beta = np.asarray(cond, dtype) * (f(0.5) * dt_over_eps) * iv
             denom = one + beta
@@ -918,7 +943,8 @@ class OracleProgram:
     e_terms: list = field(default_factory=list)
     material: Material3D | None = None  # 3D
     h_coeffs: tuple | None = None  # 2D (decay, source)
-    e_coeffs: dict | None = None  # 2D component -> (decay, source)
+    e_coeffs: dict | None = None  # 2D component -> (decay, source); 3D with h_coeffs_3d: coefficient form
+    h_coeffs_3d: dict | None = None  # 3D component -> (decay, source) (beamz's CUDA path)
     metallic_edges: frozenset = frozenset()
     sources: list = field(default_factory=list)
     monitors: list = field(default_factory=list)
@@ -950,7 +976,7 @@ def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
     if program.ndim == 3:
         sm = program.material.sigma_m if program.material is not None else (0.0, 0.0, 0.0)
         hx, hy, hz, state.psi_h = update_h_3d(fields, state.psi_h, program.h_terms, program.dt,
-                                              program.resolution, sm)
+                                              program.resolution, sm, program.h_coeffs_3d)
         fields["Hx"], fields["Hy"], fields["Hz"] = hx, hy, hz
     else:
         new, state.psi_h = update_h_2d(fields, state.psi_h, program.h_terms, program.resolution,
@@ -963,7 +989,8 @@ def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
     # 3. E, E sources, E masks.
     if program.ndim == 3:
         ex, ey, ez, state.psi_e = update_e_3d(fields, state.psi_e, program.e_terms, program.dt,
-                                              program.resolution, program.material, program.metallic_edges)
+                                              program.resolution, program.material, program.metallic_edges,
+                                              program.e_coeffs if program.h_coeffs_3d is not None else None)
         fields["Ex"], fields["Ey"], fields["Ez"] = ex, ey, ez
     else:
         new, state.psi_e = update_e_2d(fields, state.psi_e, program.e_terms, program.resolution,
