@@ -407,6 +407,36 @@ def lossy_site_coefficients_3d(eps_grid: np.ndarray, sigma_grid: np.ndarray, dt:
     return e_site, h_site, e_eps
 
 
+def lossy_site_coefficients_2d(eps_grid: np.ndarray, sigma_grid: np.ndarray, dt: float, polarization: str = "tm"):
+    """2D analogue of :func:`lossy_site_coefficients_3d`: eps and sigma sampled
+    on each active component's support (lattice.py:919-972, the H supports of
+    the matched magnetic conductivity sigma * MU_0 / EPS_0 included,
+    lattice.py:1117-1129), then precompute_e/h_update_coefficients
+    (kernels.py:704-728).  Returns ``(e_site, h_site, e_site_eps)``."""
+    f32 = np.float32
+    dt = float(dt)
+    eps = np.asarray(eps_grid, f32)
+    sig = np.asarray(sigma_grid, f32)
+    e_comps = ("Ez",) if polarization == "tm" else ("Ex", "Ey")
+    h_comps = ("Hx", "Hy") if polarization == "tm" else ("Hz",)
+    e_site, h_site, e_eps = {}, {}, {}
+    for c in e_comps:
+        ep = np.asarray(site_values_2d(eps, c, polarization), f32)
+        sg = np.asarray(site_values_2d(sig, c, polarization), f32)
+        denom = 1.0 + sg * dt / (2.0 * EPS_0 * ep)
+        decay = ((1.0 - sg * dt / (2.0 * EPS_0 * ep)) / denom).astype(f32)
+        source = ((dt / (EPS_0 * ep)) / denom).astype(f32)
+        e_site[c], e_eps[c] = (decay, source), ep
+    base = sig * f32(1.0) * MU_0 / EPS_0
+    for c in h_comps:
+        sm = np.asarray(site_values_2d(base, c, polarization), f32)
+        denom = 1.0 + sm * dt / (2.0 * MU_0)
+        decay = ((1.0 - sm * dt / (2.0 * MU_0)) / denom).astype(f32)
+        source = ((dt / MU_0) / denom).astype(f32)
+        h_site[c] = (decay, source)
+    return e_site, h_site, e_eps
+
+
 def site_values_2d(eps_grid: np.ndarray, component: str, polarization: str = "tm") -> np.ndarray:
     """2D supports take the owning voxel (beamz/lattice.py:935-972)."""
     ny, nx = eps_grid.shape

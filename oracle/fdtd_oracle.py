@@ -645,10 +645,13 @@ def e_coefficients_2d(eps_site, dt, dtype=np.float32):
 
 def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm"):
     """TM: beamz/simulation/kernels.py:731-738, 771-788, 1217-1243;
-    TE: kernels.py:791-797, 838-850, 1286-1300."""
+    TE: kernels.py:791-797, 838-850, 1286-1300.  ``h_coeffs`` is one
+    (decay, source) pair for every H component, or a dict component ->
+    (decay, source) (per-site arrays of a magnetically lossy material)."""
     dtype = fields["Ez" if polarization == "tm" else "Hz"].dtype
     res = dtype.type(resolution)
-    decay, source = h_coeffs
+    per = h_coeffs if isinstance(h_coeffs, dict) else None
+    decay, source = h_coeffs["Hx" if polarization == "tm" else "Hz"] if per else h_coeffs
     new_psi = list(psi_h) if psi_h else []
     if polarization == "tm":
         ez, hx, hy = fields["Ez"], fields["Hx"], fields["Hy"]
@@ -660,6 +663,8 @@ def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm")
         else:
             c0, c1 = d0, -d1
         hx_n = decay * hx - source * c0
+        if per:
+            decay, source = per["Hy"]
         hy_n = decay * hy - source * c1
         return {"Hx": hx_n.astype(dtype), "Hy": hy_n.astype(dtype)}, new_psi
     ex, ey, hz = fields["Ex"], fields["Ey"], fields["Hz"]

@@ -59,6 +59,25 @@ def main(argv=None) -> None:
         dec, src = ref.kernels.precompute_h_update_coefficients(sm, dt)
         out[f"sigm_{c}"] = np.asarray(sm)
         out[f"decay_{c}"], out[f"source_{c}"] = np.asarray(dec), np.asarray(src)
+    # 2D (lattice.py:1091-1140): each active support samples eps, sigma and
+    # the matched magnetic conductivity; then the same precompute functions.
+    grid2 = (6, 7)
+    eps2 = rng.choice(np.array([1.0, 2.085, 12.11], np.float32), size=grid2)
+    sig2 = rng.choice(np.array([0.0, 2.5e3, 4.0e4], np.float32), size=grid2)
+    dt2 = float(0.7 * 20e-9 / (299792458.0 * 2.0**0.5))
+    out.update(eps2=eps2, sigma2=sig2, dt2=np.float64(dt2))
+    base = jnp.asarray(sig2) * jnp.asarray(np.float32(1.0)) * 1.25663706212e-6 / 8.8541878128e-12
+    for pol, e_comps, h_comps in (("tm", ("Ez",), ("Hx", "Hy")), ("te", ("Ex", "Ey"), ("Hz",))):
+        for c in e_comps:
+            e = ref.lattice.sample_voxel_grid_at_component_2d(jnp.asarray(eps2), c, "xy", pol)
+            s = ref.lattice.sample_voxel_grid_at_component_2d(jnp.asarray(sig2), c, "xy", pol)
+            dec, src = ref.kernels.precompute_e_update_coefficients(
+                shape=np.shape(e), conductivity=s, permittivity=e, dt=dt2, region=(slice(None),) * 2)
+            out[f"{pol}_eps_{c}"], out[f"{pol}_decay_{c}"], out[f"{pol}_source_{c}"] = map(np.asarray, (e, dec, src))
+        for c in h_comps:
+            sm = ref.lattice.sample_voxel_grid_at_component_2d(base, c, "xy", pol)
+            dec, src = ref.kernels.precompute_h_update_coefficients(sm, dt2)
+            out[f"{pol}_decay_{c}"], out[f"{pol}_source_{c}"] = np.asarray(dec), np.asarray(src)
     np.savez(args.out, **out)
     print(f"wrote {args.out}: {len(out)} arrays")
 

@@ -101,3 +101,57 @@ def assert_family_close(got: dict, ref: dict, tol: float) -> None:
         for c in comps:
             err = float(np.linalg.norm(np.asarray(got[c], np.float64) - np.asarray(ref[c], np.float64)))
             assert err <= tol * scale, f"{c}: {err:.3e} > {tol} * {scale:.3e}"
+
+
+def test_lossy_2d_coefficients_match_the_reference():
+    for pol in ("tm", "te"):
+        e, h, eps = P.lossy_site_coefficients_2d(GOLD["eps2"], GOLD["sigma2"], float(GOLD["dt2"]), pol)
+        for c, (dec, src) in {**e, **h}.items():
+            np.testing.assert_array_equal(dec, GOLD[f"{pol}_decay_{c}"], err_msg=f"{pol} {c}")
+            np.testing.assert_array_equal(src, GOLD[f"{pol}_source_{c}"], err_msg=f"{pol} {c}")
+        for c in e:
+            np.testing.assert_array_equal(eps[c], GOLD[f"{pol}_eps_{c}"], err_msg=f"{pol} {c}")
+
+
+def lossy_scene_2d(grid=(21, 26), polarization="tm", seed=0, pml_cells=4, nsteps=12):
+    """A conductive 2D scene (eps and sigma boxes, CPML, a pre-E point source,
+    a line monitor) and the matching oracle program (per-component E and H
+    coefficient arrays: beamz's 2D path applies decay/source in both backends)."""
+    rng = np.random.default_rng(seed)
+    res = 20e-9
+    dt = float(0.7 * res / (P.LIGHT_SPEED * 2.0**0.5))
+    eps = np.full(grid, 2.085, np.float32)
+    sigma = np.zeros(grid, np.float32)
+    for _ in range(2):
+        y0, x0 = int(rng.integers(1, grid[0] - 5)), int(rng.integers(1, grid[1] - 5))
+        eps[y0:y0 + 5, x0:x0 + 6] = 12.11
+        sigma[y0:y0 + 5, x0:x0 + 6] = rng.choice([5e3, 4e4])
+    e_site, h_site, e_eps = P.lossy_site_coefficients_2d(eps, sigma, dt, polarization)
+    h_terms, e_terms = P.plan_cpml(grid, dt, res, pml_cells=pml_cells, polarization=polarization)
+    f0 = P.LIGHT_SPEED / 1.55e-6
+    wave = P.gaussian_pulse((np.arange(nsteps) + 0.5) * dt, f0, 0.5 * f0, offset=0.3)
+    comp = "Ez" if polarization == "tm" else "Ey"
+    srcs = [P.SourcePlan(comp, "pre_e", (grid[0] // 2, grid[1] // 3), np.array([[-dt / (P.EPS_0 * 2.085)]], np.float32),
+                         wave)]
+    idx, w = [], []
+    rows = np.arange(2, grid[0] - 2)
+    for c in P.COMPONENTS:
+        sy, sx = P.component_shape(c, grid, polarization)
+        idx.append((np.minimum(rows, sy - 1) * sx + min(2 * grid[1] // 3, sx - 1)).astype(np.int32)[:, None])
+        w.append(np.ones((rows.size, 1), np.float32))
+    mask = np.array([1.0 if c in P.active_components(2, polarization) else 0.0 for c in P.COMPONENTS], np.float32)
+    mon = P.DftMonitorPlan(np.array([0.95 * f0, 1.05 * f0], np.float32), idx, w, mask)
+    spec = P.ProgramSpec(tuple(grid), dt, res, polarization=polarization, e_site=e_site, h_site=h_site,
+                         e_site_eps=e_eps, h_terms=h_terms, e_terms=e_terms, sources=srcs, monitors=[mon],
+                         total_steps=nsteps)
+    shapes = O.component_shapes(grid, polarization)
+    terms = lambda ts: [O.CpmlTerm(t.component, t.axis, t.sign, t.low, t.high, t.a, t.b, t.inv_kappa,  # noqa: E731
+                                   shapes[t.component][t.axis]) for t in ts]
+    sources = [O.SlabSource(s.component, s.timing, tuple(s.start), np.asarray(s.coeff, np.float32),
+                            np.asarray(s.waveform, np.float32)) for s in srcs]
+    monitors = [O.DftMonitor(mon.freqs, mon.indices, mon.weights, mon.component_mask)]
+    oprog = O.OracleProgram(tuple(grid), dt, res, terms(h_terms), terms(e_terms), sources=sources,
+                            monitors=monitors, polarization=polarization)
+    oprog.h_coeffs = h_site
+    oprog.e_coeffs = e_site
+    return spec, oprog

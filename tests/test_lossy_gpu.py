@@ -49,3 +49,18 @@ def test_lossy_fields_decay_faster_than_lossless():
     prog0 = R.compile_program(plain)
     lossless = R.field_diagnostics(R.run_steps(R.initial_state(prog0), prog0, 60), prog0).energy
     assert 0.0 < lossy < lossless
+
+
+@pytest.mark.parametrize("pol", ["tm", "te"])
+@pytest.mark.parametrize("schedule", ["fused", "phases"])
+def test_lossy_2d_step_matches_the_oracle_bit_for_bit(pol, schedule):
+    from tests.test_lossy import lossy_scene_2d
+
+    spec, oprog = lossy_scene_2d(polarization=pol, seed=4)
+    fields = random_initial_fields(spec, seed=10)
+    prog = R.compile_program(spec, schedule=schedule)
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, 12).numpy()
+    st = O.run(oracle_state(oprog, fields), oprog, 12)
+    for c in P.active_components(2, pol):
+        np.testing.assert_array_equal(out[c], st.fields[c], err_msg=c)
+    assert O.relative_l2(out["dft_re"], st.dft_re) <= 1e-4
