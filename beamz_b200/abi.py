@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 6
+FDTD_ABI_VERSION = 7
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
@@ -46,6 +46,8 @@ EXPORTED_SYMBOLS = (
     "fdtd_adjoint_curl",
     "fdtd_field_diagnostics",
     "fdtd_dft_change",
+    "fdtd_pack_gather",
+    "fdtd_voxel_histogram",
     "fdtd_adjoint_step_noalloc",
     "fdtd_graph_create",
     "fdtd_graph_launch",
@@ -147,6 +149,18 @@ class FdtdDiagnostics(ctypes.Structure):
 
 class FdtdDftChange(ctypes.Structure):
     _fields_ = [("prev_re", FdtdBuffer), ("prev_im", FdtdBuffer), ("out", FdtdBuffer)]
+
+
+class FdtdGatherPack(ctypes.Structure):
+    _fields_ = [
+        ("indices_in", FdtdBuffer),
+        ("weights_in", FdtdBuffer),
+        ("indices_out", FdtdBuffer),
+        ("weights_out", FdtdBuffer),
+        ("dims", ctypes.c_int32 * 3),
+        ("row", ctypes.c_int64),
+        ("plane", ctypes.c_int64),
+    ]
 
 
 class FdtdRegistration(ctypes.Structure):
@@ -274,6 +288,10 @@ def load_library(path: str | None = None):
         lib.fdtd_field_diagnostics.restype = ctypes.c_int
         lib.fdtd_dft_change.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(FdtdDftChange)]
         lib.fdtd_dft_change.restype = ctypes.c_int
+        lib.fdtd_pack_gather.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdGatherPack)]
+        lib.fdtd_pack_gather.restype = ctypes.c_int
+        lib.fdtd_voxel_histogram.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdBuffer), ctypes.POINTER(FdtdBuffer)]
+        lib.fdtd_voxel_histogram.restype = ctypes.c_int
         lib.fdtd_graph_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(ctypes.c_void_p)]
         lib.fdtd_graph_create.restype = ctypes.c_int
         lib.fdtd_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]

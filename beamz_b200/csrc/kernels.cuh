@@ -144,6 +144,20 @@ struct DftDev {
   float dt;
 };
 
+// Gather-plan packing (planner.cu): one (monitor, component) plan.
+struct GatherPackDev {
+  const int* idx_in = nullptr;    // [points, slots_in]
+  const float* w_in = nullptr;
+  int* idx_out = nullptr;         // [K, pmax]
+  float* w_out = nullptr;
+  int points = 0, slots_in = 0, pmax = 0;
+  int dz = 0, dy = 0, dx = 0;     // component extents
+  int64_t row = 0, plane = 0;     // device layout strides
+};
+
+cudaError_t launch_gather_pack(cudaStream_t s, const GatherPackDev& g);
+cudaError_t launch_voxel_histogram(cudaStream_t s, const uint8_t* v, int64_t n, int* counts);
+
 // Field diagnostics (diag.cu): one component's view.
 struct DiagComp {
   const float* field = nullptr;   // stored array (dense, or pitched rows)

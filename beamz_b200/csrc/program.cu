@@ -912,6 +912,50 @@ int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChang
                                                   static_cast<double*>(c->out.data)));
 }
 
+int fdtd_pack_gather(void* stream, const FdtdGatherPack* g) {
+  if (g == nullptr) return fdtd::kInvalid;
+  const FdtdBuffer &ii = g->indices_in, &wi = g->weights_in, &io = g->indices_out, &wo = g->weights_out;
+  if (ii.element_type != FDTD_S32 || !fdtd::is_f32(wi) || io.element_type != FDTD_S32 || !fdtd::is_f32(wo))
+    return fdtd::kInvalid;
+  if (ii.rank != 2 || wi.rank != 2 || io.rank != 2 || wo.rank != 2) return fdtd::kInvalid;
+  if (wi.dims[0] != ii.dims[0] || wi.dims[1] != ii.dims[1] || wo.dims[0] != io.dims[0] || wo.dims[1] != io.dims[1])
+    return fdtd::kInvalid;
+  const int64_t points = ii.dims[0], slots = ii.dims[1], K = io.dims[0], pmax = io.dims[1];
+  if (slots > K || points > pmax || slots > 32 || pmax >= (int64_t{1} << 31)) return fdtd::kInvalid;
+  if (g->dims[0] < 1 || g->dims[1] < 1 || g->dims[2] < 1 || g->row < g->dims[2] ||
+      g->plane < g->row * static_cast<int64_t>(g->dims[1]) ||
+      static_cast<int64_t>(g->dims[0]) * g->plane >= (int64_t{1} << 31))
+    return fdtd::kInvalid;
+  if (points > 0 && (ii.data == nullptr || wi.data == nullptr || io.data == nullptr || wo.data == nullptr))
+    return fdtd::kInvalid;
+  fdtd::GatherPackDev d;
+  d.idx_in = static_cast<const int*>(ii.data);
+  d.w_in = static_cast<const float*>(wi.data);
+  d.idx_out = static_cast<int*>(io.data);
+  d.w_out = static_cast<float*>(wo.data);
+  d.points = static_cast<int>(points);
+  d.slots_in = static_cast<int>(slots);
+  d.pmax = static_cast<int>(pmax);
+  d.dz = g->dims[0];
+  d.dy = g->dims[1];
+  d.dx = g->dims[2];
+  d.row = g->row;
+  d.plane = g->plane;
+  return static_cast<int>(fdtd::launch_gather_pack(static_cast<cudaStream_t>(stream), d));
+}
+
+int fdtd_voxel_histogram(void* stream, const FdtdBuffer* voxels, const FdtdBuffer* counts) {
+  if (voxels == nullptr || counts == nullptr) return fdtd::kInvalid;
+  if (voxels->element_type != FDTD_U8 || counts->element_type != FDTD_S32 || fdtd::elements(*counts) != 256 ||
+      counts->data == nullptr)
+    return fdtd::kInvalid;
+  const int64_t n = fdtd::elements(*voxels);
+  if (n < 0 || (n > 0 && voxels->data == nullptr)) return fdtd::kInvalid;
+  return static_cast<int>(fdtd::launch_voxel_histogram(static_cast<cudaStream_t>(stream),
+                                                       static_cast<const uint8_t*>(voxels->data), n,
+                                                       static_cast<int*>(counts->data)));
+}
+
 int fdtd_graph_create(void* stream, const FdtdProgram* program, void** graph) {
   if (program == nullptr || graph == nullptr || stream == nullptr || program->nsteps < 1) return fdtd::kInvalid;
   *graph = nullptr;

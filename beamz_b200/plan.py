@@ -303,13 +303,17 @@ def codebook_tables(eps_used: np.ndarray, dt_over_eps, present: dict, with_eps: 
     return (luts, coef, eps) if with_eps else (luts, coef)
 
 
-def compact_materials(voxel_ids: np.ndarray, eps_table: np.ndarray):
+def compact_materials(voxel_ids: np.ndarray, eps_table: np.ndarray, counts=None):
     """Compact voxel ids to 0..m-1 over the ids that occur.
 
     Returns ``(remap, eps_used)``: ``remap`` is a 256-entry int32 table from
     voxel id to compact index and ``eps_used`` the m permittivities.
+    ``counts`` (the 256-bin voxel-id histogram, e.g. from the device) saves
+    counting the ids here.
     """
-    used = np.flatnonzero(np.bincount(np.asarray(voxel_ids, np.uint8).reshape(-1), minlength=256))
+    if counts is None:
+        counts = np.bincount(np.asarray(voxel_ids, np.uint8).reshape(-1), minlength=256)
+    used = np.flatnonzero(np.asarray(counts))
     if used.size > CODEBOOK_MAX_MATERIALS:
         raise CodebookOverflow(f"{used.size} materials (> {CODEBOOK_MAX_MATERIALS}) for the site codebook")
     remap = np.zeros(256, np.int32)
@@ -599,9 +603,20 @@ def sources_clear_of_monitors(spec) -> bool:
             flat = idx[np.asarray(mon.weights[ci]) != 0]
             if flat.size == 0:
                 continue
-            coords = np.unravel_index(flat.astype(np.int64), component_shape(c, spec.grid_shape, spec.polarization))
+            shape = component_shape(c, spec.grid_shape, spec.polarization)
+            flat = flat.astype(np.int64)
             for start, ext in boxes[c]:
-                inside = np.ones(flat.shape, bool)
+                # only offsets between the box's first and last cell can be in it
+                first = tuple(max(lo, 0) for lo in start)
+                last = tuple(min(lo + n, d) - 1 for lo, n, d in zip(start, ext, shape))
+                if any(a > b for a, b in zip(first, last)):
+                    continue
+                lo_flat, hi_flat = np.ravel_multi_index(first, shape), np.ravel_multi_index(last, shape)
+                near = flat[(flat >= lo_flat) & (flat <= hi_flat)]
+                if near.size == 0:
+                    continue
+                coords = np.unravel_index(near, shape)
+                inside = np.ones(near.shape, bool)
                 for a, (lo, n) in enumerate(zip(start, ext)):
                     inside &= (coords[a] >= lo) & (coords[a] < lo + n)
                 if inside.any():

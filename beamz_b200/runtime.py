@@ -73,15 +73,18 @@ def _replicated_slab(torch, ids, remap, k0: int, k1: int):
 
 
 def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, z_block: int = 32,
-                         with_eps: bool = False):
+                         with_eps: bool = False, ids=None, counts=None):
     """Site-id words (Z+1, Y+1, pitch) int32 and coefficient tables (3, 256) on
     the device; equal bit for bit to :func:`beamz_b200.plan.site_codebook` (the
     device part is integer gathers only; coefficients come from the host).
-    With ``with_eps`` also the (3, 256) site permittivities of the ids."""
+    With ``with_eps`` also the (3, 256) site permittivities of the ids.
+    ``ids`` (the voxel ids already on the device) and ``counts`` (their
+    histogram) save an upload and a host count."""
     torch = _torch()
-    remap_np, eps_used = compact_materials(voxel_ids, eps_table)
+    remap_np, eps_used = compact_materials(voxel_ids, eps_table, counts)
     m = int(eps_used.size)
-    ids = torch.as_tensor(np.ascontiguousarray(voxel_ids, np.uint8), device=device)
+    if ids is None:
+        ids = torch.as_tensor(np.ascontiguousarray(voxel_ids, np.uint8), device=device)
     remap = torch.as_tensor(remap_np, device=device)
     nz, ny, nx = (int(v) for v in ids.shape)
     blocks = [(k, min(k + z_block, nz + 1)) for k in range(0, nz + 1, z_block)]
@@ -122,18 +125,24 @@ class DftArena:
     layout: list  # per monitor: (value_offset, freq_count, point_count, weight_offset)
 
 
-def nonzero_first(indices: np.ndarray, weights: np.ndarray):
-    """Per point (row), move the nonzero-weight neighbours to the front,
-    keeping their order, so a gather may stop at the first zero weight."""
-    order = np.argsort(weights == 0.0, axis=1, kind="stable")
-    return np.take_along_axis(indices, order, axis=1), np.take_along_axis(weights, order, axis=1)
+def voxel_histogram(ids, device):
+    """Counts of every voxel id of a device uint8 tensor (fdtd_voxel_histogram)."""
+    torch = _torch()
+    counts = torch.empty(256, dtype=torch.int32, device=device)
+    lib = abi.load_library()
+    stream = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    b_ids, b_counts = abi.buffer_of(ids), abi.buffer_of(counts)
+    abi.check(lib.fdtd_voxel_histogram(stream, ctypes.byref(b_ids), ctypes.byref(b_counts)), "fdtd_voxel_histogram")
+    return counts.cpu().numpy()
 
 
-def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
-    """Pad every monitor to a common (P, K, F) and lay out the ragged arena.
-
-    ``remap(c, flat)`` converts dense flat offsets of component ``c`` into the
-    device layout's offsets (pitched programs)."""
+def pack_dft_monitors(monitors, device, shapes, strides) -> DftArena | None:
+    """Pad every monitor to a common (P, K, F), lay out the ragged arena, and
+    pack each (monitor, component) gather plan on the device
+    (fdtd_pack_gather): per point the nonzero-weight neighbours first, in
+    order, so a gather may stop at the first zero weight, and every offset in
+    the device layout.  ``shapes[c]`` is component ``c``'s stored shape and
+    ``strides(c)`` the (row, plane) element strides of its device array."""
     if not monitors:
         return None
     M = len(monitors)
@@ -142,8 +151,38 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
     F = max(len(m.freqs) for m in monitors)
     if F > 64:
         raise ValueError("at most 64 frequencies per monitor")
-    indices = np.zeros((M, 6, K, P), np.int32)  # neighbour-major (see FdtdDft)
-    weights = np.zeros((M, 6, K, P), np.float32)
+    torch = _torch()
+    indices = torch.zeros((M, 6, K, P), dtype=torch.int32, device=device)  # neighbour-major (see FdtdDft)
+    weights = torch.zeros((M, 6, K, P), dtype=torch.float32, device=device)
+    lib = abi.load_library()
+    cur = torch.cuda.current_stream(device)
+    stream = ctypes.c_void_p(cur.cuda_stream)
+    # Every (monitor, component) plan goes up in one pinned staging copy.
+    plans = [(m, c, np.asarray(mon.indices[c]).reshape(mon.points, -1), np.asarray(mon.weights[c]))
+             for m, mon in enumerate(monitors) for c in range(6)]
+    total = sum(a.size for _m, _c, a, _w in plans)
+    host_i = torch.empty(total, dtype=torch.int32, pin_memory=True)
+    host_w = torch.empty(total, dtype=torch.float32, pin_memory=True)
+    hi, hw = host_i.numpy(), host_w.numpy()
+    o = 0
+    for _m, _c, a, w in plans:
+        hi[o : o + a.size] = a.reshape(-1)
+        hw[o : o + a.size] = w.reshape(-1)
+        o += a.size
+    dev_i = host_i.to(device, non_blocking=True)
+    dev_w = host_w.to(device, non_blocking=True)
+    o = 0
+    for m, c, a, _w in plans:
+        g = abi.FdtdGatherPack()
+        g.indices_in = abi.buffer_of(dev_i[o : o + a.size].view(a.shape))
+        g.weights_in = abi.buffer_of(dev_w[o : o + a.size].view(a.shape))
+        g.indices_out, g.weights_out = abi.buffer_of(indices[m, c]), abi.buffer_of(weights[m, c])
+        dims = (1,) * (3 - len(shapes[c])) + tuple(shapes[c])  # 2D: z extent 1
+        for ax, n in enumerate(dims):
+            g.dims[ax] = int(n)
+        g.row, g.plane = strides(c)
+        abi.check(lib.fdtd_pack_gather(stream, ctypes.byref(g)), "fdtd_pack_gather")
+        o += a.size
     freqs = np.zeros((M, F), np.float32)
     masks = np.zeros((M, 6), np.float32)
     counts = np.zeros((M, 5), np.int32)
@@ -153,13 +192,6 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
     layout = []
     for m, mon in enumerate(monitors):
         p, nf = mon.points, len(mon.freqs)
-        for c in range(6):
-            ic, wc = mon.indices[c], mon.weights[c]
-            if remap is not None:
-                ic = remap(c, ic)
-            ic, wc = nonzero_first(np.asarray(ic), np.asarray(wc, np.float32))
-            indices[m, c, : ic.shape[1], :p] = ic.T
-            weights[m, c, : wc.shape[1], :p] = wc.T
         freqs[m, :nf] = mon.freqs
         masks[m] = mon.component_mask
         counts[m] = (nf, p, max(1, int(mon.interval)), voff, woff)
@@ -168,9 +200,10 @@ def pack_dft_monitors(monitors, device, remap=None) -> DftArena | None:
         layout.append((voff, nf, p, woff))
         voff += 6 * nf * p
         woff += nf
-    torch = _torch()
     t = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
-    return DftArena(t(indices), t(weights), t(freqs), t(masks), t(counts), t(codes), t(windows), voff, woff, layout)
+    arena = DftArena(indices, weights, t(freqs), t(masks), t(counts), t(codes), t(windows), voff, woff, layout)
+    cur.synchronize()  # the plan is complete before any stream of the program reads it
+    return arena
 
 
 class DeviceProgram:
@@ -201,8 +234,10 @@ class DeviceProgram:
             self.pitch = -(-(nx + 1) // 4) * 4
             self.bank_shape = (nz + 1, ny + 1, self.pitch)
             try:
+                ids = torch.as_tensor(np.ascontiguousarray(spec.voxel_ids, np.uint8), device=dev)
                 self.site_ids, self.site_coef, self.site_eps_table = device_site_codebook(
-                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev, with_eps=True)
+                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev, with_eps=True, ids=ids,
+                    counts=voxel_histogram(ids, dev))
                 layout = "pitched"
             except CodebookOverflow:
                 if layout == "pitched":
@@ -305,7 +340,7 @@ class DeviceProgram:
             d.coeff = buf(_f32(coeff, dev))
             d.waveform = buf(_f32(np.asarray(src.waveform, np.float32).reshape(-1), dev))
         # Monitors.
-        self.arena = pack_dft_monitors(spec.monitors, dev, self._remap if layout == "pitched" else None)
+        self.arena = pack_dft_monitors(spec.monitors, dev, [self.shapes[c] for c in COMPONENTS], self._strides)
         if self.arena is not None:
             a = self.arena
             s.dft.monitor_count = len(spec.monitors)
@@ -314,11 +349,13 @@ class DeviceProgram:
         self._times_for(max(int(spec.total_steps), 1))
         self.struct = s
 
-    def _remap(self, c: int, flat: np.ndarray) -> np.ndarray:
-        """Dense flat offsets of component ``c`` -> pitched offsets."""
-        dz, dy, dx = self.shapes[COMPONENTS[c]]
-        k, j, i = np.unravel_index(np.asarray(flat, np.int64), (dz, dy, dx))
-        return ((k * (self.bank_shape[1]) + j) * self.pitch + i).astype(np.int32)
+    def _strides(self, c: int):
+        """(row, plane) element strides of component ``c``'s device array."""
+        if self.layout == "pitched":
+            return self.pitch, self.bank_shape[1] * self.pitch
+        shape = tuple(self.shapes[COMPONENTS[c]])
+        _dz, dy, dx = (1,) * (3 - len(shape)) + shape  # 2D: z extent 1
+        return dx, dy * dx
 
     def diag_site_eps(self, component: str):
         """Device relative permittivity of one E component over its stored

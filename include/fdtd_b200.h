@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 6
+#define FDTD_ABI_VERSION 7
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -357,6 +357,34 @@ typedef struct FdtdDftChange {
  * copies the arena into prev_re / prev_im.  Masked-off components and
  * frequencies beyond a monitor's count report zeros. */
 int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChange* c);
+
+/* ---- On-device planning -------------------------------------------------
+ * beamz packs monitor gather plans and compacts voxel materials on the host
+ * (beamz/simulation/cuda/runtime.py:530-618, compile.py:146-187); these move
+ * the per-element part of that work to the device. */
+
+/* One (monitor, component) gather plan and where its packed form goes. */
+typedef struct FdtdGatherPack {
+  FdtdBuffer indices_in;   /* S32 [P, Kc]: dense flat offsets into the component */
+  FdtdBuffer weights_in;   /* F32 [P, Kc] */
+  FdtdBuffer indices_out;  /* S32 [K, Pmax] (Kc <= K, P <= Pmax): the program's [M, 6, K, Pmax] slice */
+  FdtdBuffer weights_out;  /* F32 [K, Pmax] */
+  int32_t dims[3];         /* the component's stored extents (z, y, x) */
+  int64_t row, plane;      /* element strides of the device layout (dense: x, y*x; pitched: P, (Y+1)*P) */
+} FdtdGatherPack;
+
+/* Per point p < P: the slots with a nonzero weight first, then the others,
+ * each group in slot order, into rows 0..Kc-1 of column p; each offset
+ * (k, j, i) = unravel(flat, dims) becomes k*plane + j*row + i, an offset
+ * outside the component becomes -1 (never gathered).  Rows Kc..K-1 and
+ * columns P..Pmax-1 are left as they are (zero in a fresh plan).  No beamz
+ * counterpart (its runtime packs on the host). */
+int fdtd_pack_gather(void* stream, const FdtdGatherPack* g);
+
+/* counts[v] = number of voxels with id v (U8 voxels, S32 [256] counts, set
+ * to zero first): the materials a program uses, for the codebook's compact
+ * material indices (beamz compacts on the host, compile.py:146-187). */
+int fdtd_voxel_histogram(void* stream, const FdtdBuffer* voxels, const FdtdBuffer* counts);
 
 /* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
 void fdtd_clear_graph_cache(void);

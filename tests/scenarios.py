@@ -144,3 +144,29 @@ def oracle_state(prog: O.OracleProgram, fields=None, dtype=np.float32):
         for c, v in fields.items():
             st.fields[c] = np.asarray(v, dtype).copy()
     return st
+
+
+def pack_dft_monitors_host(monitors, shapes, strides):
+    """Host restatement of the device gather packing (the engine's earlier host
+    path), for equivalence tests: per monitor and component, the (P, K) plan
+    remapped to the device layout's offsets and reordered nonzero weights
+    first (stable), laid out neighbour-major [M, 6, K, Pmax]."""
+    M = len(monitors)
+    P = max(m.points for m in monitors)
+    K = max(max(np.asarray(a).reshape(m.points, -1).shape[1] for a in m.indices) for m in monitors)
+    indices = np.zeros((M, 6, K, P), np.int32)
+    weights = np.zeros((M, 6, K, P), np.float32)
+    for m, mon in enumerate(monitors):
+        p = mon.points
+        for c in range(6):
+            ic = np.asarray(mon.indices[c]).reshape(p, -1).astype(np.int64)
+            wc = np.asarray(mon.weights[c], np.float32).reshape(p, -1)
+            dims = (1,) * (3 - len(shapes[c])) + tuple(shapes[c])
+            k, j, i = np.unravel_index(ic, dims)
+            row, plane = strides(c)
+            ic = (k * plane + j * row + i).astype(np.int32)
+            order = np.argsort(wc == 0.0, axis=1, kind="stable")
+            ic, wc = np.take_along_axis(ic, order, axis=1), np.take_along_axis(wc, order, axis=1)
+            indices[m, c, : ic.shape[1], :p] = ic.T
+            weights[m, c, : wc.shape[1], :p] = wc.T
+    return indices, weights

@@ -300,6 +300,40 @@ def test_dft_sampling_beside_the_next_step_is_bit_identical(graphs):
     assert np.abs(outs[1]["dft_re"]).max() > 0
 
 
+@pytest.mark.parametrize("case", ["pitched", "dense3d", "tm", "te"])
+def test_device_packed_gather_plans_equal_the_host_packing(case):
+    """fdtd_pack_gather builds the [M, 6, K, P] plan (nonzero weights first,
+    device-layout offsets) bit for bit as the host restatement does,
+    including monitors of different sizes and zero weights between nonzero ones."""
+    from beamz_b200 import workloads as W
+    from tests.scenarios import pack_dft_monitors_host
+
+    if case in ("pitched", "dense3d"):
+        spec = W.scene_3d_512(total_steps=10, shape=(24, 40, 56), pml_cells=4, n_monitors=3, n_freqs=2)
+        schedule = "fused" if case == "pitched" else "phases"
+    else:
+        spec = scenario_2d(grid=(17, 23), polarization=case, nsteps=10)
+        schedule = "fused"
+    mon = spec.monitors[0]
+    w = [np.asarray(a, np.float32).copy() for a in mon.weights]
+    for a in w:  # a zero between nonzero slots, so the reorder moves something
+        if a.shape[1] > 2:
+            a[::3, 0] = 0.0
+    spec.monitors[0] = P.DftMonitorPlan(mon.freqs, mon.indices, w, mon.component_mask)
+    prog = R.compile_program(spec, schedule=schedule)
+    assert (prog.layout == "pitched") == (case == "pitched")
+    idx, wts = pack_dft_monitors_host(spec.monitors, [prog.shapes[c] for c in P.COMPONENTS], prog._strides)
+    np.testing.assert_array_equal(prog.arena.indices.cpu().numpy(), idx)
+    np.testing.assert_array_equal(prog.arena.weights.cpu().numpy(), wts)
+
+
+def test_device_voxel_histogram_counts_every_id():
+    ids = np.random.default_rng(3).integers(0, 7, size=(33, 17, 29)).astype(np.uint8)
+    ids[0, 0, :5] = 250
+    got = R.voxel_histogram(torch.as_tensor(ids, device="cuda"), torch.device("cuda"))
+    np.testing.assert_array_equal(got, np.bincount(ids.reshape(-1), minlength=256))
+
+
 @pytest.mark.parametrize("dims", [3, 2])
 def test_dft_step_batching_is_bit_identical(dims):
     """Samples buffered and flushed every few steps (and at every call's end)

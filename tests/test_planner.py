@@ -160,3 +160,20 @@ def test_sources_clear_of_monitors():
     assert not P.sources_clear_of_monitors(with_source("Ey", "pre_e"))
     assert P.sources_clear_of_monitors(with_source("Ey", "e"))  # written before the sample is taken
     assert P.sources_clear_of_monitors(with_source("Ex", "pre_e"))  # Ex is masked off on these planes
+    # Boxes of every size, some reaching past the grid, against a brute-force scan.
+    shape = P.component_shape("Ey", spec.grid_shape)
+    gathered = set()
+    for m in spec.monitors:
+        if float(m.component_mask[ci]) != 0.0:
+            gathered.update(int(v) for v in np.asarray(m.indices[ci])[np.asarray(m.weights[ci]) != 0])
+    rng = np.random.default_rng(5)
+    for _ in range(40):
+        ext = tuple(int(v) for v in rng.integers(1, 9, 3))
+        start = tuple(int(rng.integers(-3, d)) for d in shape)
+        cells = {int(np.ravel_multi_index((k, j, i), shape))
+                 for k in range(max(start[0], 0), min(start[0] + ext[0], shape[0]))
+                 for j in range(max(start[1], 0), min(start[1] + ext[1], shape[1]))
+                 for i in range(max(start[2], 0), min(start[2] + ext[2], shape[2]))}
+        src = P.SourcePlan("Ey", "pre_e", start, np.ones(ext, np.float32), np.zeros(4, np.float32))
+        got = P.sources_clear_of_monitors(dataclasses.replace(spec, sources=[src]))
+        assert got == (not (cells & gathered)), (start, ext)
