@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 7
+FDTD_ABI_VERSION = 8
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
@@ -209,6 +209,8 @@ class FdtdProgram(ctypes.Structure):
         ("step_counter", FdtdBuffer),
         ("step_time", FdtdBuffer),
         ("status", FdtdBuffer),
+        ("metric_h", FdtdBuffer * 3),
+        ("metric_e", FdtdBuffer * 3),
     ]
 
 

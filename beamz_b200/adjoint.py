@@ -55,6 +55,8 @@ class AdjointProblem:
         torch = _torch()
         if spec.e_site is None:
             raise ValueError("the adjoint needs a per-site E material (ProgramSpec.e_site)")
+        if spec.metrics is not None:
+            raise ValueError("the adjoint step is the transpose of the isotropic-grid step (no derivative metrics)")
         self.runtime = runtime
         self.spec = spec
         self.nsteps = int(nsteps)

@@ -152,12 +152,12 @@ __device__ __forceinline__ float add_h_sources(const Step3D& p, const float* amp
 // Backward difference at `coord` of an axis with n samples, with beamz's ghost
 // planes (beamz/lattice.py:523-551): zero beyond a metallic wall, otherwise a
 // copy of the edge sample, so the edge derivative vanishes.
-__device__ __forceinline__ float ghost_diff(float center, float below, int coord, int n, bool low_wall, bool high_wall,
-                                            float res, float inv_res) {
+__device__ __forceinline__ float ghost_diff(const Step3D& p, int axis, float center, float below, int coord, int n,
+                                            bool low_wall, bool high_wall) {
   if (n == 0) return 0.0f;
-  if (coord == 0) return low_wall ? div_rn(center - 0.0f, res, inv_res) : 0.0f;
-  if (coord == n) return high_wall ? div_rn(0.0f - below, res, inv_res) : 0.0f;
-  return div_rn(center - below, res, inv_res);
+  if (coord == 0) return low_wall ? de(p, axis, coord, center - 0.0f) : 0.0f;
+  if (coord == n) return high_wall ? de(p, axis, coord, 0.0f - below) : 0.0f;
+  return de(p, axis, coord, center - below);
 }
 
 // Staged E value; components outside the active set read as zero (2D).
@@ -179,7 +179,6 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
   const int k0 = blockIdx.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, kmax);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
-  const float res = p.res, inv_res = p.inv_res;
 
   if (Mat == FDTD_MATERIAL_VOXEL) {
     for (int e = tid; e < 256; e += NT) sm.table[e] = p.em.eps_table[e];
@@ -231,8 +230,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
       const bool own = ly > 0 && lx > 0 && emit;
       float hx = 0.0f, hy = 0.0f, hz = 0.0f;
       if (((Active >> 3) & 1) && k < dHx.z && j >= 0 && j < dHx.y && i >= 0 && i < dHx.x) {
-        float d0 = div_rn(ev<Active>(sm, e0, 2, ly + 1, lx) - ev<Active>(sm, e0, 2, ly, lx), res, inv_res);
-        float d1 = div_rn(ev<Active>(sm, e1, 1, ly, lx) - ev<Active>(sm, e0, 1, ly, lx), res, inv_res);
+        float d0 = dh(p, 1, j, ev<Active>(sm, e0, 2, ly + 1, lx) - ev<Active>(sm, e0, 2, ly, lx));
+        float d1 = dh(p, 0, k, ev<Active>(sm, e1, 1, ly, lx) - ev<Active>(sm, e0, 1, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<1>(p.ht[0], d0, k, j, i, own);
           d1 = cpml_correct<0>(p.ht[1], d1, k, j, i, own);
@@ -244,8 +243,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         if (own) p.hout[0][o] = hx;
       }
       if (((Active >> 4) & 1) && k < dHy.z && j >= 0 && j < dHy.y && i >= 0 && i < dHy.x) {
-        float d0 = div_rn(ev<Active>(sm, e1, 0, ly, lx) - ev<Active>(sm, e0, 0, ly, lx), res, inv_res);
-        float d1 = div_rn(ev<Active>(sm, e0, 2, ly, lx + 1) - ev<Active>(sm, e0, 2, ly, lx), res, inv_res);
+        float d0 = dh(p, 0, k, ev<Active>(sm, e1, 0, ly, lx) - ev<Active>(sm, e0, 0, ly, lx));
+        float d1 = dh(p, 2, i, ev<Active>(sm, e0, 2, ly, lx + 1) - ev<Active>(sm, e0, 2, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<0>(p.ht[2], d0, k, j, i, own);
           d1 = cpml_correct<2>(p.ht[3], d1, k, j, i, own);
@@ -257,8 +256,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         if (own) p.hout[1][o] = hy;
       }
       if (((Active >> 5) & 1) && k < dHz.z && j >= 0 && j < dHz.y && i >= 0 && i < dHz.x) {
-        float d0 = div_rn(ev<Active>(sm, e0, 1, ly, lx + 1) - ev<Active>(sm, e0, 1, ly, lx), res, inv_res);
-        float d1 = div_rn(ev<Active>(sm, e0, 0, ly + 1, lx) - ev<Active>(sm, e0, 0, ly, lx), res, inv_res);
+        float d0 = dh(p, 2, i, ev<Active>(sm, e0, 1, ly, lx + 1) - ev<Active>(sm, e0, 1, ly, lx));
+        float d1 = dh(p, 1, j, ev<Active>(sm, e0, 0, ly + 1, lx) - ev<Active>(sm, e0, 0, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<2>(p.ht[4], d0, k, j, i, own);
           d1 = cpml_correct<1>(p.ht[5], d1, k, j, i, own);
@@ -281,8 +280,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
       const int pb = hb ^ 1;  // H(k-1), never read at k == 0 (ghost branch)
       const int v0 = (k + 2) % 3, v1 = k % 3;  // voxel planes clip(k-1), clip(k)
       if (((Active >> 0) & 1) && k < dEx.z && j < dEx.y && i < dEx.x) {
-        float d0 = ghost_diff(sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly - 1][lx], j, dHz.y, wy0, wy1, res, inv_res);
-        float d1 = ghost_diff(sm.hn[hb][1][ly][lx], sm.hn[pb][1][ly][lx], k, dHy.z, wz0, wz1, res, inv_res);
+        float d0 = ghost_diff(p, 1, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly - 1][lx], j, dHz.y, wy0, wy1);
+        float d1 = ghost_diff(p, 0, sm.hn[hb][1][ly][lx], sm.hn[pb][1][ly][lx], k, dHy.z, wz0, wz1);
         if (Cpml) {
           d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
           d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -300,8 +299,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         p.eout[0][o] = e;
       }
       if (((Active >> 1) & 1) && k < dEy.z && j < dEy.y && i < dEy.x) {
-        float d0 = ghost_diff(sm.hn[hb][0][ly][lx], sm.hn[pb][0][ly][lx], k, dHx.z, wz0, wz1, res, inv_res);
-        float d1 = ghost_diff(sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly][lx - 1], i, dHz.x, wx0, wx1, res, inv_res);
+        float d0 = ghost_diff(p, 0, sm.hn[hb][0][ly][lx], sm.hn[pb][0][ly][lx], k, dHx.z, wz0, wz1);
+        float d1 = ghost_diff(p, 2, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly][lx - 1], i, dHz.x, wx0, wx1);
         if (Cpml) {
           d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
           d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -319,8 +318,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         p.eout[1][o] = e;
       }
       if (((Active >> 2) & 1) && k < dEz.z && j < dEz.y && i < dEz.x) {
-        float d0 = ghost_diff(sm.hn[hb][1][ly][lx], sm.hn[hb][1][ly][lx - 1], i, dHy.x, wx0, wx1, res, inv_res);
-        float d1 = ghost_diff(sm.hn[hb][0][ly][lx], sm.hn[hb][0][ly - 1][lx], j, dHx.y, wy0, wy1, res, inv_res);
+        float d0 = ghost_diff(p, 2, sm.hn[hb][1][ly][lx], sm.hn[hb][1][ly][lx - 1], i, dHy.x, wx0, wx1);
+        float d1 = ghost_diff(p, 1, sm.hn[hb][0][ly][lx], sm.hn[hb][0][ly - 1][lx], j, dHx.y, wy0, wy1);
         if (Cpml) {
           d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
           d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);

@@ -155,13 +155,13 @@ __device__ __forceinline__ void store_vox(typename L::Smem& sm, const VoxRegs<R>
   }
 }
 
-__device__ __forceinline__ float ghost(float center, float below, bool at_low, bool at_high, bool low_wall,
-                                       bool high_wall, float res, float inv_res) {
+__device__ __forceinline__ float ghost(const Step3D& p, int axis, int coord, float center, float below, bool at_low,
+                                       bool at_high, bool low_wall, bool high_wall) {
   // beamz/lattice.py:523-551: zero beyond a metallic wall, else a copy of the
   // edge sample so that the edge derivative vanishes.
-  if (at_low) return low_wall ? div_rn(center - 0.0f, res, inv_res) : 0.0f;
-  if (at_high) return high_wall ? div_rn(0.0f - below, res, inv_res) : 0.0f;
-  return div_rn(center - below, res, inv_res);
+  if (at_low) return low_wall ? de(p, axis, coord, center - 0.0f) : 0.0f;
+  if (at_high) return high_wall ? de(p, axis, coord, 0.0f - below) : 0.0f;
+  return de(p, axis, coord, center - below);
 }
 
 __device__ __forceinline__ float h_sources(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
@@ -198,8 +198,6 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
   const int k0 = blockIdx.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, Z + 1);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
-  const float res = p.res, inv_res = p.inv_res;
-
   if (Mat == FDTD_MATERIAL_VOXEL)
     for (int e = tid; e < 256; e += L::NT) sm.table[e] = p.em.eps_table[e];
   if (tid < p.n_hsrc) sm.amp[tid] = source_amplitude(p.hsrc[tid], p.step_counter[0] + p.step_offset);
@@ -261,8 +259,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       const float ez = sm.e[e0][2][ly][lx], ey = sm.e[e0][1][ly][lx], ex = sm.e[e0][0][ly][lx];
       if (which & 1) {  // Hx: dEz/dy - dEy/dz
         const bool ok = zZ && yY && iX1;
-        float d0 = div_rn(sm.e[e0][2][ly + 1][lx] - ez, res, inv_res);
-        float d1 = div_rn(sm.e[e1][1][ly][lx] - ey, res, inv_res);
+        float d0 = dh(p, 1, j, sm.e[e0][2][ly + 1][lx] - ez);
+        float d1 = dh(p, 0, k, sm.e[e1][1][ly][lx] - ey);
         if (cpml && ok) {
           d0 = cpml_correct<1>(p.ht[0], d0, k, j, ii, own);
           d1 = cpml_correct<0>(p.ht[1], d1, k, j, ii, own);
@@ -277,8 +275,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 2) {  // Hy: dEx/dz - dEz/dx
         const bool ok = zZ && yY1 && iX;
-        float d0 = div_rn(sm.e[e1][0][ly][lx] - ex, res, inv_res);
-        float d1 = div_rn(sm.e[e0][2][ly][lx + 1] - ez, res, inv_res);
+        float d0 = dh(p, 0, k, sm.e[e1][0][ly][lx] - ex);
+        float d1 = dh(p, 2, ii, sm.e[e0][2][ly][lx + 1] - ez);
         if (cpml && ok) {
           d0 = cpml_correct<0>(p.ht[2], d0, k, j, ii, own);
           d1 = cpml_correct<2>(p.ht[3], d1, k, j, ii, own);
@@ -293,8 +291,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 4) {  // Hz: dEy/dx - dEx/dy
         const bool ok = yY && iX;
-        float d0 = div_rn(sm.e[e0][1][ly][lx + 1] - ey, res, inv_res);
-        float d1 = div_rn(sm.e[e0][0][ly + 1][lx] - ex, res, inv_res);
+        float d0 = dh(p, 2, ii, sm.e[e0][1][ly][lx + 1] - ey);
+        float d1 = dh(p, 1, j, sm.e[e0][0][ly + 1][lx] - ex);
         if (cpml && ok) {
           d0 = cpml_correct<2>(p.ht[4], d0, k, j, ii, own);
           d1 = cpml_correct<1>(p.ht[5], d1, k, j, ii, own);
@@ -330,8 +328,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         const float hx = sm.hn[hb][0][ly][lx], hy = sm.hn[hb][1][ly][lx], hz = sm.hn[hb][2][ly][lx];
         // Ex: dHz/dy - dHy/dz
         if (yY1 && xX) {
-          float d0 = ghost(hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1, res, inv_res);
-          float d1 = ghost(hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1, res, inv_res);
+          float d0 = ghost(p, 1, j, hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1);
+          float d1 = ghost(p, 0, k, hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1);
           if (cpml) {
             d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
             d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -350,8 +348,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ey: dHx/dz - dHz/dx
         if (yY && xX1) {
-          float d0 = ghost(hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1, res, inv_res);
-          float d1 = ghost(hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1, res, inv_res);
+          float d0 = ghost(p, 0, k, hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1);
+          float d1 = ghost(p, 2, i, hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1);
           if (cpml) {
             d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
             d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -370,8 +368,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ez: dHy/dx - dHx/dy
         if (zZ && yY1 && xX1) {
-          float d0 = ghost(hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1, res, inv_res);
-          float d1 = ghost(hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1, res, inv_res);
+          float d0 = ghost(p, 2, i, hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1);
+          float d1 = ghost(p, 1, j, hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1);
           if (cpml) {
             d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
             d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);

@@ -21,6 +21,26 @@ __device__ __forceinline__ float h_update(const HMaterial& m, int c, int64_t o, 
 
 __device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
 
+__device__ __forceinline__ int axis_cells(const Step3D& p, int axis) { return axis == 0 ? p.Z : (axis == 1 ? p.Y : p.X); }
+
+// A forward difference of E along `axis` at H coordinate `c`, as a derivative:
+// times the inverse distance of a metric grid (beamz/simulation/kernels.py:
+// 164-176, 293-323; cuda/src/update.cu:172-203), else divided by the cell
+// size (kernels.py:477-488).  Coordinates of halo cells that are never
+// stored are clamped into the metric.
+__device__ __forceinline__ float dh(const Step3D& p, int axis, int c, float diff) {
+  const float* m = p.metric_h[axis];
+  if (m == nullptr) return div_rn(diff, p.res, p.inv_res);
+  return diff * m[clampi(c, axis_cells(p, axis) - 1)];
+}
+
+// A backward difference of H along `axis` at E coordinate `c` (0..n_axis).
+__device__ __forceinline__ float de(const Step3D& p, int axis, int c, float diff) {
+  const float* m = p.metric_e[axis];
+  if (m == nullptr) return div_rn(diff, p.res, p.inv_res);
+  return diff * m[clampi(c, axis_cells(p, axis))];
+}
+
 __device__ __forceinline__ float vox_eps(const EMaterial& m, int Z, int Y, int X, int k, int j, int i) {
   k = clampi(k, Z - 1);
   j = clampi(j, Y - 1);

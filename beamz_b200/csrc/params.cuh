@@ -56,6 +56,9 @@ struct Step3D {
   // FDTD_LAYOUT_PITCHED: floats per row of every field and site-id array.
   int pitch;
   int* status;  // optional error word for expired bounded waits
+  // Derivative metrics per axis (z, y, x), or null (isotropic: divide by res).
+  const float* metric_h[3];  // [n_axis]: forward differences feeding H
+  const float* metric_e[3];  // [n_axis + 1]: backward differences feeding E
 };
 
 // 2D (canonical xy plane) step/phase parameters; z extent is 1.

@@ -30,13 +30,14 @@ __device__ __forceinline__ float ld(const Step3D& p, const float* const* base, i
 }
 
 // Forward difference of E component `c` along `axis` at (k, j, i), divided by
-// the cell size (beamz/simulation/kernels.py:477-488: jnp.diff(...) / resolution).
+// the cell size (beamz/simulation/kernels.py:477-488: jnp.diff(...) / resolution)
+// or scaled by the grid's metric (kernels.py:506-551).
 template <int Active>
 __device__ __forceinline__ float fdiff(const Step3D& p, int c, int axis, int k, int j, int i) {
   if (!active<Active>(c)) return 0.0f;
   const float lo = ld<Active>(p, p.ein, c, k, j, i);
   const float hi = ld<Active>(p, p.ein, c, k + (axis == 0), j + (axis == 1), i + (axis == 2));
-  return div_rn(hi - lo, p.res, p.inv_res);
+  return dh(p, axis, axis == 0 ? k : (axis == 1 ? j : i), hi - lo);
 }
 
 // Backward difference of H component `c` along `axis` with beamz's ghost
@@ -51,16 +52,15 @@ __device__ __forceinline__ float bdiff(const Step3D& p, int c, int axis, int k, 
   if (n == 0) return 0.0f;
   if (coord == 0) {
     if (!wall(p.metallic, axis, false)) return 0.0f;
-    return div_rn(ld<Active>(p, p.hin, c, k, j, i) - 0.0f, p.res, p.inv_res);
+    return de(p, axis, coord, ld<Active>(p, p.hin, c, k, j, i) - 0.0f);
   }
   if (coord == n) {
     if (!wall(p.metallic, axis, true)) return 0.0f;
-    return div_rn(0.0f - ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2)),
-                  p.res, p.inv_res);
+    return de(p, axis, coord, 0.0f - ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2)));
   }
   const float hi = ld<Active>(p, p.hin, c, k, j, i);
   const float lo = ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2));
-  return div_rn(hi - lo, p.res, p.inv_res);
+  return de(p, axis, coord, hi - lo);
 }
 
 template <int Active, bool Cpml, int Mat>

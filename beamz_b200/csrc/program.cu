@@ -82,6 +82,12 @@ bool check_coeff(const FdtdBuffer& b, int64_t full) {
   return n == 1 || n == full;
 }
 
+bool has_metric(const FdtdProgram& p) {
+  for (int a = 0; a < 3; ++a)
+    if (p.metric_h[a].data != nullptr || p.metric_e[a].data != nullptr) return true;
+  return false;
+}
+
 int validate(const FdtdProgram& p) {
   if (p.abi_version != FDTD_ABI_VERSION) return kInvalid;
   Layout L;
@@ -123,6 +129,19 @@ int validate(const FdtdProgram& p) {
         return kInvalid;
     } else {
       if (!check_coeff(p.h_decay[c - 3], n) || !check_coeff(p.h_source_site[c - 3], n)) return kInvalid;
+    }
+  }
+  if (has_metric(p)) {
+    if (pitched) return kInvalid;
+    for (int a = 0; a < 3; ++a) {
+      const int n = a == 0 ? L.Z : (a == 1 ? L.Y : L.X);
+      const FdtdBuffer &mh = p.metric_h[a], &me = p.metric_e[a];
+      if (p.ndim == 2 && a == 0) {
+        if (mh.data != nullptr || me.data != nullptr) return kInvalid;
+        continue;
+      }
+      if (!is_f32(mh) || mh.rank != 1 || mh.dims[0] != n || mh.data == nullptr) return kInvalid;
+      if (!is_f32(me) || me.rank != 1 || me.dims[0] != n + 1 || me.data == nullptr) return kInvalid;
     }
   }
   if (p.material_kind == FDTD_MATERIAL_VOXEL) {
@@ -292,6 +311,10 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   s.z_chunk = p.z_chunk;
   s.pitch = static_cast<int>(p.pitch);
   s.status = static_cast<int*>(p.status.data);
+  for (int a = 0; a < 3; ++a) {
+    s.metric_h[a] = static_cast<const float*>(p.metric_h[a].data);
+    s.metric_e[a] = static_cast<const float*>(p.metric_e[a].data);
+  }
   // An axis without absorber terms has no slab anywhere, the faces included.
   for (int a = 0; a < 3; ++a) {
     s.cpml_inner[a][0] = -(1 << 30);
@@ -698,6 +721,7 @@ bool f32_sized(const FdtdBuffer& b, int64_t n) { return is_f32(b) && b.data != n
 int check_adjoint(const FdtdProgram& p, const FdtdAdjointStep& a, const Layout& L, bool need_box) {
   if (a.abi_version != FDTD_ABI_VERSION) return kInvalid;
   if (p.layout != FDTD_LAYOUT_DENSE) return kInvalid;
+  if (has_metric(p)) return kInvalid;  // the transpose is written for the isotropic step
   const int64_t bz = a.box_hi[0] - a.box_lo[0], by = a.box_hi[1] - a.box_lo[1], bx = a.box_hi[2] - a.box_lo[2];
   bool any_box = false;
   for (int c = 0; c < 3; ++c) any_box = any_box || a.curl[c].data != nullptr || a.grad[c].data != nullptr;

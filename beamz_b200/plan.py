@@ -641,6 +641,75 @@ def step_times(t0: float, dt: float, nsteps: int) -> np.ndarray:
 # ---------------------------------------------------------------------------
 
 
+METRIC_NAMES = ("e_to_h_x", "e_to_h_y", "e_to_h_z", "h_to_e_x", "h_to_e_y", "h_to_e_z")
+
+
+@dataclass(frozen=True)
+class DerivativeMetrics:
+    """Separable inverse distances of the staggered derivatives of an
+    axis-uniform or rectilinear grid (beamz/simulation/model.py:290-303).
+
+    ``e_to_h_a`` multiplies the forward differences along axis ``a`` that
+    feed H (one value per cell, or one scalar on an axis-uniform grid);
+    ``h_to_e_a`` the backward differences that feed E (cells + 1 values, or
+    one scalar).  An axis the grid lacks (z in 2D) holds an empty array."""
+
+    e_to_h_x: np.ndarray
+    e_to_h_y: np.ndarray
+    e_to_h_z: np.ndarray
+    h_to_e_x: np.ndarray
+    h_to_e_y: np.ndarray
+    h_to_e_z: np.ndarray
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n in METRIC_NAMES}
+
+    def along(self, name: str, n: int) -> np.ndarray:
+        """``name``'s inverse distances as ``n`` float32 values (a scalar is
+        repeated), the form the device takes."""
+        v = np.asarray(getattr(self, name), np.float32)
+        if v.ndim == 0:
+            return np.full(n, v, np.float32)
+        if v.shape != (n,):
+            raise ValueError(f"{name}: {v.shape[0]} inverse distances for {n} positions")
+        return np.ascontiguousarray(v)
+
+
+def derivative_metrics(widths: dict, kind: str = "rectilinear") -> DerivativeMetrics | None:
+    """Inverse distances from per-axis cell widths (``{"x": w, "y": w[, "z": w]}``
+    in metres, float64), as beamz compiles them (compile.py:209-239):
+
+    * ``"isotropic_uniform"``: None (every difference over the cell size);
+    * ``"axis_uniform"``: one float32 scalar 1/w[0] per axis, both staggers;
+    * ``"rectilinear"``: forward 1/w per cell; backward 1/w[0], then
+      2/(w[i-1] + w[i]) between cells, then 1/w[-1]; each computed in float64
+      and rounded once to float32.
+    """
+    if kind == "isotropic_uniform":
+        return None
+    if kind not in ("axis_uniform", "rectilinear"):
+        raise ValueError(f"unknown metric kind {kind!r}")
+    empty = np.zeros((0,), np.float32)
+    forward, backward = {}, {}
+    for axis in ("x", "y", "z"):
+        if axis not in widths:
+            continue
+        w = np.asarray(widths[axis], np.float64).reshape(-1)
+        if w.size == 0 or not np.all(w > 0):
+            raise ValueError(f"axis {axis}: cell widths must be positive")
+        if kind == "axis_uniform":
+            forward[axis] = backward[axis] = np.float32(1.0 / float(w[0]))
+            continue
+        back = np.empty(w.size + 1, np.float64)
+        back[0], back[-1] = 1.0 / w[0], 1.0 / w[-1]
+        if w.size > 1:
+            back[1:-1] = 2.0 / (w[:-1] + w[1:])
+        forward[axis] = (1.0 / w).astype(np.float32)
+        backward[axis] = back.astype(np.float32)
+    return DerivativeMetrics(*(forward.get(a, empty) for a in ("x", "y", "z")),
+                             *(backward.get(a, empty) for a in ("x", "y", "z")))
+
+
 @dataclass
 class ProgramSpec:
     """Host description of one simulation's step program."""
@@ -665,6 +734,9 @@ class ProgramSpec:
     monitors: list = field(default_factory=list)
     total_steps: int = 1
     t0: float = 0.0
+    # Derivative metrics of an axis-uniform or rectilinear grid; None on the
+    # isotropic grid (differences over `resolution`).
+    metrics: DerivativeMetrics | None = None
 
     @property
     def ndim(self) -> int:

@@ -222,9 +222,11 @@ class DeviceProgram:
         self.shapes = {c: component_shape(c, spec.grid_shape, spec.polarization) for c in COMPONENTS}
         dev = self.device
         h_uniform = all(np.ndim(d) == 0 and np.ndim(s_) == 0 for d, s_ in spec.h_coefficients().values())
-        pitched_ok = (spec.ndim == 3 and spec.voxel_ids is not None and schedule == "fused" and h_uniform)
+        pitched_ok = (spec.ndim == 3 and spec.voxel_ids is not None and schedule == "fused" and h_uniform
+                      and spec.metrics is None)
         if layout == "pitched" and not pitched_ok:
-            raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule and uniform H")
+            raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule, uniform H and an "
+                             "isotropic grid")
         f32 = np.float32
         dt_over_eps = f32(spec.dt) / f32(EPS_0)
         self.site_ids = self.site_coef = self.site_eps_table = None
@@ -339,6 +341,16 @@ class DeviceProgram:
                 coeff = coeff.reshape((1, *coeff.shape))
             d.coeff = buf(_f32(coeff, dev))
             d.waveform = buf(_f32(np.asarray(src.waveform, np.float32).reshape(-1), dev))
+        # Derivative metrics (axis-uniform / rectilinear grids).
+        if spec.metrics is not None:
+            cells = tuple(int(v) for v in spec.grid_shape)
+            axes = (("z", cells[0]), ("y", cells[1]), ("x", cells[2])) if spec.ndim == 3 else (
+                (None, 0), ("y", cells[0]), ("x", cells[1]))
+            for a, (name, n) in enumerate(axes):
+                if name is None:
+                    continue
+                s.metric_h[a] = buf(_f32(spec.metrics.along(f"e_to_h_{name}", n), dev))
+                s.metric_e[a] = buf(_f32(spec.metrics.along(f"h_to_e_{name}", n + 1), dev))
         # Monitors.
         self.arena = pack_dft_monitors(spec.monitors, dev, [self.shapes[c] for c in COMPONENTS], self._strides)
         if self.arena is not None:

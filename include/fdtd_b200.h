@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 7
+#define FDTD_ABI_VERSION 8
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -211,6 +211,17 @@ typedef struct FdtdProgram {
   FdtdBuffer step_counter; /* S32 [1]: absolute step of the next step, advanced on device */
   FdtdBuffer step_time;    /* F32 [T]: t + dt after absolute step s (FP32-accumulated clock) */
   FdtdBuffer status;       /* S32 [1], optional: set nonzero when a bounded device wait expired */
+  /* Derivative metrics of an axis-uniform or rectilinear grid (beamz:
+   * DerivativeMetricPlan, model.py:290-303; BeamzLaunch metric_kind/metrics,
+   * cuda/src/launch.h:24-33).  All null: the isotropic grid, each difference
+   * divided by `resolution`.  Otherwise, for every axis a of the grid (z, y, x;
+   * 2D: y, x, with z null), metric_h[a] is F32 [n_a] (n_a = cells along a):
+   * the inverse distances that multiply the forward differences of the H
+   * update at each H coordinate; metric_e[a] is F32 [n_a + 1], those of the
+   * backward differences of the E update at each E coordinate (an axis-uniform
+   * grid repeats one value).  FDTD_LAYOUT_DENSE only; no adjoint. */
+  FdtdBuffer metric_h[3];
+  FdtdBuffer metric_e[3];
 } FdtdProgram;
 
 /* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */

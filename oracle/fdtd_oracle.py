@@ -491,6 +491,26 @@ def _ghost_pad_2d(arr, axis, metallic_edges):
     return np.concatenate((low, arr, high), axis=axis)
 
 
+def _metric_diff(arr, axis, res, inverse_distance=None):
+    """Difference along ``axis`` over the cell size: ``np.diff / res`` on an
+    isotropic grid (kernels.py:477-488), ``np.diff * inverse_distance`` (a
+    scalar or one value per difference along the axis) with a derivative
+    metric (kernels.py:164-176)."""
+    d = np.diff(arr, axis=axis)
+    if inverse_distance is None:
+        return d / res
+    m = np.asarray(inverse_distance, d.dtype)
+    if m.ndim == 0:
+        return d * m
+    shape = [1] * d.ndim
+    shape[axis] = m.shape[0]
+    return d * m.reshape(shape)
+
+
+def _metric(metrics, name):
+    return None if metrics is None else metrics[name]
+
+
 @dataclass
 class Material3D:
     """E-site permittivity (and optional conductivity) plus H-site magnetic
@@ -511,9 +531,13 @@ def material_from_voxels(voxel_eps: np.ndarray, voxel_sigma=None, dtype=np.float
     return Material3D(eps, tuple(sample_e_site_3d(s, c) for c in ("Ex", "Ey", "Ez")))
 
 
-def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0), coeffs=None):
+def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0), coeffs=None, metrics=None):
     """beamz/simulation/kernels.py:458-503 (``h_terms`` empty => kernels.py:267-290
     without CPML).  Returns (hx, hy, hz, psi_h).
+
+    ``metrics`` (a mapping with beamz's ``DerivativeMetricPlan`` names,
+    model.py:290-303) scales each difference by its inverse distance instead
+    of dividing by the cell size (kernels.py:293-323, 506-551).
 
     ``coeffs`` (component -> (decay, source) arrays) selects the form of
     beamz's CUDA path instead, which receives precomputed coefficients:
@@ -524,12 +548,12 @@ def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0),
     f = dtype.type
     res = f(resolution)
     derivs = (
-        np.diff(ez, axis=1) / res,
-        np.diff(ey, axis=0) / res,
-        np.diff(ex, axis=0) / res,
-        np.diff(ez, axis=2) / res,
-        np.diff(ey, axis=2) / res,
-        np.diff(ex, axis=1) / res,
+        _metric_diff(ez, 1, res, _metric(metrics, "e_to_h_y")),
+        _metric_diff(ey, 0, res, _metric(metrics, "e_to_h_z")),
+        _metric_diff(ex, 0, res, _metric(metrics, "e_to_h_z")),
+        _metric_diff(ez, 2, res, _metric(metrics, "e_to_h_x")),
+        _metric_diff(ey, 2, res, _metric(metrics, "e_to_h_x")),
+        _metric_diff(ex, 1, res, _metric(metrics, "e_to_h_y")),
     )
     one = f(1.0)
     dt_over_mu = f(dt) / f(MU_0)
@@ -565,9 +589,11 @@ def update_h_3d(fields, psi_h, h_terms, dt, resolution, sigma_m=(0.0, 0.0, 0.0),
     return out[0].astype(dtype), out[1].astype(dtype), out[2].astype(dtype), new_psi
 
 
-def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, metallic_edges=(), coeffs=None):
+def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, metallic_edges=(), coeffs=None,
+                metrics=None):
     """beamz/simulation/kernels.py:554-626 (``e_terms`` empty =>
-    kernels.py:326-388).  Returns (ex, ey, ez, psi_e)."""
+    kernels.py:326-388).  Returns (ex, ey, ez, psi_e).  ``metrics`` as in
+    :func:`update_h_3d` (kernels.py:391-455, 629-701)."""
     ex, ey, ez, hx, hy, hz = (fields[c] for c in COMPONENTS)
     dtype = ex.dtype
     f = dtype.type
@@ -581,12 +607,12 @@ def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, me
         "hx_y": _ghost_pad(hx, 1, metallic_edges),
     }
     derivs = (
-        np.diff(views["hz_y"], axis=1) / res,
-        np.diff(views["hy_z"], axis=0) / res,
-        np.diff(views["hx_z"], axis=0) / res,
-        np.diff(views["hz_x"], axis=2) / res,
-        np.diff(views["hy_x"], axis=2) / res,
-        np.diff(views["hx_y"], axis=1) / res,
+        _metric_diff(views["hz_y"], 1, res, _metric(metrics, "h_to_e_y")),
+        _metric_diff(views["hy_z"], 0, res, _metric(metrics, "h_to_e_z")),
+        _metric_diff(views["hx_z"], 0, res, _metric(metrics, "h_to_e_z")),
+        _metric_diff(views["hz_x"], 2, res, _metric(metrics, "h_to_e_x")),
+        _metric_diff(views["hy_x"], 2, res, _metric(metrics, "h_to_e_x")),
+        _metric_diff(views["hx_y"], 1, res, _metric(metrics, "h_to_e_y")),
     )
     one = f(1.0)
     dt_over_eps = f(dt) / f(EPS_0)
@@ -643,11 +669,12 @@ def e_coefficients_2d(eps_site, dt, dtype=np.float32):
     return np.ones_like(eps), (f(dt) / (f(EPS_0) * eps)).astype(dtype)
 
 
-def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm"):
+def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm", metrics=None):
     """TM: beamz/simulation/kernels.py:731-738, 771-788, 1217-1243;
     TE: kernels.py:791-797, 838-850, 1286-1300.  ``h_coeffs`` is one
     (decay, source) pair for every H component, or a dict component ->
-    (decay, source) (per-site arrays of a magnetically lossy material)."""
+    (decay, source) (per-site arrays of a magnetically lossy material).
+    ``metrics``: inverse distances as in :func:`update_h_3d` (kernels.py:880-1012)."""
     dtype = fields["Ez" if polarization == "tm" else "Hz"].dtype
     res = dtype.type(resolution)
     per = h_coeffs if isinstance(h_coeffs, dict) else None
@@ -655,8 +682,8 @@ def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm")
     new_psi = list(psi_h) if psi_h else []
     if polarization == "tm":
         ez, hx, hy = fields["Ez"], fields["Hx"], fields["Hy"]
-        d0 = (ez[1:, :] - ez[:-1, :]) / res
-        d1 = (ez[:, 1:] - ez[:, :-1]) / res
+        d0 = _metric_diff(ez, 0, res, _metric(metrics, "e_to_h_y"))
+        d1 = _metric_diff(ez, 1, res, _metric(metrics, "e_to_h_x"))
         if h_terms:
             c0, new_psi[0] = correct_cpml_term(d0, psi_h[0], h_terms[0])
             c1, new_psi[1] = correct_cpml_term(d1, psi_h[1], h_terms[1])
@@ -668,8 +695,8 @@ def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm")
         hy_n = decay * hy - source * c1
         return {"Hx": hx_n.astype(dtype), "Hy": hy_n.astype(dtype)}, new_psi
     ex, ey, hz = fields["Ex"], fields["Ey"], fields["Hz"]
-    d0 = (ey[:, 1:] - ey[:, :-1]) / res
-    d1 = (ex[1:, :] - ex[:-1, :]) / res
+    d0 = _metric_diff(ey, 1, res, _metric(metrics, "e_to_h_x"))
+    d1 = _metric_diff(ex, 0, res, _metric(metrics, "e_to_h_y"))
     if h_terms:
         c0, new_psi[0] = correct_cpml_term(d0, psi_h[0], h_terms[0])
         c1, new_psi[1] = correct_cpml_term(d1, psi_h[1], h_terms[1])
@@ -679,7 +706,7 @@ def update_h_2d(fields, psi_h, h_terms, resolution, h_coeffs, polarization="tm")
     return {"Hz": (decay * hz - source * curl).astype(dtype)}, new_psi
 
 
-def update_e_2d(fields, psi_e, e_terms, resolution, e_coeffs, metallic_edges=(), polarization="tm"):
+def update_e_2d(fields, psi_e, e_terms, resolution, e_coeffs, metallic_edges=(), polarization="tm", metrics=None):
     """TM: kernels.py:741-769, 800-823, 1258-1283; TE: kernels.py:800-836,
     852-860, 1303-1342.  ``e_coeffs`` maps component -> (decay, source)."""
     new_psi = list(psi_e) if psi_e else []
@@ -689,8 +716,8 @@ def update_e_2d(fields, psi_e, e_terms, resolution, e_coeffs, metallic_edges=(),
         res = dtype.type(resolution)
         phy = _ghost_pad_2d(hy, 1, metallic_edges)
         phx = _ghost_pad_2d(hx, 0, metallic_edges)
-        d_hy_dx = (phy[:, 1:] - phy[:, :-1]) / res
-        d_hx_dy = (phx[1:, :] - phx[:-1, :]) / res
+        d_hy_dx = _metric_diff(phy, 1, res, _metric(metrics, "h_to_e_x"))
+        d_hx_dy = _metric_diff(phx, 0, res, _metric(metrics, "h_to_e_y"))
         if e_terms:
             c0, new_psi[0] = correct_cpml_term(d_hy_dx, psi_e[0], e_terms[0])
             c1, new_psi[1] = correct_cpml_term(d_hx_dy, psi_e[1], e_terms[1])
@@ -704,8 +731,8 @@ def update_e_2d(fields, psi_e, e_terms, resolution, e_coeffs, metallic_edges=(),
     res = dtype.type(resolution)
     py = _ghost_pad_2d(hz, 0, metallic_edges)
     px = _ghost_pad_2d(hz, 1, metallic_edges)
-    d_hz_dy = (py[1:, :] - py[:-1, :]) / res
-    d_hz_dx = (px[:, 1:] - px[:, :-1]) / res
+    d_hz_dy = _metric_diff(py, 0, res, _metric(metrics, "h_to_e_y"))
+    d_hz_dx = _metric_diff(px, 1, res, _metric(metrics, "h_to_e_x"))
     if e_terms:
         c0, new_psi[0] = correct_cpml_term(d_hz_dy, psi_e[0], e_terms[0])
         c1, new_psi[1] = correct_cpml_term(d_hz_dx, psi_e[1], e_terms[1])
@@ -954,6 +981,7 @@ class OracleProgram:
     sources: list = field(default_factory=list)
     monitors: list = field(default_factory=list)
     polarization: str = "tm"
+    metrics: dict | None = None  # DerivativeMetricPlan names -> inverse distances (None: isotropic)
 
     @property
     def ndim(self):
@@ -981,11 +1009,11 @@ def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
     if program.ndim == 3:
         sm = program.material.sigma_m if program.material is not None else (0.0, 0.0, 0.0)
         hx, hy, hz, state.psi_h = update_h_3d(fields, state.psi_h, program.h_terms, program.dt,
-                                              program.resolution, sm, program.h_coeffs_3d)
+                                              program.resolution, sm, program.h_coeffs_3d, program.metrics)
         fields["Hx"], fields["Hy"], fields["Hz"] = hx, hy, hz
     else:
         new, state.psi_h = update_h_2d(fields, state.psi_h, program.h_terms, program.resolution,
-                                       program.h_coeffs, program.polarization)
+                                       program.h_coeffs, program.polarization, program.metrics)
         fields.update(new)
     # 2. H sources and H masks.
     apply_sources(fields, program.sources, "h", step)
@@ -995,11 +1023,13 @@ def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
     if program.ndim == 3:
         ex, ey, ez, state.psi_e = update_e_3d(fields, state.psi_e, program.e_terms, program.dt,
                                               program.resolution, program.material, program.metallic_edges,
-                                              program.e_coeffs if program.h_coeffs_3d is not None else None)
+                                              program.e_coeffs if program.h_coeffs_3d is not None else None,
+                                              program.metrics)
         fields["Ex"], fields["Ey"], fields["Ez"] = ex, ey, ez
     else:
         new, state.psi_e = update_e_2d(fields, state.psi_e, program.e_terms, program.resolution,
-                                       program.e_coeffs, program.metallic_edges, program.polarization)
+                                       program.e_coeffs, program.metallic_edges, program.polarization,
+                                       program.metrics)
         fields.update(new)
     apply_sources(fields, program.sources, "e", step)
     for c in ("Ex", "Ey", "Ez"):

@@ -32,7 +32,8 @@ def to_oracle(spec: P.ProgramSpec, dtype=np.float32) -> O.OracleProgram:
         woff += len(m.freqs)
     prog = O.OracleProgram(tuple(spec.grid_shape), float(spec.dt), float(spec.resolution), terms(spec.h_terms),
                            terms(spec.e_terms), metallic_edges=frozenset(spec.metallic_edges), sources=sources,
-                           monitors=monitors, polarization=spec.polarization)
+                           monitors=monitors, polarization=spec.polarization,
+                           metrics=spec.metrics.as_dict() if spec.metrics is not None else None)
     if spec.ndim == 3:
         eps = np.asarray(spec.eps_table, np.float32)[spec.voxel_ids]
         prog.material = O.material_from_voxels(eps, dtype=dtype)
@@ -170,3 +171,20 @@ def pack_dft_monitors_host(monitors, shapes, strides):
             indices[m, c, : ic.shape[1], :p] = ic.T
             weights[m, c, : wc.shape[1], :p] = wc.T
     return indices, weights
+
+
+def with_metrics(spec: P.ProgramSpec, kind="rectilinear", seed=0, spread=(1.0, 1.6)) -> P.ProgramSpec:
+    """``spec`` on an axis-uniform or rectilinear grid: seeded cell widths in
+    ``spread`` x the cell size on every axis (never below it, so the spec's
+    time step stays stable)."""
+    import dataclasses
+
+    rng = np.random.default_rng(seed)
+    axes = ("z", "y", "x") if spec.ndim == 3 else ("y", "x")
+    widths = {}
+    for a, n in zip(axes, spec.grid_shape):
+        if kind == "axis_uniform":
+            widths[a] = np.full(int(n), spec.resolution * rng.uniform(*spread))
+        else:
+            widths[a] = spec.resolution * rng.uniform(*spread, int(n))
+    return dataclasses.replace(spec, metrics=P.derivative_metrics(widths, kind))
