@@ -52,14 +52,24 @@ __device__ __forceinline__ int64_t lin(const Dims& d, int k, int j, int i) {
   return (static_cast<int64_t>(k) * d.y + j) * static_cast<int64_t>(d.x) + i;
 }
 
-// Correctly rounded a / b given r = RN(1 / b): one residual FMA and one
-// corrective FMA (Markstein, "IA-64 and Elementary Functions", 2000, thm 8.10).
-// Exact-rounding holds for normal quotients; finite-difference quotients of
-// field values are far from the subnormal range.
-__device__ __forceinline__ float div_rn(float a, float b, float r) {
-  const float q = a * r;
-  const float e = fmaf(-q, b, a);
-  return fmaf(e, r, q);
+// Power-of-two scale of div_rn's residual (exact in both directions).
+constexpr float kDivScale = 0x1p50f;
+constexpr float kDivUnscale = 0x1p-50f;
+
+// Correctly rounded a / b from bs = b 2^50 and rs = RN(1 / b) 2^-50: one
+// residual FMA and one corrective FMA (Markstein, "IA-64 and Elementary
+// Functions", 2000, thm 8.10), evaluated on a 2^50 a.  The theorem needs the
+// residual a - q b exactly representable, which fails once it falls into the
+// subnormal range (|a| below about 2^-103: the leading edge of a wavefront
+// grown from zero fields); scaled by 2^50 it never does for |a| >= 2^-149.
+// q = (2^50 a) rs is the same product as a RN(1/b), so for every other a the
+// result equals the unscaled form.  Valid while a RN(1/b) is normal and
+// |a| < 2^78 (fields in SI units on cells below 0.1 mm).
+__device__ __forceinline__ float div_rn(float a, float bs, float rs) {
+  const float as = a * kDivScale;
+  const float q = as * rs;
+  const float e = fmaf(-q, bs, as);
+  return fmaf(e, rs, q);
 }
 
 // One packed CPML recurrence term as seen by a kernel.

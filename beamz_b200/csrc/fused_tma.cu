@@ -260,10 +260,11 @@ __device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
   return f2unpack(r);
 }
 
-// div_rn on a pair: q = a r, e = fma(q, -b, a), q + e r (fdtd_common.cuh).
+// div_rn on a pair (fdtd_common.cuh): r2 = (rs, rs), nb2 = (-bs, -bs).
 __device__ __forceinline__ float2 f2div(float2 a, float2 r2, float2 nb2) {
-  const float2 q = f2mul(a, r2);
-  const float2 e = f2fma(q, nb2, a);
+  const float2 as = f2mul(a, make_float2(kDivScale, kDivScale));
+  const float2 q = f2mul(as, r2);
+  const float2 e = f2fma(q, nb2, as);
   return f2fma(e, r2, q);
 }
 
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 && R == 1 ? 5 : 1024 / (32 * 
   const int k0 = blockIdx.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, Z + 1);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
-  const float res = p.res, inv_res = p.inv_res;
+  const float res = p.div_bs, inv_res = p.div_rs;  // div_rn's scaled cell size and reciprocal
   const int P = p.pitch, PL = (Y + 1) * p.pitch;
 
   if (tid == 0) {

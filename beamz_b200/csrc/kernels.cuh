@@ -30,14 +30,14 @@ __device__ __forceinline__ int axis_cells(const Step3D& p, int axis) { return ax
 // stored are clamped into the metric.
 __device__ __forceinline__ float dh(const Step3D& p, int axis, int c, float diff) {
   const float* m = p.metric_h[axis];
-  if (m == nullptr) return div_rn(diff, p.res, p.inv_res);
+  if (m == nullptr) return div_rn(diff, p.div_bs, p.div_rs);
   return diff * m[clampi(c, axis_cells(p, axis) - 1)];
 }
 
 // A backward difference of H along `axis` at E coordinate `c` (0..n_axis).
 __device__ __forceinline__ float de(const Step3D& p, int axis, int c, float diff) {
   const float* m = p.metric_e[axis];
-  if (m == nullptr) return div_rn(diff, p.res, p.inv_res);
+  if (m == nullptr) return div_rn(diff, p.div_bs, p.div_rs);
   return diff * m[clampi(c, axis_cells(p, axis))];
 }
 

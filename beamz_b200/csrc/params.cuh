@@ -37,6 +37,7 @@ struct Step3D {
   float* eout[3];
   float* hout[3];
   float res, inv_res;
+  float div_bs, div_rs;  // res 2^50 and inv_res 2^-50: div_rn's operands
   float dt_over_eps;
   int metallic;
   int cpml;

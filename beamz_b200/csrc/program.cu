@@ -267,6 +267,8 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   }
   s.res = p.resolution;
   s.inv_res = p.inv_resolution;
+  s.div_bs = p.resolution * kDivScale;
+  s.div_rs = p.inv_resolution * kDivUnscale;
   s.dt_over_eps = p.dt_over_eps;
   s.metallic = p.metallic_edges;
   if (p.ndim == 2) s.metallic &= ~(FDTD_EDGE_FRONT | FDTD_EDGE_BACK);

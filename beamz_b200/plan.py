@@ -381,6 +381,56 @@ def h_site_sample_3d(grid: np.ndarray, component: str) -> np.ndarray:
     return np.ascontiguousarray(g[np.ix_(*idx)])
 
 
+def sponge_conductivity(grid_shape, resolution, base_sigma=0.0, edges=None, thickness=None, sigma_max=None,
+                        order: int = 3, reflection: float = 1e-6) -> np.ndarray:
+    """Cell-centred float32 conductivity of a graded sponge absorber on a
+    uniform grid, combined with the material's own: beamz's ``Absorber`` /
+    ``PML(formulation="sponge")`` lowering (beamz/devices/_boundary_compile.py:
+    206-262, 406-423, 616-650) and ``_total_conductivity`` (lattice.py:978-998).
+
+    Per axis (3D z, y, x; 2D y, x) the cell coordinates are ``linspace(0, L,
+    n)`` (L = n * resolution, float64 rounded to float32) and the profile
+    sigma_max * (d / thickness)**order grows with the depth d into each chosen
+    face; the three axis profiles are summed (x, y, z order) and the larger of
+    that sum and ``base_sigma`` is kept per cell.  ``thickness`` defaults to 12
+    cells (beamz's ``PML``; its ``Absorber`` takes metres), and ``sigma_max`` to
+    -(order + 1) ln(reflection) / (2 eta max(thickness, resolution)).  The
+    result feeds :func:`lossy_site_coefficients_3d` / ``_2d``."""
+    f32 = np.float32
+    shape = tuple(int(n) for n in grid_shape)
+    ndim = len(shape)
+    res = float(resolution)
+    edges = set(ALL_EDGES_3D if ndim == 3 else ALL_EDGES_2D) if edges is None else set(edges)
+    thk = 12 * res if thickness is None else float(thickness)
+    if sigma_max is None:
+        eta = np.sqrt(MU_0 / (EPS_0 * 1.0))
+        sigma_max = -(order + 1) * np.log(max(reflection, 1e-16)) / (2.0 * eta * max(thk, res))
+    walls = dict(zip(("z", "y", "x"), _WALLS_3D)) if ndim == 3 else dict(zip(("y", "x"), _WALLS_2D))
+    names = ("z", "y", "x") if ndim == 3 else ("y", "x")
+    profiles = {}
+    for axis, name in enumerate(names):
+        n = shape[axis]
+        length = n * res
+        coords = np.linspace(0.0, length, n).astype(f32)
+        sigma = np.zeros(n, f32)
+        low, high = walls[name]
+        if low in edges:
+            dist = np.clip(f32(thk) - coords, f32(0.0), None)
+            sigma = sigma + f32(sigma_max) * (dist / f32(thk)) ** order
+        if high in edges:
+            dist = np.clip(coords - f32(length - thk), f32(0.0), None)
+            sigma = sigma + f32(sigma_max) * (dist / f32(thk)) ** order
+        bshape = [1] * ndim
+        bshape[axis] = n
+        profiles[name] = np.broadcast_to(sigma.reshape(bshape), shape)
+    total = np.zeros(shape, f32) + np.asarray(base_sigma, f32)
+    pml = np.zeros_like(np.asarray(base_sigma, f32))
+    for name in ("x", "y", "z"):
+        if name in profiles:
+            pml = pml + profiles[name]
+    return np.maximum(total, pml).astype(f32)
+
+
 def lossy_site_coefficients_3d(eps_grid: np.ndarray, sigma_grid: np.ndarray, dt: float):
     """Per-site update coefficients of a conductive, non-magnetic 3D material,
     as beamz's CUDA path receives them (beamz/simulation/compile.py:563-640):

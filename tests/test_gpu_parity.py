@@ -279,6 +279,34 @@ def test_fields_are_bit_identical_to_the_fp32_oracle(case, schedule):
         assert O.relative_l2(mine, ref) <= DFT_TOL
 
 
+WAVEFRONT_CASES = {
+    "3d_pitched": (lambda: scenario_3d(grid=(12, 16, 40), seed=8, nsteps=40, metallic=("top",)), "fused"),
+    "3d_dense": (lambda: scenario_3d(grid=(12, 16, 40), seed=8, nsteps=40, metallic=("top",)), "phases"),
+    "2d_tm": (lambda: scenario_2d(grid=(31, 37), polarization="tm", nsteps=40), "fused"),
+    "2d_te": (lambda: scenario_2d(grid=(31, 37), polarization="te", nsteps=40), "phases"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(WAVEFRONT_CASES))
+def test_wavefronts_from_zero_fields_are_bit_identical(case):
+    """Fields grown from zero by the sources: ahead of each wavefront the
+    values fall through the subnormal range, where the division of a tiny
+    difference by the cell size must still round as the oracle's does."""
+    build, schedule = WAVEFRONT_CASES[case]
+    spec = build()
+    prog = R.compile_program(spec, schedule=schedule)
+    assert (prog.layout == "pitched") == (case == "3d_pitched")
+    out = R.run_steps(R.initial_state(prog), prog, 40).numpy()
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog), oprog, 40)
+    tiny = 0
+    for c in P.active_components(spec.ndim, spec.polarization):
+        np.testing.assert_array_equal(out[c], st.fields[c], err_msg=c)
+        v = np.abs(st.fields[c])
+        tiny += int(np.count_nonzero((v > 0) & (v < 2.0**-100)))
+    assert tiny > 0  # the case reaches the tiny range
+
+
 @pytest.mark.parametrize("graphs", [True, False])
 def test_dft_sampling_beside_the_next_step_is_bit_identical(graphs):
     """Samples taken on a side stream while the next step runs give the same

@@ -37,10 +37,12 @@ def test_lossy_coefficients_match_the_reference():
     np.testing.assert_array_equal(e64["Ex"][0], GOLD["decay_Ex"])
 
 
-def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12):
+def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12, sigma_of=None):
     """A conductive 3D scene (boxes of eps and of sigma, CPML on every face,
     a pre-E dipole, an H source and a DFT plane) as a ProgramSpec, and the
-    oracle program with both lossy forms available."""
+    oracle program with both lossy forms available.  ``sigma_of(sigma)``
+    replaces the conductivity grid (e.g. adds a sponge); ``pml_cells`` 0
+    leaves out the CPML."""
     rng = np.random.default_rng(seed)
     res = 20e-9
     dt = float(0.99 * res / (P.LIGHT_SPEED * 3.0**0.5))
@@ -52,8 +54,10 @@ def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12):
         box = tuple(slice(a, b) for a, b in zip(lo, hi))
         eps[box] = rng.choice([12.11, 4.0])
         sigma[box] = rng.choice([5e3, 4e4])
+    if sigma_of is not None:
+        sigma = sigma_of(sigma)
     e_site, h_site, e_eps = P.lossy_site_coefficients_3d(eps, sigma, dt)
-    h_terms, e_terms = P.plan_cpml(grid, dt, res, pml_cells=pml_cells)
+    h_terms, e_terms = P.plan_cpml(grid, dt, res, pml_cells=pml_cells) if pml_cells else ([], [])
     f0 = P.LIGHT_SPEED / 1.55e-6
     wave = P.gaussian_pulse((np.arange(nsteps) + 0.5) * dt, f0, 0.5 * f0, offset=0.3)
     c = tuple(n // 2 for n in grid)
