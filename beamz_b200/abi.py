@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 8
+FDTD_ABI_VERSION = 9
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_dft_change",
     "fdtd_pack_gather",
     "fdtd_voxel_histogram",
+    "fdtd_monitor_reduce",
     "fdtd_adjoint_step_noalloc",
     "fdtd_graph_create",
     "fdtd_graph_launch",
@@ -160,6 +161,24 @@ class FdtdGatherPack(ctypes.Structure):
         ("dims", ctypes.c_int32 * 3),
         ("row", ctypes.c_int64),
         ("plane", ctypes.c_int64),
+    ]
+
+
+class FdtdMonitorReduce(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("freq_count", ctypes.c_int32),
+        ("value_offset", ctypes.c_int64),
+        ("point_count", ctypes.c_int64),
+        ("e", ctypes.c_int32 * 2),
+        ("h", ctypes.c_int32 * 2),
+        ("rows", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("scale", FdtdBuffer),
+        ("weights", FdtdBuffer),
+        ("profile_re", FdtdBuffer),
+        ("profile_im", FdtdBuffer),
+        ("out", FdtdBuffer),
     ]
 
 
@@ -294,6 +313,9 @@ def load_library(path: str | None = None):
         lib.fdtd_pack_gather.restype = ctypes.c_int
         lib.fdtd_voxel_histogram.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdBuffer), ctypes.POINTER(FdtdBuffer)]
         lib.fdtd_voxel_histogram.restype = ctypes.c_int
+        lib.fdtd_monitor_reduce.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram),
+                                            ctypes.POINTER(FdtdMonitorReduce)]
+        lib.fdtd_monitor_reduce.restype = ctypes.c_int
         lib.fdtd_graph_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.POINTER(ctypes.c_void_p)]
         lib.fdtd_graph_create.restype = ctypes.c_int
         lib.fdtd_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]

@@ -164,6 +164,21 @@ struct DftDev {
   float dt;
 };
 
+// Monitor-plane reduction (analysis.cu); see FdtdMonitorReduce.
+struct MonitorReduceDev {
+  const float* re = nullptr;
+  const float* im = nullptr;
+  int64_t value_offset = 0, points = 0;
+  int freqs = 0, rows = 0;
+  int e[2] = {0, 0}, h[2] = {0, 0};
+  const double* scale = nullptr;    // [F, 3]
+  const double* weights = nullptr;  // [2, P]
+  const double* prof_re = nullptr;  // [rows, F, 4, P]
+  const double* prof_im = nullptr;
+  double* out = nullptr;            // [max(rows, 1), F, 2, 2]
+};
+cudaError_t launch_monitor_reduce(cudaStream_t s, const MonitorReduceDev& r);
+
 // Gather-plan packing (planner.cu): one (monitor, component) plan.
 struct GatherPackDev {
   const int* idx_in = nullptr;    // [points, slots_in]

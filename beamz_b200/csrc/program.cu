@@ -938,6 +938,44 @@ int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChang
                                                   static_cast<double*>(c->out.data)));
 }
 
+int fdtd_monitor_reduce(void* stream, const FdtdProgram* program, const FdtdMonitorReduce* r) {
+  if (program == nullptr || r == nullptr) return fdtd::kInvalid;
+  const FdtdProgram& p = *program;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  if (r->abi_version != FDTD_ABI_VERSION || p.dft.monitor_count <= 0) return fdtd::kInvalid;
+  const int64_t arena = fdtd::elements(p.dft.re);
+  const int64_t F = r->freq_count, P = r->point_count;
+  if (F < 1 || P < 0 || r->value_offset < 0 || r->rows < 0 || r->value_offset + 6 * F * P > arena)
+    return fdtd::kInvalid;
+  for (int q = 0; q < 2; ++q)
+    if (r->e[q] < 0 || r->e[q] > 2 || r->h[q] < 3 || r->h[q] > 5) return fdtd::kInvalid;
+  auto f64 = [](const FdtdBuffer& b, int64_t n) {
+    return b.element_type == FDTD_F64 && fdtd::elements(b) == n && (n == 0 || b.data != nullptr);
+  };
+  const int64_t rows = r->rows > 0 ? r->rows : 1;
+  if (!f64(r->scale, F * 3) || !f64(r->weights, 2 * P) || !f64(r->out, rows * F * 4)) return fdtd::kInvalid;
+  if (r->rows > 0 && (!f64(r->profile_re, rows * F * 4 * P) || !f64(r->profile_im, rows * F * 4 * P)))
+    return fdtd::kInvalid;
+  fdtd::MonitorReduceDev d;
+  d.re = static_cast<const float*>(p.dft.re.data);
+  d.im = static_cast<const float*>(p.dft.im.data);
+  d.value_offset = r->value_offset;
+  d.points = P;
+  d.freqs = static_cast<int>(F);
+  d.rows = r->rows;
+  for (int q = 0; q < 2; ++q) {
+    d.e[q] = r->e[q];
+    d.h[q] = r->h[q];
+  }
+  d.scale = static_cast<const double*>(r->scale.data);
+  d.weights = static_cast<const double*>(r->weights.data);
+  d.prof_re = static_cast<const double*>(r->profile_re.data);
+  d.prof_im = static_cast<const double*>(r->profile_im.data);
+  d.out = static_cast<double*>(r->out.data);
+  return static_cast<int>(fdtd::launch_monitor_reduce(static_cast<cudaStream_t>(stream), d));
+}
+
 int fdtd_pack_gather(void* stream, const FdtdGatherPack* g) {
   if (g == nullptr) return fdtd::kInvalid;
   const FdtdBuffer &ii = g->indices_in, &wi = g->weights_in, &io = g->indices_out, &wo = g->weights_out;

@@ -700,3 +700,101 @@ def dft_change(state: DeviceState, program: DeviceProgram, monitors=None):
         den = max(float(np.sqrt(r[k][1])), float(np.sqrt(r[k][2])))
         changes.append(0.0 if den <= tiny and num <= tiny else num / den)
     return max(changes, default=0.0), finite
+
+
+def monitor_values(state: DeviceState, program: DeviceProgram, monitor: int) -> dict:
+    """Host copy of one monitor's stored DFT values: component -> complex128
+    [F, P] (the arena slice beamz records as ``dft_fields``)."""
+    voff, nf, npts, _woff = program.arena.layout[monitor]
+    n = 6 * nf * npts
+    re = state.dft_re[voff:voff + n].cpu().numpy().astype(np.float64).reshape(6, nf, npts)
+    im = state.dft_im[voff:voff + n].cpu().numpy().astype(np.float64).reshape(6, nf, npts)
+    return {c: re[i] + 1j * im[i] for i, c in enumerate(COMPONENTS)}
+
+
+def _tangential_pairs(axis: str):
+    """(E1, E2, H1, H2) tangential to a plane normal (beamz/devices/modes/
+    fields.py:15-19) as component indices: pair 0 = (E1, H1), pair 1 = (E2, H2)."""
+    names = {"x": ("Ey", "Ez", "Hz", "Hy"), "y": ("Ez", "Ex", "Hx", "Hz"), "z": ("Ex", "Ey", "Hy", "Hx")}[axis]
+    return names, [COMPONENT_INDEX[names[0]], COMPONENT_INDEX[names[1]]], \
+        [COMPONENT_INDEX[names[2]], COMPONENT_INDEX[names[3]]]
+
+
+def _flux_scales(state: DeviceState, program: DeviceProgram, monitor: int, base_dt):
+    """Per frequency (alpha, phase re, phase im): stored values times alpha =
+    2 / max(window weight sum, 1e-18) (beamz/simulation/observe.py:166-179),
+    H values also times exp(-i pi f dt) with a base time step (observe.py:182-187)."""
+    _voff, nf, _npts, woff = program.arena.layout[monitor]
+    wsum = state.dft_w[woff:woff + nf].cpu().numpy().astype(np.float64)
+    alpha = 2.0 / np.maximum(wsum, 1e-18)
+    freqs = np.asarray(program.spec.monitors[monitor].freqs, dtype=float)[:nf]
+    phase = np.exp(-1j * np.pi * freqs * base_dt) if base_dt else np.ones(nf, np.complex128)
+    return np.stack([alpha, phase.real, phase.imag], axis=1)
+
+
+def _monitor_reduce(state, program, monitor, e, h, scale, weights, profiles=None):
+    torch = _torch()
+    voff, nf, npts, _woff = program.arena.layout[monitor]
+    rows = 0 if profiles is None else int(profiles.shape[0])
+    dev = program.device
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)  # noqa: E731
+    keep = [f64(scale), f64(weights)]
+    out = torch.empty((max(rows, 1), nf, 2, 2), dtype=torch.float64, device=dev)
+    r = abi.FdtdMonitorReduce()
+    r.abi_version = abi.FDTD_ABI_VERSION
+    r.freq_count, r.value_offset, r.point_count = nf, voff, npts
+    r.e[:], r.h[:] = e, h
+    r.rows = rows
+    r.scale, r.weights, r.out = abi.buffer_of(keep[0]), abi.buffer_of(keep[1]), abi.buffer_of(out)
+    if rows:
+        keep += [f64(profiles.real), f64(profiles.imag)]
+        r.profile_re, r.profile_im = abi.buffer_of(keep[2]), abi.buffer_of(keep[3])
+    s = program.fill(state, 0)
+    abi.check(program.lib.fdtd_monitor_reduce(_stream(program), ctypes.byref(s), ctypes.byref(r)),
+              "fdtd_monitor_reduce")
+    o = out.cpu().numpy()
+    return o[..., 0] + 1j * o[..., 1]  # [rows or 1, F, pair]
+
+
+def monitor_dft_flux(state: DeviceState, program: DeviceProgram, monitor: int, axis: str, sign: float = 1.0,
+                     integration_weights=None, measure=None, base_dt=None) -> np.ndarray:
+    """Power through a plane monitor per frequency, on the device arena
+    (beamz/simulation/observe.py:198-234 monitor_dft_flux):
+    0.5 Re sum_p sign (E1 conj(H1) - E2 conj(H2)) w_p over the flux-normalised
+    fields, ``axis`` the plane normal ("x", "y", "z"), w the per-point
+    ``integration_weights`` (size P) or else a constant ``measure``."""
+    _voff, nf, npts, _woff = program.arena.layout[monitor]
+    _names, e, h = _tangential_pairs(axis)
+    iw = np.asarray(() if integration_weights is None else integration_weights, dtype=float).reshape(-1)
+    per_point = iw.size == npts
+    if not per_point and measure is None:
+        raise ValueError("monitor_dft_flux needs integration weights of one per point or a measure")
+    w = iw if per_point else np.ones(npts)
+    sums = _monitor_reduce(state, program, monitor, e, h, _flux_scales(state, program, monitor, base_dt),
+                           np.stack([w, w]))[0]
+    flux = 0.5 * np.real(sign * (sums[:, 0] - sums[:, 1]))
+    return flux if per_point else flux * float(measure)
+
+
+def modal_overlap(state: DeviceState, program: DeviceProgram, monitor: int, modes, axis: str, measure=1.0,
+                  direction_sign: float = 1.0, base_dt=None) -> np.ndarray:
+    """Overlap of a plane monitor's flux-normalised DFT fields with each mode,
+    per frequency, on the device arena (beamz/devices/modes/fields.py:76-129
+    _modal_overlap): 0.25 dir [sum w1 (E1 conj(Hm1) + conj(Em1) H1) -
+    sum w2 (E2 conj(Hm2) + conj(Em2) H2)].  ``modes`` is a list of mappings
+    component name -> complex profile [F, P] (or [P] for every frequency) of
+    the four tangential components; ``measure`` a scalar, a per-point array
+    or a mapping E name -> per-point weights.  Returns [len(modes), F]."""
+    _voff, nf, npts, _woff = program.arena.layout[monitor]
+    names, e, h = _tangential_pairs(axis)
+    weights = np.empty((2, npts))
+    for q in range(2):
+        m = measure[names[q]] if isinstance(measure, dict) else measure
+        weights[q] = np.broadcast_to(np.asarray(m, dtype=float).reshape(-1) if np.ndim(m) else float(m), (npts,))
+    prof = np.empty((len(modes), nf, 4, npts), np.complex128)
+    for r, mode in enumerate(modes):
+        for k, name in enumerate(names):
+            prof[r, :, k] = np.broadcast_to(np.asarray(mode[name], np.complex128).reshape(-1, npts), (nf, npts))
+    sums = _monitor_reduce(state, program, monitor, e, h, _flux_scales(state, program, monitor, base_dt),
+                           weights, prof)
+    return 0.25 * float(direction_sign) * (sums[:, :, 0] - sums[:, :, 1])

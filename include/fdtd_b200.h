@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 8
+#define FDTD_ABI_VERSION 9
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -396,6 +396,36 @@ int fdtd_pack_gather(void* stream, const FdtdGatherPack* g);
  * to zero first): the materials a program uses, for the codebook's compact
  * material indices (beamz compacts on the host, compile.py:146-187). */
 int fdtd_voxel_histogram(void* stream, const FdtdBuffer* voxels, const FdtdBuffer* counts);
+
+/* ---- Monitor-plane reductions --------------------------------------------
+ * The sums behind beamz's DFT flux through a monitor (observe.py:166-234
+ * monitor_dft_component, _flux_component, monitor_dft_flux) and its modal
+ * overlaps with mode profiles (devices/modes/fields.py:76-129 _modal_overlap),
+ * evaluated on the device arena instead of a host copy of it. */
+typedef struct FdtdMonitorReduce {
+  int32_t abi_version;     /* FDTD_ABI_VERSION */
+  int32_t freq_count;      /* F of the monitor */
+  int64_t value_offset;    /* the monitor's first element in program->dft.re/im */
+  int64_t point_count;     /* P of the monitor */
+  int32_t e[2];            /* E component (0..2) of each (E, H) pair */
+  int32_t h[2];            /* H component (3..5) of each pair */
+  int32_t rows;            /* mode profile rows; 0 = field products (flux) */
+  int32_t reserved;
+  FdtdBuffer scale;        /* F64 [F, 3]: alpha_f, phase_f (re, im) */
+  FdtdBuffer weights;      /* F64 [2, P]: point weights of pair 0 and pair 1 */
+  FdtdBuffer profile_re;   /* F64 [rows, F, 4, P]: each row's e0, e1, h0, h1 (rows > 0) */
+  FdtdBuffer profile_im;
+  FdtdBuffer out;          /* F64 [max(rows, 1), F, 2, 2]: per pair q the complex sum */
+} FdtdMonitorReduce;
+
+/* With E_q = alpha_f v(e[q]) and H_q = (alpha_f v(h[q])) phase_f, v(c) the
+ * arena value re + i im of component c at value_offset + (c F + f) P + p:
+ *   rows == 0:  out[0, f, q] = sum_p weights[q, p] E_q conj(H_q)
+ *   rows > 0:   out[r, f, q] = sum_p weights[q, p] (E_q conj(G_{2+q}) + conj(G_q) H_q)
+ * where G_k = profile_re + i profile_im [r, f, k, p].  Each term is formed in
+ * double with numpy's complex operand order; the sums run in a fixed order.
+ * No beamz counterpart (beamz copies the arena to the host and sums there). */
+int fdtd_monitor_reduce(void* stream, const FdtdProgram* program, const FdtdMonitorReduce* r);
 
 /* Drop every cached CUDA graph (beamz: cuda/src/graph.cu cache reset). */
 void fdtd_clear_graph_cache(void);

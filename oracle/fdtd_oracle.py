@@ -1138,3 +1138,68 @@ def relative_monitor_change(current: dict, previous: dict | None):
         den = max(float(np.linalg.norm(cur)), float(np.linalg.norm(prev)))
         changes.append(0.0 if den <= tiny and num <= tiny else num / den)
     return max(changes, default=0.0)
+
+
+# ---------------------------------------------------------------------------
+# Monitor analysis: DFT flux and modal overlaps (float64 / complex128)
+# ---------------------------------------------------------------------------
+
+# beamz/devices/modes/fields.py:15-19 -- (E1, E2, H1, H2) tangential to a plane
+# normal; E1 pairs with H1 (+), E2 with H2 (-).
+TANGENTIAL_COMPONENTS = {
+    "x": ("Ey", "Ez", "Hz", "Hy"),
+    "y": ("Ez", "Ex", "Hx", "Hz"),
+    "z": ("Ex", "Ey", "Hy", "Hx"),
+}
+
+
+def monitor_dft_component(values, weight_sum):
+    """beamz/simulation/observe.py:166-179: the stored DFT values of one
+    component, [F, P] complex, over half the accumulated window weight."""
+    values = np.asarray(values, np.complex128)
+    weights = np.maximum(np.asarray(weight_sum, dtype=float), 1e-18).reshape(-1, 1)
+    return (2.0 / weights) * values
+
+
+def flux_component(values, weight_sum, component: str, freqs, base_dt):
+    """beamz/simulation/observe.py:182-187: H values also carry the half-step
+    phase exp(-i pi f dt) when the monitor has a base time step."""
+    v = monitor_dft_component(values, weight_sum)
+    if component.startswith("H") and base_dt:
+        phase = np.exp(-1j * np.pi * np.asarray(freqs, dtype=float) * base_dt)
+        v = v * phase[:, None]
+    return v
+
+
+def monitor_dft_flux(fields: dict, axis: str, sign: float = 1.0, integration_weights=None, measure=None):
+    """beamz/simulation/observe.py:198-234 on flux-normalised fields
+    (component -> [F, P]): 0.5 Re sum sign (E1 conj(H1) - E2 conj(H2)) w, with
+    per-point integration weights when given (size P), else times ``measure``."""
+    e1, e2, h1, h2 = TANGENTIAL_COMPONENTS[axis]
+    component = fields[e1] * np.conjugate(fields[h1]) - fields[e2] * np.conjugate(fields[h2])
+    iw = np.asarray(() if integration_weights is None else integration_weights, dtype=float).reshape(-1)
+    if iw.size == component.shape[1]:
+        return 0.5 * np.real(np.sum(sign * component * iw[None, :], axis=1))
+    return 0.5 * np.real(np.sum(sign * component, axis=1)) * float(measure)
+
+
+def modal_overlap(fields: dict, mode: dict, axis: str, measure, direction_sign: float = 1.0):
+    """beamz/devices/modes/fields.py:76-129 for equal-size profiles:
+    0.25 dir [sum w1 (E1 conj(Hm1) + conj(Em1) H1) - sum w2 (E2 conj(Hm2) + conj(Em2) H2)],
+    ``measure`` a scalar, a per-point array or a mapping E name -> weights."""
+    names = TANGENTIAL_COMPONENTS[axis]
+
+    def paired(e_name, h_name, sign):
+        ef = np.asarray(fields[e_name], np.complex128).reshape(-1)
+        hf = np.asarray(fields[h_name], np.complex128).reshape(-1)
+        em = np.asarray(mode[e_name], np.complex128).reshape(-1)
+        hm = np.asarray(mode[h_name], np.complex128).reshape(-1)
+        if isinstance(measure, dict):
+            w = np.asarray(measure[e_name], dtype=float).reshape(-1)
+        else:
+            raw = np.asarray(measure, dtype=float)
+            w = raw if raw.ndim == 0 else raw.reshape(-1)
+        return np.complex128(np.sum(w * sign * (ef * np.conjugate(hm) + np.conjugate(em) * hf)))
+
+    overlap = paired(names[0], names[2], 1.0) + paired(names[1], names[3], -1.0)
+    return np.complex128(0.25 * float(direction_sign) * overlap)
