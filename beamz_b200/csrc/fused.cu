@@ -152,12 +152,13 @@ __device__ __forceinline__ float add_h_sources(const Step3D& p, const float* amp
 // Backward difference at `coord` of an axis with n samples, with beamz's ghost
 // planes (beamz/lattice.py:523-551): zero beyond a metallic wall, otherwise a
 // copy of the edge sample, so the edge derivative vanishes.
+template <bool Metric>
 __device__ __forceinline__ float ghost_diff(const Step3D& p, int axis, float center, float below, int coord, int n,
                                             bool low_wall, bool high_wall) {
   if (n == 0) return 0.0f;
-  if (coord == 0) return low_wall ? de(p, axis, coord, center - 0.0f) : 0.0f;
-  if (coord == n) return high_wall ? de(p, axis, coord, 0.0f - below) : 0.0f;
-  return de(p, axis, coord, center - below);
+  if (coord == 0) return low_wall ? de<Metric>(p, axis, coord, center - 0.0f) : 0.0f;
+  if (coord == n) return high_wall ? de<Metric>(p, axis, coord, 0.0f - below) : 0.0f;
+  return de<Metric>(p, axis, coord, center - below);
 }
 
 // Staged E value; components outside the active set read as zero (2D).
@@ -166,7 +167,7 @@ __device__ __forceinline__ float ev(const S& sm, int slot, int c, int ly, int lx
   return ((Active >> c) & 1) ? sm.e[slot][c][ly][lx] : 0.0f;
 }
 
-template <int TX, int TY, int Active, bool Cpml, int Mat>
+template <int TX, int TY, int Active, bool Cpml, int Mat, bool Metric>
 __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
   using S = FusedSmem<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -230,8 +231,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
       const bool own = ly > 0 && lx > 0 && emit;
       float hx = 0.0f, hy = 0.0f, hz = 0.0f;
       if (((Active >> 3) & 1) && k < dHx.z && j >= 0 && j < dHx.y && i >= 0 && i < dHx.x) {
-        float d0 = dh(p, 1, j, ev<Active>(sm, e0, 2, ly + 1, lx) - ev<Active>(sm, e0, 2, ly, lx));
-        float d1 = dh(p, 0, k, ev<Active>(sm, e1, 1, ly, lx) - ev<Active>(sm, e0, 1, ly, lx));
+        float d0 = dh<Metric>(p, 1, j, ev<Active>(sm, e0, 2, ly + 1, lx) - ev<Active>(sm, e0, 2, ly, lx));
+        float d1 = dh<Metric>(p, 0, k, ev<Active>(sm, e1, 1, ly, lx) - ev<Active>(sm, e0, 1, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<1>(p.ht[0], d0, k, j, i, own);
           d1 = cpml_correct<0>(p.ht[1], d1, k, j, i, own);
@@ -243,8 +244,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         if (own) p.hout[0][o] = hx;
       }
       if (((Active >> 4) & 1) && k < dHy.z && j >= 0 && j < dHy.y && i >= 0 && i < dHy.x) {
-        float d0 = dh(p, 0, k, ev<Active>(sm, e1, 0, ly, lx) - ev<Active>(sm, e0, 0, ly, lx));
-        float d1 = dh(p, 2, i, ev<Active>(sm, e0, 2, ly, lx + 1) - ev<Active>(sm, e0, 2, ly, lx));
+        float d0 = dh<Metric>(p, 0, k, ev<Active>(sm, e1, 0, ly, lx) - ev<Active>(sm, e0, 0, ly, lx));
+        float d1 = dh<Metric>(p, 2, i, ev<Active>(sm, e0, 2, ly, lx + 1) - ev<Active>(sm, e0, 2, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<0>(p.ht[2], d0, k, j, i, own);
           d1 = cpml_correct<2>(p.ht[3], d1, k, j, i, own);
@@ -256,8 +257,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         if (own) p.hout[1][o] = hy;
       }
       if (((Active >> 5) & 1) && k < dHz.z && j >= 0 && j < dHz.y && i >= 0 && i < dHz.x) {
-        float d0 = dh(p, 2, i, ev<Active>(sm, e0, 1, ly, lx + 1) - ev<Active>(sm, e0, 1, ly, lx));
-        float d1 = dh(p, 1, j, ev<Active>(sm, e0, 0, ly + 1, lx) - ev<Active>(sm, e0, 0, ly, lx));
+        float d0 = dh<Metric>(p, 2, i, ev<Active>(sm, e0, 1, ly, lx + 1) - ev<Active>(sm, e0, 1, ly, lx));
+        float d1 = dh<Metric>(p, 1, j, ev<Active>(sm, e0, 0, ly + 1, lx) - ev<Active>(sm, e0, 0, ly, lx));
         if (Cpml) {
           d0 = cpml_correct<2>(p.ht[4], d0, k, j, i, own);
           d1 = cpml_correct<1>(p.ht[5], d1, k, j, i, own);
@@ -280,8 +281,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
       const int pb = hb ^ 1;  // H(k-1), never read at k == 0 (ghost branch)
       const int v0 = (k + 2) % 3, v1 = k % 3;  // voxel planes clip(k-1), clip(k)
       if (((Active >> 0) & 1) && k < dEx.z && j < dEx.y && i < dEx.x) {
-        float d0 = ghost_diff(p, 1, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly - 1][lx], j, dHz.y, wy0, wy1);
-        float d1 = ghost_diff(p, 0, sm.hn[hb][1][ly][lx], sm.hn[pb][1][ly][lx], k, dHy.z, wz0, wz1);
+        float d0 = ghost_diff<Metric>(p, 1, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly - 1][lx], j, dHz.y, wy0, wy1);
+        float d1 = ghost_diff<Metric>(p, 0, sm.hn[hb][1][ly][lx], sm.hn[pb][1][ly][lx], k, dHy.z, wz0, wz1);
         if (Cpml) {
           d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
           d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -299,8 +300,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         p.eout[0][o] = e;
       }
       if (((Active >> 1) & 1) && k < dEy.z && j < dEy.y && i < dEy.x) {
-        float d0 = ghost_diff(p, 0, sm.hn[hb][0][ly][lx], sm.hn[pb][0][ly][lx], k, dHx.z, wz0, wz1);
-        float d1 = ghost_diff(p, 2, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly][lx - 1], i, dHz.x, wx0, wx1);
+        float d0 = ghost_diff<Metric>(p, 0, sm.hn[hb][0][ly][lx], sm.hn[pb][0][ly][lx], k, dHx.z, wz0, wz1);
+        float d1 = ghost_diff<Metric>(p, 2, sm.hn[hb][2][ly][lx], sm.hn[hb][2][ly][lx - 1], i, dHz.x, wx0, wx1);
         if (Cpml) {
           d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
           d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -318,8 +319,8 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
         p.eout[1][o] = e;
       }
       if (((Active >> 2) & 1) && k < dEz.z && j < dEz.y && i < dEz.x) {
-        float d0 = ghost_diff(p, 2, sm.hn[hb][1][ly][lx], sm.hn[hb][1][ly][lx - 1], i, dHy.x, wx0, wx1);
-        float d1 = ghost_diff(p, 1, sm.hn[hb][0][ly][lx], sm.hn[hb][0][ly - 1][lx], j, dHx.y, wy0, wy1);
+        float d0 = ghost_diff<Metric>(p, 2, sm.hn[hb][1][ly][lx], sm.hn[hb][1][ly][lx - 1], i, dHy.x, wx0, wx1);
+        float d1 = ghost_diff<Metric>(p, 1, sm.hn[hb][0][ly][lx], sm.hn[hb][0][ly - 1][lx], j, dHx.y, wy0, wy1);
         if (Cpml) {
           d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
           d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);
@@ -343,11 +344,11 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
   cp_async_wait<0>();
 }
 
-template <int TX, int TY, int Active, bool Cpml, int Mat>
+template <int TX, int TY, int Active, bool Cpml, int Mat, bool Metric>
 cudaError_t launch_fused_t(cudaStream_t s, const Step3D& p) {
   using S = FusedSmem<TX, TY>;
   const size_t smem = sizeof(S);
-  auto kern = fused_step_kernel<TX, TY, Active, Cpml, Mat>;
+  auto kern = fused_step_kernel<TX, TY, Active, Cpml, Mat, Metric>;
   static bool configured = false;
   if (!configured) {
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -367,7 +368,8 @@ template <int Active, bool Cpml, int Mat>
 cudaError_t launch_fused_tile(cudaStream_t s, const Step3D& p, int tx, int ty) {
   (void)tx;
   (void)ty;
-  return launch_fused_t<32, 8, Active, Cpml, Mat>(s, p);
+  if (has_metric(p)) return launch_fused_t<32, 8, Active, Cpml, Mat, true>(s, p);
+  return launch_fused_t<32, 8, Active, Cpml, Mat, false>(s, p);
 }
 
 template <int Active>

@@ -155,13 +155,14 @@ __device__ __forceinline__ void store_vox(typename L::Smem& sm, const VoxRegs<R>
   }
 }
 
+template <bool Metric>
 __device__ __forceinline__ float ghost(const Step3D& p, int axis, int coord, float center, float below, bool at_low,
                                        bool at_high, bool low_wall, bool high_wall) {
   // beamz/lattice.py:523-551: zero beyond a metallic wall, else a copy of the
   // edge sample so that the edge derivative vanishes.
-  if (at_low) return low_wall ? de(p, axis, coord, center - 0.0f) : 0.0f;
-  if (at_high) return high_wall ? de(p, axis, coord, 0.0f - below) : 0.0f;
-  return de(p, axis, coord, center - below);
+  if (at_low) return low_wall ? de<Metric>(p, axis, coord, center - 0.0f) : 0.0f;
+  if (at_high) return high_wall ? de<Metric>(p, axis, coord, 0.0f - below) : 0.0f;
+  return de<Metric>(p, axis, coord, center - below);
 }
 
 __device__ __forceinline__ float h_sources(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
@@ -185,7 +186,7 @@ __device__ __forceinline__ bool sources_hit(const Step3D& p, int k, int jlo, int
   return false;
 }
 
-template <int NW, int R, int D, bool Cpml, int Mat>
+template <int NW, int R, int D, bool Cpml, int Mat, bool Metric>
 __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
   using L = Lean<NW, R, D>;
   using S = typename L::Smem;
@@ -259,8 +260,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       const float ez = sm.e[e0][2][ly][lx], ey = sm.e[e0][1][ly][lx], ex = sm.e[e0][0][ly][lx];
       if (which & 1) {  // Hx: dEz/dy - dEy/dz
         const bool ok = zZ && yY && iX1;
-        float d0 = dh(p, 1, j, sm.e[e0][2][ly + 1][lx] - ez);
-        float d1 = dh(p, 0, k, sm.e[e1][1][ly][lx] - ey);
+        float d0 = dh<Metric>(p, 1, j, sm.e[e0][2][ly + 1][lx] - ez);
+        float d1 = dh<Metric>(p, 0, k, sm.e[e1][1][ly][lx] - ey);
         if (cpml && ok) {
           d0 = cpml_correct<1>(p.ht[0], d0, k, j, ii, own);
           d1 = cpml_correct<0>(p.ht[1], d1, k, j, ii, own);
@@ -275,8 +276,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 2) {  // Hy: dEx/dz - dEz/dx
         const bool ok = zZ && yY1 && iX;
-        float d0 = dh(p, 0, k, sm.e[e1][0][ly][lx] - ex);
-        float d1 = dh(p, 2, ii, sm.e[e0][2][ly][lx + 1] - ez);
+        float d0 = dh<Metric>(p, 0, k, sm.e[e1][0][ly][lx] - ex);
+        float d1 = dh<Metric>(p, 2, ii, sm.e[e0][2][ly][lx + 1] - ez);
         if (cpml && ok) {
           d0 = cpml_correct<0>(p.ht[2], d0, k, j, ii, own);
           d1 = cpml_correct<2>(p.ht[3], d1, k, j, ii, own);
@@ -291,8 +292,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 4) {  // Hz: dEy/dx - dEx/dy
         const bool ok = yY && iX;
-        float d0 = dh(p, 2, ii, sm.e[e0][1][ly][lx + 1] - ey);
-        float d1 = dh(p, 1, j, sm.e[e0][0][ly + 1][lx] - ex);
+        float d0 = dh<Metric>(p, 2, ii, sm.e[e0][1][ly][lx + 1] - ey);
+        float d1 = dh<Metric>(p, 1, j, sm.e[e0][0][ly + 1][lx] - ex);
         if (cpml && ok) {
           d0 = cpml_correct<2>(p.ht[4], d0, k, j, ii, own);
           d1 = cpml_correct<1>(p.ht[5], d1, k, j, ii, own);
@@ -328,8 +329,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         const float hx = sm.hn[hb][0][ly][lx], hy = sm.hn[hb][1][ly][lx], hz = sm.hn[hb][2][ly][lx];
         // Ex: dHz/dy - dHy/dz
         if (yY1 && xX) {
-          float d0 = ghost(p, 1, j, hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1);
-          float d1 = ghost(p, 0, k, hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1);
+          float d0 = ghost<Metric>(p, 1, j, hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1);
+          float d1 = ghost<Metric>(p, 0, k, hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1);
           if (cpml) {
             d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
             d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -348,8 +349,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ey: dHx/dz - dHz/dx
         if (yY && xX1) {
-          float d0 = ghost(p, 0, k, hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1);
-          float d1 = ghost(p, 2, i, hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1);
+          float d0 = ghost<Metric>(p, 0, k, hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1);
+          float d1 = ghost<Metric>(p, 2, i, hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1);
           if (cpml) {
             d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
             d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -368,8 +369,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ez: dHy/dx - dHx/dy
         if (zZ && yY1 && xX1) {
-          float d0 = ghost(p, 2, i, hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1);
-          float d1 = ghost(p, 1, j, hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1);
+          float d0 = ghost<Metric>(p, 2, i, hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1);
+          float d1 = ghost<Metric>(p, 1, j, hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1);
           if (cpml) {
             d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
             d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);
@@ -393,11 +394,11 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
   wait_group<0>();
 }
 
-template <int NW, int R, int D, bool Cpml, int Mat>
+template <int NW, int R, int D, bool Cpml, int Mat, bool Metric = false>
 cudaError_t launch_lean_t(cudaStream_t s, const Step3D& p) {
   using L = Lean<NW, R, D>;
   const size_t smem = sizeof(typename L::Smem);
-  auto kern = lean_step_kernel<NW, R, D, Cpml, Mat>;
+  auto kern = lean_step_kernel<NW, R, D, Cpml, Mat, Metric>;
   static bool configured = false;
   if (!configured) {
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -415,6 +416,7 @@ cudaError_t launch_lean_t(cudaStream_t s, const Step3D& p) {
 
 template <bool Cpml, int Mat>
 cudaError_t launch_lean_shape(cudaStream_t s, const Step3D& p, int ty) {
+  if (has_metric(p)) return launch_lean_t<8, 1, 1, Cpml, Mat, true>(s, p);  // metric grids: 32 x 8 tiles
   switch (ty) {
     case 8: return launch_lean_t<8, 1, 1, Cpml, Mat>(s, p);
     case 32: return launch_lean_t<8, 4, 1, Cpml, Mat>(s, p);

@@ -23,22 +23,35 @@ __device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > h
 
 __device__ __forceinline__ int axis_cells(const Step3D& p, int axis) { return axis == 0 ? p.Z : (axis == 1 ? p.Y : p.X); }
 
+// Does the program carry derivative metrics (FdtdProgram.metric_h/_e)?
+__host__ __device__ inline bool has_metric(const Step3D& p) {
+  return p.metric_h[0] != nullptr || p.metric_h[1] != nullptr || p.metric_h[2] != nullptr;
+}
+
 // A forward difference of E along `axis` at H coordinate `c`, as a derivative:
-// times the inverse distance of a metric grid (beamz/simulation/kernels.py:
-// 164-176, 293-323; cuda/src/update.cu:172-203), else divided by the cell
-// size (kernels.py:477-488).  Coordinates of halo cells that are never
-// stored are clamped into the metric.
+// divided by the cell size (kernels.py:477-488), or with Metric times the
+// inverse distance of a metric grid (beamz/simulation/kernels.py:164-176,
+// 293-323; cuda/src/update.cu:172-203).  Kernels are instantiated per Metric
+// so the isotropic step carries no metric test.  Coordinates of halo cells
+// that are never stored are clamped into the metric; an axis without one (z
+// of a 2D program, whose z differences are of inactive components) divides.
+template <bool Metric>
 __device__ __forceinline__ float dh(const Step3D& p, int axis, int c, float diff) {
-  const float* m = p.metric_h[axis];
-  if (m == nullptr) return div_rn(diff, p.div_bs, p.div_rs);
-  return diff * m[clampi(c, axis_cells(p, axis) - 1)];
+  if constexpr (Metric) {
+    const float* m = p.metric_h[axis];
+    if (m != nullptr) return diff * m[clampi(c, axis_cells(p, axis) - 1)];
+  }
+  return div_rn(diff, p.div_bs, p.div_rs);
 }
 
 // A backward difference of H along `axis` at E coordinate `c` (0..n_axis).
+template <bool Metric>
 __device__ __forceinline__ float de(const Step3D& p, int axis, int c, float diff) {
-  const float* m = p.metric_e[axis];
-  if (m == nullptr) return div_rn(diff, p.div_bs, p.div_rs);
-  return diff * m[clampi(c, axis_cells(p, axis))];
+  if constexpr (Metric) {
+    const float* m = p.metric_e[axis];
+    if (m != nullptr) return diff * m[clampi(c, axis_cells(p, axis))];
+  }
+  return div_rn(diff, p.div_bs, p.div_rs);
 }
 
 __device__ __forceinline__ float vox_eps(const EMaterial& m, int Z, int Y, int X, int k, int j, int i) {

@@ -32,18 +32,18 @@ __device__ __forceinline__ float ld(const Step3D& p, const float* const* base, i
 // Forward difference of E component `c` along `axis` at (k, j, i), divided by
 // the cell size (beamz/simulation/kernels.py:477-488: jnp.diff(...) / resolution)
 // or scaled by the grid's metric (kernels.py:506-551).
-template <int Active>
+template <int Active, bool Metric>
 __device__ __forceinline__ float fdiff(const Step3D& p, int c, int axis, int k, int j, int i) {
   if (!active<Active>(c)) return 0.0f;
   const float lo = ld<Active>(p, p.ein, c, k, j, i);
   const float hi = ld<Active>(p, p.ein, c, k + (axis == 0), j + (axis == 1), i + (axis == 2));
-  return dh(p, axis, axis == 0 ? k : (axis == 1 ? j : i), hi - lo);
+  return dh<Metric>(p, axis, axis == 0 ? k : (axis == 1 ? j : i), hi - lo);
 }
 
 // Backward difference of H component `c` along `axis` with beamz's ghost
 // planes: zero beyond a metallic wall, else a copy of the edge plane
 // (beamz/lattice.py:523-551, beamz/simulation/kernels.py:574-586).
-template <int Active>
+template <int Active, bool Metric>
 __device__ __forceinline__ float bdiff(const Step3D& p, int c, int axis, int k, int j, int i) {
   if (!active<Active>(c)) return 0.0f;
   const Dims d = component_dims(c, p.Z, p.Y, p.X);
@@ -52,18 +52,18 @@ __device__ __forceinline__ float bdiff(const Step3D& p, int c, int axis, int k, 
   if (n == 0) return 0.0f;
   if (coord == 0) {
     if (!wall(p.metallic, axis, false)) return 0.0f;
-    return de(p, axis, coord, ld<Active>(p, p.hin, c, k, j, i) - 0.0f);
+    return de<Metric>(p, axis, coord, ld<Active>(p, p.hin, c, k, j, i) - 0.0f);
   }
   if (coord == n) {
     if (!wall(p.metallic, axis, true)) return 0.0f;
-    return de(p, axis, coord, 0.0f - ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2)));
+    return de<Metric>(p, axis, coord, 0.0f - ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2)));
   }
   const float hi = ld<Active>(p, p.hin, c, k, j, i);
   const float lo = ld<Active>(p, p.hin, c, k - (axis == 0), j - (axis == 1), i - (axis == 2));
-  return de(p, axis, coord, hi - lo);
+  return de<Metric>(p, axis, coord, hi - lo);
 }
 
-template <int Active, bool Cpml, int Mat>
+template <int Active, bool Cpml, int Mat, bool Metric>
 __global__ void __launch_bounds__(256) phase_h_kernel(Step3D p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -72,8 +72,8 @@ __global__ void __launch_bounds__(256) phase_h_kernel(Step3D p) {
   if (active<Active>(3)) {
     const Dims d = component_dims(3, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = fdiff<Active>(p, 2, 1, k, j, i);
-      float d1 = fdiff<Active>(p, 1, 0, k, j, i);
+      float d0 = fdiff<Active, Metric>(p, 2, 1, k, j, i);
+      float d1 = fdiff<Active, Metric>(p, 1, 0, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<1>(p.ht[0], d0, k, j, i, true);
         d1 = cpml_correct<0>(p.ht[1], d1, k, j, i, true);
@@ -88,8 +88,8 @@ __global__ void __launch_bounds__(256) phase_h_kernel(Step3D p) {
   if (active<Active>(4)) {
     const Dims d = component_dims(4, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = fdiff<Active>(p, 0, 0, k, j, i);
-      float d1 = fdiff<Active>(p, 2, 2, k, j, i);
+      float d0 = fdiff<Active, Metric>(p, 0, 0, k, j, i);
+      float d1 = fdiff<Active, Metric>(p, 2, 2, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<0>(p.ht[2], d0, k, j, i, true);
         d1 = cpml_correct<2>(p.ht[3], d1, k, j, i, true);
@@ -104,8 +104,8 @@ __global__ void __launch_bounds__(256) phase_h_kernel(Step3D p) {
   if (active<Active>(5)) {
     const Dims d = component_dims(5, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = fdiff<Active>(p, 1, 2, k, j, i);
-      float d1 = fdiff<Active>(p, 0, 1, k, j, i);
+      float d0 = fdiff<Active, Metric>(p, 1, 2, k, j, i);
+      float d1 = fdiff<Active, Metric>(p, 0, 1, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<2>(p.ht[4], d0, k, j, i, true);
         d1 = cpml_correct<1>(p.ht[5], d1, k, j, i, true);
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) phase_h_kernel(Step3D p) {
   }
 }
 
-template <int Active, bool Cpml, int Mat>
+template <int Active, bool Cpml, int Mat, bool Metric>
 __global__ void __launch_bounds__(256) phase_e_kernel(Step3D p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -127,8 +127,8 @@ __global__ void __launch_bounds__(256) phase_e_kernel(Step3D p) {
   if (active<Active>(0)) {
     const Dims d = component_dims(0, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = bdiff<Active>(p, 5, 1, k, j, i);
-      float d1 = bdiff<Active>(p, 4, 0, k, j, i);
+      float d0 = bdiff<Active, Metric>(p, 5, 1, k, j, i);
+      float d1 = bdiff<Active, Metric>(p, 4, 0, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
         d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -143,8 +143,8 @@ __global__ void __launch_bounds__(256) phase_e_kernel(Step3D p) {
   if (active<Active>(1)) {
     const Dims d = component_dims(1, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = bdiff<Active>(p, 3, 0, k, j, i);
-      float d1 = bdiff<Active>(p, 5, 2, k, j, i);
+      float d0 = bdiff<Active, Metric>(p, 3, 0, k, j, i);
+      float d1 = bdiff<Active, Metric>(p, 5, 2, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
         d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -159,8 +159,8 @@ __global__ void __launch_bounds__(256) phase_e_kernel(Step3D p) {
   if (active<Active>(2)) {
     const Dims d = component_dims(2, p.Z, p.Y, p.X);
     if (k < d.z && j < d.y && i < d.x) {
-      float d0 = bdiff<Active>(p, 4, 2, k, j, i);
-      float d1 = bdiff<Active>(p, 3, 1, k, j, i);
+      float d0 = bdiff<Active, Metric>(p, 4, 2, k, j, i);
+      float d1 = bdiff<Active, Metric>(p, 3, 1, k, j, i);
       if (Cpml) {
         d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
         d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);
@@ -186,10 +186,13 @@ cudaError_t launch_phase_t(cudaStream_t s, const Step3D& p, int phase) {
   if (zmax == 0 || ymax == 0 || xmax == 0) return cudaSuccess;
   const dim3 block(32, 8, 1);
   const dim3 grid((xmax + 31) / 32, (ymax + 7) / 8, zmax);
+  const bool metric = has_metric(p);
   if (phase == 0) {
-    phase_h_kernel<Active, Cpml, Mat><<<grid, block, 0, s>>>(p);
+    if (metric) phase_h_kernel<Active, Cpml, Mat, true><<<grid, block, 0, s>>>(p);
+    else phase_h_kernel<Active, Cpml, Mat, false><<<grid, block, 0, s>>>(p);
   } else {
-    phase_e_kernel<Active, Cpml, Mat><<<grid, block, 0, s>>>(p);
+    if (metric) phase_e_kernel<Active, Cpml, Mat, true><<<grid, block, 0, s>>>(p);
+    else phase_e_kernel<Active, Cpml, Mat, false><<<grid, block, 0, s>>>(p);
   }
   return cudaPeekAtLastError();
 }
