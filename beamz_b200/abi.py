@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 9
+FDTD_ABI_VERSION = 10
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_launch_program",
     "fdtd_apply_sources",
     "fdtd_accumulate_dft",
+    "fdtd_record_fields",
     "fdtd_copy_component",
     "fdtd_adjoint_step",
     "fdtd_adjoint_curl",
@@ -186,6 +187,25 @@ class FdtdRegistration(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char_p), ("fn", ctypes.c_void_p)]
 
 
+FDTD_MAX_RECORDERS = 4
+
+
+class FdtdRecorder(ctypes.Structure):
+    _fields_ = [
+        ("interval", ctypes.c_int32),
+        ("capacity", ctypes.c_int32),
+        ("component_count", ctypes.c_int32),
+        ("components", ctypes.c_int32 * 6),
+        ("signs", ctypes.c_float * 6),
+        ("indices", FdtdBuffer * 6),
+        ("weights", FdtdBuffer * 6),
+        ("values", FdtdBuffer * 6),
+        ("steps", FdtdBuffer),
+        ("times", FdtdBuffer),
+        ("count", FdtdBuffer),
+    ]
+
+
 class FdtdProgram(ctypes.Structure):
     _fields_ = [
         ("abi_version", ctypes.c_int32),
@@ -230,6 +250,9 @@ class FdtdProgram(ctypes.Structure):
         ("status", FdtdBuffer),
         ("metric_h", FdtdBuffer * 3),
         ("metric_e", FdtdBuffer * 3),
+        ("recorder_count", ctypes.c_int32),
+        ("reserved_recorders", ctypes.c_int32),
+        ("recorders", FdtdRecorder * FDTD_MAX_RECORDERS),
     ]
 
 
@@ -294,6 +317,8 @@ def load_library(path: str | None = None):
         lib.fdtd_apply_sources.restype = ctypes.c_int
         lib.fdtd_accumulate_dft.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32]
         lib.fdtd_accumulate_dft.restype = ctypes.c_int
+        lib.fdtd_record_fields.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdProgram), ctypes.c_int32]
+        lib.fdtd_record_fields.restype = ctypes.c_int
         lib.fdtd_copy_component.argtypes = [ctypes.c_void_p, ctypes.POINTER(FdtdBuffer), ctypes.POINTER(FdtdBuffer),
                                             ctypes.POINTER(ctypes.c_int64)]
         lib.fdtd_copy_component.restype = ctypes.c_int

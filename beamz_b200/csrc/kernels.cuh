@@ -192,6 +192,27 @@ struct MonitorReduceDev {
 };
 cudaError_t launch_monitor_reduce(cudaStream_t s, const MonitorReduceDev& r);
 
+// One field recorder for one step (recorder.cu); see FdtdRecorder.
+struct RecorderDev {
+  int interval = 1, capacity = 0, ncomp = 0;
+  int64_t start[7] = {0, 0, 0, 0, 0, 0, 0};  // prefix sums of the value counts
+  float sign[6] = {1, 1, 1, 1, 1, 1};
+  int slots[6] = {0, 0, 0, 0, 0, 0};          // gather slots K; 0 = whole component
+  const int* idx[6] = {};
+  const float* w[6] = {};
+  float* values[6] = {};
+  const float* field[6] = {};                 // the component in the step's output bank
+  int64_t field_len[6] = {};
+  int64_t dy[6] = {}, dx[6] = {};             // component extents (whole recorders)
+  int64_t row[6] = {}, plane[6] = {};         // device-layout strides
+  int* steps = nullptr;
+  float* times = nullptr;
+  int* count = nullptr;
+  const float* step_time = nullptr;
+  int step_time_len = 0;
+};
+cudaError_t launch_record(cudaStream_t s, const RecorderDev& r, const int* counter, int step_offset);
+
 // Gather-plan packing (planner.cu): one (monitor, component) plan.
 struct GatherPackDev {
   const int* idx_in = nullptr;    // [points, slots_in]

@@ -229,7 +229,74 @@ int validate(const FdtdProgram& p) {
         (!is_f32(d.samples) || elements(d.samples) != static_cast<int64_t>(d.batch) * M * 6 * d.indices.dims[3]))
       return kInvalid;
   }
+  if (p.recorder_count < 0 || p.recorder_count > FDTD_MAX_RECORDERS) return kInvalid;
+  if (p.recorder_count > 0 && (!is_f32(p.step_time) || elements(p.step_time) < 1 || p.step_time.data == nullptr))
+    return kInvalid;
+  for (int r = 0; r < p.recorder_count; ++r) {
+    const FdtdRecorder& rec = p.recorders[r];
+    if (rec.interval < 1 || rec.capacity < 0 || rec.component_count < 1 || rec.component_count > 6) return kInvalid;
+    const int64_t cap = rec.capacity;
+    if (rec.steps.element_type != FDTD_S32 || elements(rec.steps) != cap || (cap > 0 && rec.steps.data == nullptr))
+      return kInvalid;
+    if (!is_f32(rec.times) || elements(rec.times) != cap || (cap > 0 && rec.times.data == nullptr)) return kInvalid;
+    if (rec.count.element_type != FDTD_S32 || elements(rec.count) != 2 || rec.count.data == nullptr) return kInvalid;
+    for (int q = 0; q < rec.component_count; ++q) {
+      const int c = rec.components[q];
+      if (c < 0 || c > 5 || !((L.active >> c) & 1)) return kInvalid;
+      const FdtdBuffer &ix = rec.indices[q], &w = rec.weights[q];
+      int64_t V;
+      if (ix.data == nullptr && w.data == nullptr) {
+        V = dims_count(component_dims(c, L.Z, L.Y, L.X));
+      } else {
+        if (ix.element_type != FDTD_S32 || !is_f32(w) || ix.rank != 2 || w.rank != 2 || ix.data == nullptr ||
+            w.data == nullptr || ix.dims[0] != w.dims[0] || ix.dims[1] != w.dims[1] || ix.dims[0] < 1 ||
+            ix.dims[0] > 32)
+          return kInvalid;
+        V = ix.dims[1];
+      }
+      if (!is_f32(rec.values[q]) || elements(rec.values[q]) != cap * V || (cap * V > 0 && rec.values[q].data == nullptr))
+        return kInvalid;
+    }
+  }
   return 0;
+}
+
+// Device view of recorder r reading the component arrays of `bank`.
+RecorderDev recorder_dev(const FdtdProgram& p, const Layout& L, int r, const FdtdBuffer* bank) {
+  const FdtdRecorder& rec = p.recorders[r];
+  RecorderDev d;
+  d.interval = rec.interval;
+  d.capacity = rec.capacity;
+  d.ncomp = rec.component_count;
+  const bool pitched = p.layout == FDTD_LAYOUT_PITCHED;
+  for (int q = 0; q < d.ncomp; ++q) {
+    const int c = rec.components[q];
+    const Dims cd = component_dims(c, L.Z, L.Y, L.X);
+    d.sign[q] = rec.signs[q];
+    d.field[q] = static_cast<const float*>(bank[c].data);
+    d.field_len[q] = elements(bank[c]);
+    d.dy[q] = cd.y;
+    d.dx[q] = cd.x;
+    d.row[q] = pitched ? p.pitch : cd.x;
+    d.plane[q] = pitched ? p.pitch * (L.Y + 1) : static_cast<int64_t>(cd.y) * cd.x;
+    int64_t V;
+    if (rec.indices[q].data == nullptr) {
+      V = dims_count(cd);
+    } else {
+      d.slots[q] = static_cast<int>(rec.indices[q].dims[0]);
+      d.idx[q] = static_cast<const int*>(rec.indices[q].data);
+      d.w[q] = static_cast<const float*>(rec.weights[q].data);
+      V = rec.indices[q].dims[1];
+    }
+    d.values[q] = static_cast<float*>(rec.values[q].data);
+    d.start[q + 1] = d.start[q] + V;
+  }
+  d.steps = static_cast<int*>(rec.steps.data);
+  d.times = static_cast<float*>(rec.times.data);
+  d.count = static_cast<int*>(rec.count.data);
+  d.step_time = static_cast<const float*>(p.step_time.data);
+  d.step_time_len = static_cast<int>(elements(p.step_time));
+  return d;
 }
 
 CpmlTermDev term_dev(const FdtdCpmlTerm& t, const Dims& target, int axis, bool alt_in, bool alt_out) {
@@ -543,6 +610,10 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
       err = launch_dft(s, make_dft(p, b), counter, step);
       if (err != cudaSuccess) return err;
     }
+    for (int r = 0; r < p.recorder_count; ++r) {
+      err = launch_record(s, recorder_dev(p, L, r, b), counter, step);
+      if (err != cudaSuccess) return err;
+    }
   }
   if (ss) {  // join: the flush reads the step counter, and callers read the arena
     cudaError_t err = cudaEventRecord(ss->joined, ds);
@@ -697,6 +768,22 @@ int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_o
   if (p.dft.monitor_count == 0) return 0;
   return static_cast<int>(fdtd::launch_dft(static_cast<cudaStream_t>(stream), fdtd::make_dft(p, p.fields),
                                            static_cast<const int*>(p.step_counter.data), step_offset));
+}
+
+int fdtd_record_fields(void* stream, const FdtdProgram* program, int32_t step_offset) {
+  if (program == nullptr) return fdtd::kInvalid;
+  FdtdProgram p = *program;
+  p.schedule = FDTD_SCHEDULE_PHASES;
+  const int v = fdtd::validate(p);
+  if (v != 0) return v;
+  fdtd::Layout L;
+  fdtd::layout_of(p, &L);
+  for (int r = 0; r < p.recorder_count; ++r) {
+    const cudaError_t err = fdtd::launch_record(static_cast<cudaStream_t>(stream), fdtd::recorder_dev(p, L, r, p.fields),
+                                                static_cast<const int*>(p.step_counter.data), step_offset);
+    if (err != cudaSuccess) return static_cast<int>(err);
+  }
+  return 0;
 }
 
 int fdtd_copy_component(void* stream, const FdtdBuffer* src, const FdtdBuffer* dst, const int64_t* extent) {

@@ -631,6 +631,53 @@ def plane_monitor(grid_shape, resolution, normal_axis, position, coords_a, coord
     return DftMonitorPlan(np.asarray(freqs, np.float32), idx, w, mask, **kwargs)
 
 
+@dataclass
+class RecorderPlan:
+    """A time-domain field recorder (beamz's ``FieldRecorder``:
+    devices/monitors/compiler.py:286-412, recorded by
+    simulation/observe.py:588-646): after each step s with (s + 1) % interval
+    == 0, while fewer than ``capacity`` records exist, one record of every
+    listed component, times its sign.  ``indices``/``weights`` (per component,
+    (V, K) dense flat offsets and interpolation weights, summed over K) sample
+    a plane or line; None records the whole component in its own order."""
+
+    components: tuple
+    interval: int = 1
+    capacity: int = 1
+    indices: list | None = None
+    weights: list | None = None
+    shapes: tuple | None = None  # per component, the shape of one record
+    signs: tuple | None = None
+
+    def sign(self, q: int) -> float:
+        return 1.0 if self.signs is None else float(self.signs[q])
+
+
+def records_for(num_steps: int, interval: int) -> int:
+    """Record slots of a run: ceil(num_steps / interval) (compiler.py:282-284)."""
+    return int(np.ceil(int(num_steps) / max(1, int(interval))))
+
+
+def domain_recorder(grid_shape, components, interval: int, num_steps: int, polarization: str = "tm") -> RecorderPlan:
+    """Whole-component snapshots every ``interval`` steps (``region="domain"``)."""
+    shapes = tuple(component_shape(c, grid_shape, polarization) for c in components)
+    return RecorderPlan(tuple(components), max(1, int(interval)), records_for(num_steps, interval), shapes=shapes)
+
+
+def plane_recorder(grid_shape, resolution, normal_axis, position, coords_a, coords_b, components, interval: int,
+                   num_steps: int) -> RecorderPlan:
+    """Interpolated samples of a 3D plane every ``interval`` steps, on the
+    (coords_a, coords_b) points (the DFT plane gather of :func:`plane_gather`)."""
+    idx, w = [], []
+    for c in components:
+        i, ww = plane_gather(c, normal_axis, position, coords_a, coords_b, resolution, grid_shape)
+        idx.append(i)
+        w.append(ww)
+    shape = (len(coords_a), len(coords_b))
+    return RecorderPlan(tuple(components), max(1, int(interval)), records_for(num_steps, interval), idx, w,
+                        shapes=(shape,) * len(components))
+
+
 def sources_clear_of_monitors(spec) -> bool:
     """True when no pre-E source cell is read by a DFT monitor's gather (same
     component, nonzero weight, component not masked off).
@@ -787,6 +834,8 @@ class ProgramSpec:
     # Derivative metrics of an axis-uniform or rectilinear grid; None on the
     # isotropic grid (differences over `resolution`).
     metrics: DerivativeMetrics | None = None
+    # Time-domain field recorders (at most four).
+    recorders: list = field(default_factory=list)
 
     @property
     def ndim(self) -> int:

@@ -206,6 +206,26 @@ def pack_dft_monitors(monitors, device, shapes, strides) -> DftArena | None:
     return arena
 
 
+def _pack_plan(lib, stream, indices, weights, dims, strides, device):
+    """One (V, K) gather plan as device [K, V] arrays in the device layout,
+    nonzero weights first per value (fdtd_pack_gather)."""
+    torch = _torch()
+    ic = torch.as_tensor(np.ascontiguousarray(np.asarray(indices).reshape(len(indices), -1), np.int32), device=device)
+    wc = torch.as_tensor(np.ascontiguousarray(np.asarray(weights, np.float32).reshape(ic.shape)), device=device)
+    V, K = (int(v) for v in ic.shape)
+    out_i = torch.zeros((K, V), dtype=torch.int32, device=device)
+    out_w = torch.zeros((K, V), dtype=torch.float32, device=device)
+    g = abi.FdtdGatherPack()
+    g.indices_in, g.weights_in = abi.buffer_of(ic), abi.buffer_of(wc)
+    g.indices_out, g.weights_out = abi.buffer_of(out_i), abi.buffer_of(out_w)
+    for a, n in enumerate((1,) * (3 - len(dims)) + tuple(dims)):
+        g.dims[a] = int(n)
+    g.row, g.plane = strides
+    abi.check(lib.fdtd_pack_gather(stream, ctypes.byref(g)), "fdtd_pack_gather")
+    torch.cuda.current_stream(device).synchronize()
+    return out_i, out_w
+
+
 class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
@@ -358,6 +378,33 @@ class DeviceProgram:
             s.dft.monitor_count = len(spec.monitors)
             for name in ("indices", "weights", "freqs", "masks", "counts", "codes", "windows"):
                 setattr(s.dft, name, buf(getattr(a, name)))
+        # Time-domain field recorders.
+        if len(spec.recorders) > abi.FDTD_MAX_RECORDERS:
+            raise ValueError(f"at most {abi.FDTD_MAX_RECORDERS} field recorders")
+        self.recorders = []  # per recorder: values per record of each component
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        s.recorder_count = len(spec.recorders)
+        for r, rec in enumerate(spec.recorders):
+            d = s.recorders[r]
+            d.interval, d.capacity = max(1, int(rec.interval)), max(0, int(rec.capacity))
+            if not 1 <= len(rec.components) <= 6:
+                raise ValueError("a field recorder records 1 to 6 components")
+            d.component_count = len(rec.components)
+            counts = []
+            for q, c in enumerate(rec.components):
+                if c not in self.active:
+                    raise ValueError(f"field recorder component {c} is inactive in this program")
+                ci = COMPONENT_INDEX[c]
+                d.components[q] = ci
+                d.signs[q] = rec.sign(q)
+                if rec.indices is None:
+                    counts.append(int(np.prod(self.shapes[c])))
+                    continue
+                pi, pw = _pack_plan(self.lib, stream, rec.indices[q], rec.weights[q], self.shapes[c],
+                                    self._strides(ci), dev)
+                d.indices[q], d.weights[q] = buf(pi), buf(pw)
+                counts.append(int(pi.shape[1]))
+            self.recorders.append(counts)
         self._times_for(max(int(spec.total_steps), 1))
         self.struct = s
 
@@ -442,6 +489,11 @@ class DeviceProgram:
                 s.dft.samples = abi.buffer_of(state.dft_samples)
                 if self.dft_overlap:
                     s.flags |= abi.FDTD_FLAG_DFT_OVERLAP
+        for r, bufs in enumerate(state.records):
+            d = s.recorders[r]
+            for q, v in enumerate(bufs["values"]):
+                d.values[q] = abi.buffer_of(v)
+            d.steps, d.times, d.count = (abi.buffer_of(bufs[k]) for k in ("steps", "times", "count"))
         s.step_counter = abi.buffer_of(state.counter)
         s.step_time = abi.buffer_of(self.step_time)
         s.status = abi.buffer_of(state.status)
@@ -493,6 +545,15 @@ class DeviceState:
         if a is not None and program.dft_batch > 1:
             M, P = len(a.layout), int(a.indices.shape[3])
             self.dft_samples = torch.empty((program.dft_batch, M, 6, P), dtype=torch.float32, device=dev)
+        self.records = []
+        for rec, counts in zip(program.spec.recorders, program.recorders):
+            cap = max(0, int(rec.capacity))
+            self.records.append({
+                "values": [torch.zeros((cap, v), dtype=torch.float32, device=dev) for v in counts],
+                "steps": torch.zeros(cap, dtype=torch.int32, device=dev),
+                "times": torch.zeros(cap, dtype=torch.float32, device=dev),
+                "count": torch.zeros(2, dtype=torch.int32, device=dev),
+            })
         self.counter = torch.full((1,), int(step), dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.step = int(step)
@@ -581,8 +642,12 @@ def apply_sources(state: DeviceState, program: DeviceProgram, timing: str) -> De
 
 
 def accumulate_monitors(state: DeviceState, program: DeviceProgram) -> DeviceState:
+    """The end-of-step monitor updates: DFT accumulation, then the field
+    recorders (beamz/simulation/observe.py:649-795)."""
     s = program.fill(state, 0)
     abi.check(program.lib.fdtd_accumulate_dft(_stream(program), ctypes.byref(s), 0), "fdtd_accumulate_dft")
+    if s.recorder_count:
+        abi.check(program.lib.fdtd_record_fields(_stream(program), ctypes.byref(s), 0), "fdtd_record_fields")
     return state
 
 
@@ -798,3 +863,17 @@ def modal_overlap(state: DeviceState, program: DeviceProgram, monitor: int, mode
     sums = _monitor_reduce(state, program, monitor, e, h, _flux_scales(state, program, monitor, base_dt),
                            weights, prof)
     return 0.25 * float(direction_sign) * (sums[:, :, 0] - sums[:, :, 1])
+
+
+def recorded(state: DeviceState, program: DeviceProgram, recorder: int) -> dict:
+    """What field recorder ``recorder`` holds so far, as beamz returns it
+    (observe.py:588-646): ``steps`` (absolute step + 1 of each record),
+    ``times`` (t + dt), and per component its records [n, *shape]."""
+    rec = program.spec.recorders[recorder]
+    bufs = state.records[recorder]
+    n = int(bufs["count"][state.step & 1].item())
+    out = {"steps": bufs["steps"][:n].cpu().numpy(), "times": bufs["times"][:n].cpu().numpy()}
+    for q, c in enumerate(rec.components):
+        shape = rec.shapes[q] if rec.shapes is not None else program.shapes[c]
+        out[c] = bufs["values"][q][:n].cpu().numpy().reshape((n, *shape))
+    return out

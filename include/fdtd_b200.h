@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 9
+#define FDTD_ABI_VERSION 10
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -161,6 +161,34 @@ typedef struct FdtdDft {
   FdtdBuffer samples;
 } FdtdDft;
 
+/* A time-domain field recorder (beamz: FieldRecorder, compiled by
+ * devices/monitors/compiler.py:286-412 and updated each step by
+ * simulation/observe.py:588-646 _record_fields).  After every step s with
+ * (s + 1) % interval == 0, while fewer than `capacity` records exist, record
+ * n = count writes, for each recorded component q:
+ *   values[q][n, v] = sign[q] * field value v,
+ * where field value v is, with indices/weights null, element v of the
+ * component in its own (z, y, x) order (a "domain" recorder), else the sum
+ * over slots k of field[indices[k, v]] * weights[k, v] in slot order, up to
+ * the first zero weight (plans packed by fdtd_pack_gather); steps[n] = s + 1
+ * and times[n] = step_time[s].  `count` holds the number of records twice,
+ * double-buffered by step parity (read count[s & 1], write count[(s+1) & 1]),
+ * and starts as {0, 0}. */
+#define FDTD_MAX_RECORDERS 4
+typedef struct FdtdRecorder {
+  int32_t interval;
+  int32_t capacity;
+  int32_t component_count;  /* 1..6 */
+  int32_t components[6];    /* component index of each value set */
+  float signs[6];
+  FdtdBuffer indices[6];    /* S32 [K, V] device-layout offsets, or null */
+  FdtdBuffer weights[6];    /* F32 [K, V], or null */
+  FdtdBuffer values[6];     /* F32 [capacity, V] */
+  FdtdBuffer steps;         /* S32 [capacity] */
+  FdtdBuffer times;         /* F32 [capacity] */
+  FdtdBuffer count;         /* S32 [2] */
+} FdtdRecorder;
+
 /* A complete step program (replaces BeamzLaunch + BeamzProgramLaunch,
  * beamz: cuda/src/launch.h:19-77). */
 typedef struct FdtdProgram {
@@ -222,6 +250,10 @@ typedef struct FdtdProgram {
    * grid repeats one value).  FDTD_LAYOUT_DENSE only; no adjoint. */
   FdtdBuffer metric_h[3];
   FdtdBuffer metric_e[3];
+  /* Field recorders, run after each step's DFT sample (see FdtdRecorder). */
+  int32_t recorder_count;
+  int32_t reserved_recorders;
+  FdtdRecorder recorders[FDTD_MAX_RECORDERS];
 } FdtdProgram;
 
 /* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */
@@ -256,6 +288,11 @@ int fdtd_apply_sources(void* stream, const FdtdProgram* program, int32_t timing,
 /* Accumulate the DFT monitors once from `program->fields` for absolute step
  * counter[0] + step_offset (beamz: cuda/src/io.cu:381-401). */
 int fdtd_accumulate_dft(void* stream, const FdtdProgram* program, int32_t step_offset);
+
+/* Record every field recorder once from `program->fields` for absolute step
+ * counter[0] + step_offset (as fdtd_launch_program does after each step;
+ * beamz: observe.py:588-646). */
+int fdtd_record_fields(void* stream, const FdtdProgram* program, int32_t step_offset);
 
 /* Copy the (extent[0], extent[1], extent[2]) corner block between two rank-3
  * F32 buffers whose own dims give their row and plane pitches (dense <->

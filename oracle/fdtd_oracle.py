@@ -962,6 +962,60 @@ class OracleState:
     dft_w: np.ndarray | None = None
     t: float = 0.0
     step: int = 0
+    records: list = field(default_factory=list)  # per field recorder (see record_fields)
+
+
+@dataclass
+class FieldRecorder:
+    """A compiled time-domain field recorder (beamz/devices/monitors/
+    compiler.py:286-412): ``indices``/``weights`` per component are (V, K)
+    dense flat offsets and interpolation weights, or None for the whole
+    component."""
+
+    components: tuple
+    interval: int = 1
+    capacity: int = 1
+    indices: list | None = None
+    weights: list | None = None
+    signs: tuple | None = None
+
+
+def new_records(recorders, shapes: dict, dtype=np.float32) -> list:
+    out = []
+    for rec in recorders:
+        sizes = [int(np.prod(shapes[c])) if rec.indices is None else int(np.shape(rec.indices[q])[0])
+                 for q, c in enumerate(rec.components)]
+        out.append({"values": [np.zeros((rec.capacity, v), dtype) for v in sizes],
+                    "steps": np.zeros(rec.capacity, np.int32), "times": np.zeros(rec.capacity, dtype), "count": 0})
+    return out
+
+
+def record_fields(recorders, records, fields, step: int, t_phys) -> None:
+    """beamz/simulation/observe.py:588-646 (_record_fields): after step ``step``
+    with (step + 1) % interval == 0 (monitor_records_on_step, 322-324), while
+    fewer than ``capacity`` records exist, record each component (the whole
+    array, or sum_k field[idx[:, k]] * w[:, k] in slot order) times its sign,
+    the step + 1 and the time t + dt.  beamz sums the K slots with jnp.sum;
+    the slot order here is the engine's, as for the DFT gather."""
+    for rec, store in zip(recorders, records):
+        n = store["count"]
+        if (int(step) + 1) % max(1, int(rec.interval)) != 0 or n >= rec.capacity:
+            continue
+        for q, c in enumerate(rec.components):
+            f = np.asarray(fields[c]).reshape(-1)
+            if rec.indices is None:
+                value = f
+            else:
+                idx = np.asarray(rec.indices[q]).reshape(len(rec.indices[q]), -1)
+                w = np.asarray(rec.weights[q], f.dtype).reshape(idx.shape)
+                value = f[idx[:, 0]] * w[:, 0]
+                for k in range(1, idx.shape[1]):
+                    value = value + f[idx[:, k]] * w[:, k]
+            sign = f.dtype.type(1.0 if rec.signs is None else rec.signs[q])
+            store["values"][q][n] = value * sign
+        store["steps"][n] = int(step) + 1
+        store["times"][n] = t_phys
+        store["count"] = n + 1
 
 
 @dataclass
@@ -982,6 +1036,7 @@ class OracleProgram:
     monitors: list = field(default_factory=list)
     polarization: str = "tm"
     metrics: dict | None = None  # DerivativeMetricPlan names -> inverse distances (None: isotropic)
+    recorders: list = field(default_factory=list)  # FieldRecorder
 
     @property
     def ndim(self):
@@ -994,7 +1049,8 @@ def new_state(program: OracleProgram, dtype=np.float32, t0: float = 0.0) -> Orac
     psi_h = [np.zeros(t.psi_shape(shapes[t.component]), dtype) for t in program.h_terms]
     psi_e = [np.zeros(t.psi_shape(shapes[t.component]), dtype) for t in program.e_terms]
     nv, nw = dft_arena_sizes(program.monitors)
-    return OracleState(fields, psi_h, psi_e, np.zeros(nv, dtype), np.zeros(nv, dtype), np.zeros(nw, dtype), t0, 0)
+    return OracleState(fields, psi_h, psi_e, np.zeros(nv, dtype), np.zeros(nv, dtype), np.zeros(nw, dtype), t0, 0,
+                       new_records(program.recorders, shapes, dtype))
 
 
 def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
@@ -1041,6 +1097,7 @@ def forward_step(state: OracleState, program: OracleProgram) -> OracleState:
         t_phys = float(state.t) + float(program.dt)
     for mon in program.monitors:
         accumulate_dft(mon, (state.dft_re, state.dft_im, state.dft_w), fields, t_phys, step, program.dt)
+    record_fields(program.recorders, state.records, fields, step, t_phys)
     state.t = t_phys
     state.step = step + 1
     return state

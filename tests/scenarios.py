@@ -33,7 +33,9 @@ def to_oracle(spec: P.ProgramSpec, dtype=np.float32) -> O.OracleProgram:
     prog = O.OracleProgram(tuple(spec.grid_shape), float(spec.dt), float(spec.resolution), terms(spec.h_terms),
                            terms(spec.e_terms), metallic_edges=frozenset(spec.metallic_edges), sources=sources,
                            monitors=monitors, polarization=spec.polarization,
-                           metrics=spec.metrics.as_dict() if spec.metrics is not None else None)
+                           metrics=spec.metrics.as_dict() if spec.metrics is not None else None,
+                           recorders=[O.FieldRecorder(r.components, r.interval, r.capacity, r.indices, r.weights,
+                                                      r.signs) for r in spec.recorders])
     if spec.ndim == 3:
         eps = np.asarray(spec.eps_table, np.float32)[spec.voxel_ids]
         prog.material = O.material_from_voxels(eps, dtype=dtype)
