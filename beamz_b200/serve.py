@@ -51,6 +51,7 @@ class Result:
     arrival: float
     admitted: float
     finished: float
+    records: list | None = None  # per field recorder: runtime.recorded(...)
 
     @property
     def latency(self) -> float:
@@ -59,7 +60,8 @@ class Result:
 
 def estimate_bytes(spec: ProgramSpec, schedule: str = "fused") -> int:
     """Device bytes one simulation holds: two field banks (one for the phase
-    schedule), CPML memories (H double-banked), material, DFT arena, clock."""
+    schedule), CPML memories (H double-banked), material, DFT arena, field
+    recorders, clock."""
     active = active_components(spec.ndim, spec.polarization)
     shapes = {c: component_shape(c, spec.grid_shape, spec.polarization) for c in COMPONENTS}
     banks = 2 if schedule == "fused" else 1
@@ -77,7 +79,14 @@ def estimate_bytes(spec: ProgramSpec, schedule: str = "fused") -> int:
     for m in spec.monitors:
         points = max(int(np.asarray(ix).shape[0]) for ix in m.indices)
         dft += 6 * len(m.freqs) * points * 8 * 2 + 6 * points * 8 * 8 + 8 * 6 * points * 4  # + sample batch
-    return banks * field_bytes + material + psi + dft + 4 * max(int(spec.total_steps), 1) + (1 << 20)
+    records = 0
+    for r in spec.recorders:
+        for q, c in enumerate(r.components):
+            values = int(np.prod(shapes[c])) if r.indices is None else int(np.asarray(r.indices[q]).shape[0])
+            plan = 0 if r.indices is None else values * np.asarray(r.indices[q]).shape[1] * 8
+            records += int(r.capacity) * values * 4 + plan
+        records += int(r.capacity) * 8 + 8
+    return banks * field_bytes + material + psi + dft + records + 4 * max(int(spec.total_steps), 1) + (1 << 20)
 
 
 class _Slot:
@@ -147,7 +156,12 @@ def _collect(state, program, return_fields: bool):
         "dft_im": state.dft_im.cpu().numpy(),
         "dft_w": state.dft_w.cpu().numpy(),
         "fields": None,
+        "records": None,
     }
+    if program.spec.recorders:
+        from . import runtime
+
+        out["records"] = [runtime.recorded(state, program, r) for r in range(len(program.spec.recorders))]
     if return_fields:
         out["fields"] = {c: state.field(c).cpu().numpy() for c in COMPONENTS if c in program.active}
     return out
@@ -245,7 +259,7 @@ class ServingEngine:
                     finished = clock() - t0
                     r = slot.req
                     results[r.rid] = Result(r.rid, r.nsteps, out["dft_re"], out["dft_im"], out["dft_w"], out["fields"],
-                                            r.arrival, slot.admitted, finished)
+                                            r.arrival, slot.admitted, finished, out["records"])
                     used -= slot.nbytes
                     cells -= slot.req.spec.cells
                     slot.release()
@@ -283,7 +297,7 @@ def run_sequential(requests: list[Request], device="cuda", return_fields: bool =
         out = _collect(state, program, return_fields)
         torch.cuda.synchronize(dev)
         results[req.rid] = Result(req.rid, req.nsteps, out["dft_re"], out["dft_im"], out["dft_w"], out["fields"],
-                                  req.arrival, admitted, clock() - t0)
+                                  req.arrival, admitted, clock() - t0, out["records"])
         del state, program
     return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
 

@@ -70,6 +70,26 @@ def test_results_identical_alone_and_in_the_mix():
 
 
 @pytest.mark.gpu
+def test_recorders_identical_alone_and_in_the_mix():
+    import dataclasses
+
+    reqs = _mix()
+    for r in (reqs[1], reqs[4]):
+        spec = r.spec
+        rec = P.domain_recorder(spec.grid_shape, P.active_components(spec.ndim, spec.polarization)[:2], 25,
+                                r.nsteps, spec.polarization)
+        r.spec = dataclasses.replace(spec, recorders=[rec])
+    mixed = serve.ServingEngine(max_active=3, chunk=64).run(reqs)
+    alone = serve.run_sequential(reqs)
+    for m, a in zip(mixed, alone):
+        assert (m.records is None) == (a.records is None) == (m.rid not in (1, 4))
+        for rm, ra in zip(m.records or [], a.records or []):
+            assert len(ra["steps"]) == reqs[m.rid].nsteps // 25
+            for k in ra:
+                np.testing.assert_array_equal(rm[k], ra[k], err_msg=f"request {m.rid} {k}")
+
+
+@pytest.mark.gpu
 def test_budget_limits_residency():
     reqs = _mix()
     one = max(serve.estimate_bytes(r.spec) for r in reqs)
