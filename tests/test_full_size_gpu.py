@@ -1,0 +1,78 @@
+"""The 512 x 512 x 256 CPML workload (config 2: Si boxes, Ey dipole, four
+x-normal DFT planes) at full size, through properties that do not need the
+numpy oracle to finish: agreement with the C restatement of the reference
+(1e-5 relative L2 for fields, 1e-4 for the DFT), bitwise
+agreement of the pitched TMA kernel with the dense kernel, exact linearity
+under a power-of-two scaling, and run-to-run determinism."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from beamz_b200 import plan as P  # noqa: E402
+from beamz_b200 import runtime as R  # noqa: E402
+from beamz_b200 import workloads as W  # noqa: E402
+from oracle import fdtd_oracle as O  # noqa: E402
+from tests.scenarios import random_initial_fields  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 3
+
+
+@pytest.fixture(scope="module")
+def scene():
+    spec = W.scene_3d_512(total_steps=STEPS)
+    return spec, random_initial_fields(spec, seed=21)
+
+
+def test_config2_matches_the_c_restatement(scene):
+    from oracle import cpu_port
+
+    spec, fields = scene
+    prog = R.compile_program(spec)
+    assert prog.layout == "pitched"
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, STEPS).numpy()
+    ref = cpu_port.HostRun(spec, fields).run(STEPS, threads=0)
+    for c in P.COMPONENTS:
+        assert O.relative_l2(out[c], ref.fields[c]) <= 1e-5, c
+    assert O.relative_l2(out["dft_re"], ref.dft_re) <= 1e-4
+    assert O.relative_l2(out["dft_im"], ref.dft_im) <= 1e-4
+
+
+def test_config2_pitched_and_dense_kernels_agree_bitwise(scene):
+    spec, fields = scene
+    pitched = R.compile_program(spec)
+    a = R.run_steps(R.initial_state(pitched, fields=fields), pitched, STEPS).numpy()
+    del pitched
+    torch.cuda.empty_cache()
+    dense = R.compile_program(spec, layout="dense")
+    b = R.run_steps(R.initial_state(dense, fields=fields), dense, STEPS).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(a[c], b[c], err_msg=c)
+    for x, y in zip(a["psi_h"] + a["psi_e"], b["psi_h"] + b["psi_e"]):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_config2_is_linear_and_deterministic(scene):
+    """Without sources the step is linear: fields scaled by 2 (exact) give
+    results scaled by 2 exactly, DFT arena included; a second run repeats
+    the first bit for bit."""
+    import dataclasses
+
+    spec, fields = scene
+    spec = dataclasses.replace(spec, sources=[])
+    prog = R.compile_program(spec)
+    one = R.run_steps(R.initial_state(prog, fields=fields), prog, STEPS).numpy()
+    again = R.run_steps(R.initial_state(prog, fields=fields), prog, STEPS).numpy()
+    two = R.run_steps(R.initial_state(prog, fields={c: 2 * v for c, v in fields.items()}), prog, STEPS).numpy()
+    for c in P.COMPONENTS:
+        np.testing.assert_array_equal(again[c], one[c], err_msg=c)
+        np.testing.assert_array_equal(two[c], 2 * one[c], err_msg=c)
+    for k in ("dft_re", "dft_im"):
+        np.testing.assert_array_equal(again[k], one[k])
+        np.testing.assert_array_equal(two[k], 2 * one[k])
+    np.testing.assert_array_equal(two["dft_w"], one["dft_w"])
