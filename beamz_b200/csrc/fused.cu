@@ -41,6 +41,7 @@ struct FusedSmem {
   float eps[3][HH][HW];
   float table[256];
   float amp[kMaxFusedSources];
+  float eamp[kMaxFusedSources];
 };
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
@@ -136,6 +137,34 @@ __device__ __forceinline__ void store_voxels(FusedSmem<TX, TY>& sm, const VoxelP
   }
 }
 
+// The pre-E source phase (beamz/simulation/execute.py:467-480) on the staged
+// copy of E plane q: every pre-E source adds coeff * amplitude to the cells of
+// its box, in source order, the halo included, so each CTA sees what the
+// separate source kernel would have written into the bank (same rounding).
+template <int TX, int TY, int Active>
+__device__ __forceinline__ void add_pre_e_sources(FusedSmem<TX, TY>& sm, const Step3D& p, int q, int j0, int i0,
+                                                  int tid) {
+  using S = FusedSmem<TX, TY>;
+  constexpr int NT = TX * TY;
+  const int slot = q % S::ES;
+  for (int s = 0; s < p.n_esrc; ++s) {
+    const SourceDev& src = p.esrc[s];
+    const int c = src.component;
+    if (c > 2 || !((Active >> c) & 1)) continue;
+    const Dims d = component_dims(c, p.Z, p.Y, p.X);
+    const int z = q - src.z0;
+    if (z < 0 || z >= src.ez || q >= d.z) continue;
+    for (int e = tid; e < S::EH * S::EW; e += NT) {  // a cell stays with one thread for every source
+      const int ly = e / S::EW, lx = e - ly * S::EW;
+      const int j = j0 - 1 + ly, i = i0 - 1 + lx;
+      const int y = j - src.y0, x = i - src.x0;
+      if (j < 0 || i < 0 || j >= d.y || i >= d.x || y < 0 || x < 0 || y >= src.ey || x >= src.ex) continue;
+      float& v = sm.e[slot][c][ly][lx];
+      v = v + src.coeff[(static_cast<int64_t>(z) * src.ey + y) * src.ex + x] * sm.eamp[s];
+    }
+  }
+}
+
 // Adds every h-timing source covering (k, j, i) of H component c (3..5).
 __device__ __forceinline__ float add_h_sources(const Step3D& p, const float* amp, int c, int k, int j, int i,
                                                float h) {
@@ -185,6 +214,7 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
     for (int e = tid; e < 256; e += NT) sm.table[e] = p.em.eps_table[e];
   }
   if (tid < p.n_hsrc) sm.amp[tid] = source_amplitude(p.hsrc[tid], p.step_counter[0] + p.step_offset);
+  if (tid < p.n_esrc) sm.eamp[tid] = source_amplitude(p.esrc[tid], p.step_counter[0] + p.step_offset);
 
   // Prologue: E(kstart) joins the first group; groups m = 0..kDepth-1 carry
   // E(kstart + 1 + m) and H(kstart + m).
@@ -220,6 +250,11 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
     issue_e_plane<TX, TY, Active>(sm, p, k + 1 + kDepth, j0, i0, tid);
     issue_h_plane<TX, TY, Active>(sm, p, k + kDepth, j0, i0, tid);
     cp_async_commit();
+    if (p.n_esrc) {  // pre-E sources on the newly staged E plane(s), before any H reads them
+      if (k == kstart) add_pre_e_sources<TX, TY, Active>(sm, p, k, j0, i0, tid);
+      add_pre_e_sources<TX, TY, Active>(sm, p, k + 1, j0, i0, tid);
+      __syncthreads();
+    }
     if (Mat == FDTD_MATERIAL_VOXEL && emit) vox = load_voxels<TX, TY>(p, k + 1, j0, i0, tid);
 
     const int e0 = k % S::ES, e1 = (k + 1) % S::ES, hs = k % S::HS, hb = k & 1;

@@ -48,6 +48,8 @@ struct Step3D {
   // h-timing sources fused into the step kernel (FDTD_SCHEDULE_FUSED).
   int n_hsrc;
   SourceDev hsrc[kMaxFusedSources];
+  int n_esrc;  // pre-E sources applied inside the 2D fused kernel (else 0)
+  SourceDev esrc[kMaxFusedSources];
   const int* step_counter;
   int step_offset;
   int z_chunk;

@@ -541,6 +541,14 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
   SourceDev hsrc[kMaxFusedSources];
   for (int i = 0; i < p.source_count; ++i)
     if (p.sources[i].timing == FDTD_TIMING_H) hsrc[n_hsrc++] = source_dev(p.sources[i]);
+  // ... and, for 2D programs, the pre-E sources (added to the staged E planes,
+  // so the bank itself is never written before the step).
+  const bool fuse_pre_e = fused && p.layout == FDTD_LAYOUT_DENSE && L.active != kActive3D;
+  int n_esrc = 0;
+  SourceDev esrc[kMaxFusedSources];
+  if (fuse_pre_e)
+    for (int i = 0; i < p.source_count; ++i)
+      if (p.sources[i].timing == FDTD_TIMING_PRE_E) esrc[n_esrc++] = source_dev(p.sources[i]);
   // DFT step batching (validated: batch <= 16, samples sized [batch, M, 6, P]).
   const bool batched = p.dft.monitor_count > 0 && p.dft.batch > 1 && p.dft.samples.data != nullptr;
   float* samples = static_cast<float*>(p.dft.samples.data);
@@ -560,7 +568,7 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     const int bank = fused ? (step & 1) : 0;
     const FdtdBuffer* a = bank == 0 ? p.fields : p.fields_alt;
     const FdtdBuffer* b = fused ? (bank == 0 ? p.fields_alt : p.fields) : a;
-    cudaError_t err = enqueue_sources(s, p, L, a, FDTD_TIMING_PRE_E, step);
+    cudaError_t err = fuse_pre_e ? cudaSuccess : enqueue_sources(s, p, L, a, FDTD_TIMING_PRE_E, step);
     if (err != cudaSuccess) return err;
     Step3D sp = make_step(p, L, bank, fused, step);
     if (ss && step >= 2) {  // step `step` overwrites the bank that sample step-2 reads
@@ -570,6 +578,8 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
     if (fused) {
       sp.n_hsrc = n_hsrc;
       for (int i = 0; i < n_hsrc; ++i) sp.hsrc[i] = hsrc[i];
+      sp.n_esrc = n_esrc;
+      for (int i = 0; i < n_esrc; ++i) sp.esrc[i] = esrc[i];
       if (p.layout == FDTD_LAYOUT_PITCHED) {
         err = launch_fused_tma(s, sp, p.tile_y);
       } else if (L.active == kActive3D) {

@@ -372,9 +372,16 @@ def main():
     ms = replicas.max_over_ranks(start.elapsed_time(end), device=dev)
     cells = spec.cells
     value = replicas.aggregate_rate(cells * args.steps, ms / 1e3, world) / 1e9
-    n_src = len(spec.sources)
-    per_step = n_src + 1 + (1 if spec.monitors else 0)
-    launches = per_step * args.steps + -(-args.steps // R.GRAPH_CHUNK_STEPS)
+    # Our kernels per step: the fused step (H-timing sources inside it, and
+    # 2D pre-E sources too), one launch per other source, the DFT sample; per
+    # batch of up to dft_batch steps within a graph chunk one DFT flush; per
+    # chunk the step-counter advance.
+    separate = sum(1 for s in spec.sources
+                   if s.timing == "e" or (s.timing == "pre_e" and spec.ndim == 3))
+    per_step = 1 + separate + (1 if spec.monitors else 0)
+    chunks = [min(R.GRAPH_CHUNK_STEPS, args.steps - c) for c in range(0, args.steps, R.GRAPH_CHUNK_STEPS)]
+    flushes = sum(-(-n // prog.dft_batch) for n in chunks) if spec.monitors and prog.dft_batch > 1 else 0
+    launches = per_step * args.steps + flushes + len(chunks)
 
     # ---- dominant kernel alone: the fused step without sources or monitors ---
     if args.scene == "3d_512":

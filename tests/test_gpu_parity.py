@@ -379,3 +379,31 @@ def test_dft_step_batching_is_bit_identical(dims):
     for out in outs[1:]:
         for key in ("dft_re", "dft_im", "dft_w"):
             np.testing.assert_array_equal(out[key], outs[0][key], err_msg=key)
+
+
+@pytest.mark.parametrize("pol", ["tm", "te"])
+def test_2d_pre_e_sources_inside_the_fused_step(pol):
+    """2D fused programs add pre-E sources to the staged E planes instead of
+    the bank: overlapping boxes that cross tile edges (8-row, 32-column tiles)
+    give the oracle's fields bit for bit, like the phase schedule."""
+    import dataclasses
+
+    base = scenario_2d(grid=(37, 70), polarization=pol, nsteps=12)
+    rng = np.random.default_rng(8)
+    comp = "Ez" if pol == "tm" else "Ey"
+    extra = [P.SourcePlan(comp, "pre_e", (5, 20), rng.standard_normal((11, 30)).astype(np.float32),
+                          rng.standard_normal(12).astype(np.float32)),
+             P.SourcePlan(comp, "pre_e", (7, 25), rng.standard_normal((9, 14)).astype(np.float32),
+                          rng.standard_normal(12).astype(np.float32))]
+    if pol == "te":
+        extra.append(P.SourcePlan("Ex", "pre_e", (15, 30), rng.standard_normal((2, 5)).astype(np.float32),
+                                  rng.standard_normal(12).astype(np.float32)))
+    spec = dataclasses.replace(base, sources=list(base.sources) + extra)
+    fields = random_initial_fields(spec, seed=3)
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog, fields), oprog, 12)
+    for schedule in ("fused", "phases"):
+        prog = R.compile_program(spec, schedule=schedule)
+        out = R.run_steps(R.initial_state(prog, fields=fields), prog, 12).numpy()
+        for c in P.active_components(2, pol):
+            np.testing.assert_array_equal(out[c], st.fields[c], err_msg=f"{schedule} {c}")
