@@ -219,7 +219,7 @@ struct GatherPackDev {
   const float* w_in = nullptr;
   int* idx_out = nullptr;         // [K, pmax]
   float* w_out = nullptr;
-  int points = 0, slots_in = 0, pmax = 0;
+  int points = 0, slots_in = 0, pmax = 0, rows = 0;  // rows: K of the output
   int dz = 0, dy = 0, dx = 0;     // component extents
   int64_t row = 0, plane = 0;     // device layout strides
 };

@@ -31,8 +31,10 @@ __global__ void __launch_bounds__(kPackThreads) gather_pack_kernel(GatherPackDev
     for (int s = 0; s < g.slots_in; ++s) {
       const float ws = w[s];
       if ((ws != 0.0f) != (pass == 0)) continue;
-      g.idx_out[static_cast<int64_t>(n) * g.pmax + p] = remap_offset(idx[s], g);
-      g.w_out[static_cast<int64_t>(n) * g.pmax + p] = ws;
+      if (n < g.rows) {  // rows past the output's K hold only zero weights (the caller sizes K)
+        g.idx_out[static_cast<int64_t>(n) * g.pmax + p] = remap_offset(idx[s], g);
+        g.w_out[static_cast<int64_t>(n) * g.pmax + p] = ws;
+      }
       ++n;
     }
   }

@@ -1082,7 +1082,7 @@ int fdtd_pack_gather(void* stream, const FdtdGatherPack* g) {
   if (wi.dims[0] != ii.dims[0] || wi.dims[1] != ii.dims[1] || wo.dims[0] != io.dims[0] || wo.dims[1] != io.dims[1])
     return fdtd::kInvalid;
   const int64_t points = ii.dims[0], slots = ii.dims[1], K = io.dims[0], pmax = io.dims[1];
-  if (slots > K || points > pmax || slots > 32 || pmax >= (int64_t{1} << 31)) return fdtd::kInvalid;
+  if (K < 1 || points > pmax || slots > 32 || pmax >= (int64_t{1} << 31)) return fdtd::kInvalid;
   if (g->dims[0] < 1 || g->dims[1] < 1 || g->dims[2] < 1 || g->row < g->dims[2] ||
       g->plane < g->row * static_cast<int64_t>(g->dims[1]) ||
       static_cast<int64_t>(g->dims[0]) * g->plane >= (int64_t{1} << 31))
@@ -1097,6 +1097,7 @@ int fdtd_pack_gather(void* stream, const FdtdGatherPack* g) {
   d.points = static_cast<int>(points);
   d.slots_in = static_cast<int>(slots);
   d.pmax = static_cast<int>(pmax);
+  d.rows = static_cast<int>(K < slots ? K : slots);
   d.dz = g->dims[0];
   d.dy = g->dims[1];
   d.dx = g->dims[2];

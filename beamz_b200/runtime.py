@@ -147,13 +147,10 @@ def pack_dft_monitors(monitors, device, shapes, strides) -> DftArena | None:
         return None
     M = len(monitors)
     P = max(m.points for m in monitors)
-    K = max(max(a.shape[1] for a in m.indices) for m in monitors)
     F = max(len(m.freqs) for m in monitors)
     if F > 64:
         raise ValueError("at most 64 frequencies per monitor")
     torch = _torch()
-    indices = torch.zeros((M, 6, K, P), dtype=torch.int32, device=device)  # neighbour-major (see FdtdDft)
-    weights = torch.zeros((M, 6, K, P), dtype=torch.float32, device=device)
     lib = abi.load_library()
     cur = torch.cuda.current_stream(device)
     stream = ctypes.c_void_p(cur.cuda_stream)
@@ -171,6 +168,16 @@ def pack_dft_monitors(monitors, device, shapes, strides) -> DftArena | None:
         o += a.size
     dev_i = host_i.to(device, non_blocking=True)
     dev_w = host_w.to(device, non_blocking=True)
+    # K = the most nonzero weights any point has: the packed plans keep them
+    # first, so the zero-weight slots past them are dropped.
+    nonzero, o = [], 0
+    for _m, _c, a, _w in plans:
+        if a.size:
+            nonzero.append(torch.count_nonzero(dev_w[o : o + a.size].view(a.shape), dim=1).max())
+        o += a.size
+    K = max(1, int(torch.stack(nonzero).max().item())) if nonzero else 1
+    indices = torch.zeros((M, 6, K, P), dtype=torch.int32, device=device)  # neighbour-major (see FdtdDft)
+    weights = torch.zeros((M, 6, K, P), dtype=torch.float32, device=device)
     o = 0
     for m, c, a, _w in plans:
         g = abi.FdtdGatherPack()

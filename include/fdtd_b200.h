@@ -415,14 +415,16 @@ int fdtd_dft_change(void* stream, const FdtdProgram* program, const FdtdDftChang
 typedef struct FdtdGatherPack {
   FdtdBuffer indices_in;   /* S32 [P, Kc]: dense flat offsets into the component */
   FdtdBuffer weights_in;   /* F32 [P, Kc] */
-  FdtdBuffer indices_out;  /* S32 [K, Pmax] (Kc <= K, P <= Pmax): the program's [M, 6, K, Pmax] slice */
+  FdtdBuffer indices_out;  /* S32 [K, Pmax] (P <= Pmax): the program's [M, 6, K, Pmax] slice */
   FdtdBuffer weights_out;  /* F32 [K, Pmax] */
   int32_t dims[3];         /* the component's stored extents (z, y, x) */
   int64_t row, plane;      /* element strides of the device layout (dense: x, y*x; pitched: P, (Y+1)*P) */
 } FdtdGatherPack;
 
 /* Per point p < P: the slots with a nonzero weight first, then the others,
- * each group in slot order, into rows 0..Kc-1 of column p; each offset
+ * each group in slot order, into rows 0..min(Kc, K)-1 of column p (a K below
+ * Kc drops trailing slots, so it must cover every point's nonzero count; the
+ * runtime sizes K that way); each offset
  * (k, j, i) = unravel(flat, dims) becomes k*plane + j*row + i, an offset
  * outside the component becomes -1 (never gathered).  Rows Kc..K-1 and
  * columns P..Pmax-1 are left as they are (zero in a fresh plan).  No beamz

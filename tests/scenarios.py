@@ -153,7 +153,8 @@ def pack_dft_monitors_host(monitors, shapes, strides):
     """Host restatement of the device gather packing (the engine's earlier host
     path), for equivalence tests: per monitor and component, the (P, K) plan
     remapped to the device layout's offsets and reordered nonzero weights
-    first (stable), laid out neighbour-major [M, 6, K, Pmax]."""
+    first (stable), laid out neighbour-major [M, 6, K, Pmax], K the most
+    nonzero weights any point has."""
     M = len(monitors)
     P = max(m.points for m in monitors)
     K = max(max(np.asarray(a).reshape(m.points, -1).shape[1] for a in m.indices) for m in monitors)
@@ -172,7 +173,9 @@ def pack_dft_monitors_host(monitors, shapes, strides):
             ic, wc = np.take_along_axis(ic, order, axis=1), np.take_along_axis(wc, order, axis=1)
             indices[m, c, : ic.shape[1], :p] = ic.T
             weights[m, c, : wc.shape[1], :p] = wc.T
-    return indices, weights
+    # as the runtime: K shrinks to the most nonzero weights of any point
+    k_eff = max(1, int((weights != 0).sum(axis=2).max()))
+    return indices[:, :, :k_eff], weights[:, :, :k_eff]
 
 
 def with_metrics(spec: P.ProgramSpec, kind="rectilinear", seed=0, spread=(1.0, 1.6)) -> P.ProgramSpec:
