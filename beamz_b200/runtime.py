@@ -237,7 +237,7 @@ class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
     def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
-                 graphs=True, layout="auto", dft_batch: int = 8, dft_overlap: bool = True):
+                 graphs=True, layout="auto", dft_batch: int = 16, dft_overlap: bool = True):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
         torch = _torch()

@@ -78,7 +78,7 @@ def estimate_bytes(spec: ProgramSpec, schedule: str = "fused") -> int:
     dft = 0
     for m in spec.monitors:
         points = max(int(np.asarray(ix).shape[0]) for ix in m.indices)
-        dft += 6 * len(m.freqs) * points * 8 * 2 + 6 * points * 8 * 8 + 8 * 6 * points * 4  # + sample batch
+        dft += 6 * len(m.freqs) * points * 8 * 2 + 6 * points * 8 * 8 + 16 * 6 * points * 4  # + sample batch
     records = 0
     for r in spec.recorders:
         for q, c in enumerate(r.components):

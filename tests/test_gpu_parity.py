@@ -370,7 +370,7 @@ def test_dft_step_batching_is_bit_identical(dims):
             else scenario_2d(grid=(17, 23), polarization="tm", nsteps=37))
     fields = random_initial_fields(spec, seed=2)
     outs = []
-    for batch in (1, 8, 5):
+    for batch in (1, 8, 5, 16):
         prog = R.compile_program(spec, dft_batch=batch)
         st = R.initial_state(prog, fields=fields)
         R.run_steps(st, prog, 20)
