@@ -297,6 +297,37 @@ def adjoint_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def accuracy_report(dev) -> dict:
+    """The engine against the FP32 oracle (the reference's arithmetic) and the
+    FP64 oracle on a reduced copy of the scene (same generator), from seeded
+    random fields so every cell is live: the largest per-component relative L2
+    error of the fields and the DFT arena's."""
+    from beamz_b200 import plan as P
+    from beamz_b200 import runtime as R
+    from beamz_b200 import workloads as W
+    from oracle import fdtd_oracle as O
+    from oracle.from_spec import oracle_program
+
+    steps = 24
+    spec = W.scene_3d_512(total_steps=steps, shape=(32, 64, 64), pml_cells=6)
+    rng = np.random.default_rng(7)
+    fields = {c: rng.standard_normal(P.component_shape(c, spec.grid_shape)).astype(np.float32)
+              * np.float32(1.0 if c[0] == "E" else 1.0 / 376.73) for c in P.COMPONENTS}
+    prog = R.compile_program(spec, device=dev)
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, steps).numpy()
+    report = {"case": f"32x64x64 copy of the scene, CPML 6, {steps} steps from seeded random fields"}
+    for name, dtype in (("fp32", np.float32), ("fp64", np.float64)):
+        oprog = oracle_program(spec, dtype)
+        st = O.new_state(oprog, dtype)
+        for c, v in fields.items():
+            st.fields[c] = v.astype(dtype)
+        st = O.run(st, oprog, steps)
+        report[f"fields_rel_l2_{name}"] = float(max(O.relative_l2(out[c], st.fields[c]) for c in P.COMPONENTS))
+        report[f"dft_rel_l2_{name}"] = float(max(O.relative_l2(out["dft_re"], st.dft_re),
+                                                 O.relative_l2(out["dft_im"], st.dft_im)))
+    return report
+
+
 def main():
     args = parse()
     import torch
@@ -447,6 +478,7 @@ def main():
 
     # ---- CPU baseline (rank 0, one GPU) -------------------------------------
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.scene == "3d_512" and not args.shape:
         from oracle import cpu_port
 
@@ -462,6 +494,7 @@ def main():
         cpu = {"value": round(cspec.cells * 5 / cdt / 1e9, 4), "unit": "Gcell-updates/s", "cores": nthreads,
                "kind": "port",
                "sample": f"5 steps of a {nz}x512x512 z-slab of the scene, C restatement (OpenMP, {nthreads} threads)"}
+        accuracy = accuracy_report(dev)
 
     if rank == 0:
         line = {
@@ -478,6 +511,7 @@ def main():
                          "kernel": "tma_step_kernel" if prog.layout == "pitched" else "fused step", "kernel_ms": round(kernel_ms, 4),
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
             "peak_hbm_gb": round(peak_hbm / 1e9, 2),
+            "accuracy": accuracy,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "e2e": e2e,

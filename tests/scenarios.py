@@ -14,36 +14,9 @@ from oracle import fdtd_oracle as O
 
 
 def to_oracle(spec: P.ProgramSpec, dtype=np.float32) -> O.OracleProgram:
-    shapes = O.component_shapes(spec.grid_shape, spec.polarization)
+    from oracle.from_spec import oracle_program
 
-    def terms(ts):
-        return [O.CpmlTerm(t.component, t.axis, t.sign, t.low, t.high, t.a, t.b, t.inv_kappa,
-                           shapes[t.component][t.axis]) for t in ts]
-
-    sources = [O.SlabSource(s.component, s.timing, tuple(s.start), np.asarray(s.coeff, np.float32),
-                            np.asarray(s.waveform, np.float32)) for s in spec.sources]
-    monitors = [O.DftMonitor(m.freqs, m.indices, m.weights, m.component_mask, m.t_start, m.t_end, m.interval,
-                             m.window_code, m.normalization_code, m.length_unit) for m in spec.monitors]
-    # Arena offsets follow declaration order (beamz/simulation/observe.py:403-410).
-    voff = woff = 0
-    for m in monitors:
-        m.value_offset, m.weight_offset = voff, woff
-        voff += 6 * len(m.freqs) * m.point_count
-        woff += len(m.freqs)
-    prog = O.OracleProgram(tuple(spec.grid_shape), float(spec.dt), float(spec.resolution), terms(spec.h_terms),
-                           terms(spec.e_terms), metallic_edges=frozenset(spec.metallic_edges), sources=sources,
-                           monitors=monitors, polarization=spec.polarization,
-                           metrics=spec.metrics.as_dict() if spec.metrics is not None else None,
-                           recorders=[O.FieldRecorder(r.components, r.interval, r.capacity, r.indices, r.weights,
-                                                      r.signs) for r in spec.recorders])
-    if spec.ndim == 3:
-        eps = np.asarray(spec.eps_table, np.float32)[spec.voxel_ids]
-        prog.material = O.material_from_voxels(eps, dtype=dtype)
-    else:
-        hc = spec.h_coefficients()
-        prog.h_coeffs = hc["Hx" if spec.polarization == "tm" else "Hz"]
-        prog.e_coeffs = {c: (np.asarray(d, dtype), np.asarray(s, dtype)) for c, (d, s) in spec.e_site.items()}
-    return prog
+    return oracle_program(spec, dtype)
 
 
 def _dt3(res, courant=0.99):
