@@ -6,7 +6,7 @@
 One bench "step" is one leapfrog time step of the scene (pre-E source, H, E,
 CPML psi, PEC, DFT monitors).  The default scene is the 512 x 512 x 256
 CPML + Si-box + dipole + 4-plane DFT workload.  Every rank runs its own
-replica (the north star is single-GPU: no sharding, no collectives), so
+replica (the step is single-GPU: no sharding, no collectives), so
 ``value`` = cells x steps x ranks / max-over-ranks device time ("weak").
 
 ``--impl reference`` times the CPU restatement of beamz's float32 step

@@ -1,7 +1,7 @@
 """The 512 x 512 x 256 CPML workload (config 2: Si boxes, Ey dipole, four
 x-normal DFT planes) at full size, through properties that do not need the
 numpy oracle to finish: agreement with the C restatement of the reference
-(1e-5 relative L2 for fields, 1e-4 for the DFT), bitwise
+(accuracy bound: 1e-5 relative L2 for fields, 1e-4 for the DFT), bitwise
 agreement of the pitched TMA kernel with the dense kernel, exact linearity
 under a power-of-two scaling, and run-to-run determinism."""
 

@@ -1,7 +1,7 @@
 """CUDA path (through the C ABI) against the CPU oracle and the golden vectors.
 
 Tolerances: the step is float32 arithmetic in the reference's order of
-operations, so fields are expected to agree to a few ulps
+operations, so fields are expected to agree to a few ulps; the accuracy bar
 is relative L2 <= 1e-5 for fields and <= 1e-4 for DFT accumulators, and both
 are asserted here.
 """
