@@ -49,10 +49,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel-steps", type=int, default=200)
     ap.add_argument("--shape", default=None, help="override the scene grid as ZxYxX (profiling runs)")
-    ap.add_argument("--serving", action="store_true", help="config 4: batched serving vs one-at-a-time")
+    ap.add_argument("--serving", action="store_true", help="the request stream: batched serving vs one-at-a-time")
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
-    ap.add_argument("--adjoint", choices=["2d", "3d"], default=None, help="config 5: forward + adjoint gradient")
+    ap.add_argument("--adjoint", choices=["2d", "3d"], default=None, help="inverse design: forward + adjoint gradient")
     return ap.parse_args()
 
 
@@ -419,7 +419,7 @@ def main():
         kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw)
         kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
         kstate = R.initial_state(kprog)
-    else:  # other scenes time their own step (a second copy would not fit config 3)
+    else:  # other scenes time their own step (a second copy of the 1.6 G-cell scene would not fit)
         kprog, kstate = prog, state
         kprog._times_for(kstate.step + 3 * args.kernel_steps + 3)
     R.run_steps(kstate, kprog, 3)

@@ -1,4 +1,4 @@
-"""The 512 x 512 x 256 CPML workload (config 2: Si boxes, Ey dipole, four
+"""The 512 x 512 x 256 CPML workload (Si boxes, Ey dipole, four
 x-normal DFT planes) at full size, through properties that do not need the
 numpy oracle to finish: agreement with the C restatement of the reference
 (accuracy bound: 1e-5 relative L2 for fields, 1e-4 for the DFT), bitwise
