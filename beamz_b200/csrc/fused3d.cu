@@ -156,13 +156,14 @@ __device__ __forceinline__ void store_vox(typename L::Smem& sm, const VoxRegs<R>
 }
 
 template <bool Metric>
-__device__ __forceinline__ float ghost(const Step3D& p, int axis, int coord, float center, float below, bool at_low,
+__device__ __forceinline__ float ghost(const Step3D& p, float m, float center, float below, bool at_low,
                                        bool at_high, bool low_wall, bool high_wall) {
   // beamz/lattice.py:523-551: zero beyond a metallic wall, else a copy of the
-  // edge sample so that the edge derivative vanishes.
-  if (at_low) return low_wall ? de<Metric>(p, axis, coord, center - 0.0f) : 0.0f;
-  if (at_high) return high_wall ? de<Metric>(p, axis, coord, 0.0f - below) : 0.0f;
-  return de<Metric>(p, axis, coord, center - below);
+  // edge sample so that the edge derivative vanishes.  `m`: the coordinate's
+  // inverse distance (Metric).
+  if (at_low) return low_wall ? dm<Metric>(p, center - 0.0f, m) : 0.0f;
+  if (at_high) return high_wall ? dm<Metric>(p, 0.0f - below, m) : 0.0f;
+  return dm<Metric>(p, center - below, m);
 }
 
 __device__ __forceinline__ float h_sources(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
@@ -235,6 +236,24 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
   // CPML reach of this tile (x/y) -- planes test z separately.
   const bool cpml_xy = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + L::TX < p.cpml_inner[2][1] &&
                                  j0 - 1 >= p.cpml_inner[1][0] && j0 + L::TY < p.cpml_inner[1][1]);
+  // Metric grids: the inverse distances of this thread's columns and rows,
+  // loaded once (the plane's z values once per plane).
+  float mhx = 0.0f, mhx_halo = 0.0f, mhy_halo = 0.0f, mhy_col = 0.0f, mex = 0.0f;
+  float mhy[R], mey[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) mhy[r] = mey[r] = 0.0f;
+  if constexpr (Metric) {
+    mhx = p.metric_h[2][clampi(i, X - 1)];
+    mhx_halo = p.metric_h[2][clampi(i0 - 1, X - 1)];
+    mhy_halo = p.metric_h[1][clampi(j0 - 1, Y - 1)];
+    mhy_col = p.metric_h[1][clampi(j0 + lane, Y - 1)];
+    mex = p.metric_e[2][clampi(i, X)];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      mhy[r] = p.metric_h[1][clampi(j0 + warp * R + r, Y - 1)];
+      mey[r] = p.metric_e[1][clampi(j0 + warp * R + r, Y)];
+    }
+  }
 
   for (int k = kstart; k < k1; ++k) {
     const bool emit = k >= k0;
@@ -249,19 +268,21 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
     const bool zZ = k < Z;  // Ez Hx Hy exist on this plane (Ex Ey Hz always do: k <= Z)
     const bool cpml = Cpml && (cpml_xy || !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]));
     const bool src = p.n_hsrc > 0 && sources_hit(p, k, j0 - 1, j0 + L::TY, i0 - 1, i0 + L::TX);
+    const float mhz = Metric ? p.metric_h[0][clampi(k, Z - 1)] : 0.0f;
+    const float mez = Metric ? p.metric_e[0][clampi(k, Z)] : 0.0f;
 
     // ---- H(k) ----------------------------------------------------------------
     // One H cell at region position (ly, lx) = lattice (k, j, ii); `own` cells
     // are written back, halo cells only feed E.  Which components: bit 0 Hx,
     // 1 Hy, 2 Hz.
-    auto h_cell = [&](int ly, int lx, int j, int ii, bool own, int which) {
+    auto h_cell = [&](int ly, int lx, int j, int ii, bool own, int which, float mx, float my) {
       const bool yY = j >= 0 && j < Y, yY1 = j >= 0 && j <= Y;
       const bool iX = ii >= 0 && ii < X, iX1 = ii >= 0 && ii <= X;
       const float ez = sm.e[e0][2][ly][lx], ey = sm.e[e0][1][ly][lx], ex = sm.e[e0][0][ly][lx];
       if (which & 1) {  // Hx: dEz/dy - dEy/dz
         const bool ok = zZ && yY && iX1;
-        float d0 = dh<Metric>(p, 1, j, sm.e[e0][2][ly + 1][lx] - ez);
-        float d1 = dh<Metric>(p, 0, k, sm.e[e1][1][ly][lx] - ey);
+        float d0 = dm<Metric>(p, sm.e[e0][2][ly + 1][lx] - ez, my);
+        float d1 = dm<Metric>(p, sm.e[e1][1][ly][lx] - ey, mhz);
         if (cpml && ok) {
           d0 = cpml_correct<1>(p.ht[0], d0, k, j, ii, own);
           d1 = cpml_correct<0>(p.ht[1], d1, k, j, ii, own);
@@ -276,8 +297,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 2) {  // Hy: dEx/dz - dEz/dx
         const bool ok = zZ && yY1 && iX;
-        float d0 = dh<Metric>(p, 0, k, sm.e[e1][0][ly][lx] - ex);
-        float d1 = dh<Metric>(p, 2, ii, sm.e[e0][2][ly][lx + 1] - ez);
+        float d0 = dm<Metric>(p, sm.e[e1][0][ly][lx] - ex, mhz);
+        float d1 = dm<Metric>(p, sm.e[e0][2][ly][lx + 1] - ez, mx);
         if (cpml && ok) {
           d0 = cpml_correct<0>(p.ht[2], d0, k, j, ii, own);
           d1 = cpml_correct<2>(p.ht[3], d1, k, j, ii, own);
@@ -292,8 +313,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
       }
       if (which & 4) {  // Hz: dEy/dx - dEx/dy
         const bool ok = yY && iX;
-        float d0 = dh<Metric>(p, 2, ii, sm.e[e0][1][ly][lx + 1] - ey);
-        float d1 = dh<Metric>(p, 1, j, sm.e[e0][0][ly + 1][lx] - ex);
+        float d0 = dm<Metric>(p, sm.e[e0][1][ly][lx + 1] - ey, mx);
+        float d1 = dm<Metric>(p, sm.e[e0][0][ly + 1][lx] - ex, my);
         if (cpml && ok) {
           d0 = cpml_correct<2>(p.ht[4], d0, k, j, ii, own);
           d1 = cpml_correct<1>(p.ht[5], d1, k, j, ii, own);
@@ -310,10 +331,11 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int ly = 1 + warp * R + r;
-      h_cell(ly, 1 + lane, j0 + ly - 1, i, emit, 7);
+      h_cell(ly, 1 + lane, j0 + ly - 1, i, emit, 7, mhx, mhy[r]);
     }
-    if (warp == 0) h_cell(0, 1 + lane, j0 - 1, i, false, 1 | 4);                   // y halo row: Hx, Hz
-    if (warp == 1 && lane < L::TY) h_cell(1 + lane, 0, j0 + lane, i0 - 1, false, 2 | 4);  // x halo column: Hy, Hz
+    if (warp == 0) h_cell(0, 1 + lane, j0 - 1, i, false, 1 | 4, mhx, mhy_halo);  // y halo row: Hx, Hz
+    if (warp == 1 && lane < L::TY)
+      h_cell(1 + lane, 0, j0 + lane, i0 - 1, false, 2 | 4, mhx_halo, mhy_col);  // x halo column: Hy, Hz
     __syncthreads();
 
     // ---- E(k) ----------------------------------------------------------------
@@ -329,8 +351,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         const float hx = sm.hn[hb][0][ly][lx], hy = sm.hn[hb][1][ly][lx], hz = sm.hn[hb][2][ly][lx];
         // Ex: dHz/dy - dHy/dz
         if (yY1 && xX) {
-          float d0 = ghost<Metric>(p, 1, j, hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1);
-          float d1 = ghost<Metric>(p, 0, k, hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1);
+          float d0 = ghost<Metric>(p, mey[r], hz, sm.hn[hb][2][ly - 1][lx], ylo, yhi, wy0, wy1);
+          float d1 = ghost<Metric>(p, mez, hy, sm.hn[pb][1][ly][lx], zlo, zhiZ, wz0, wz1);
           if (cpml) {
             d0 = cpml_correct<1>(p.et[0], d0, k, j, i, true);
             d1 = cpml_correct<0>(p.et[1], d1, k, j, i, true);
@@ -349,8 +371,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ey: dHx/dz - dHz/dx
         if (yY && xX1) {
-          float d0 = ghost<Metric>(p, 0, k, hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1);
-          float d1 = ghost<Metric>(p, 2, i, hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1);
+          float d0 = ghost<Metric>(p, mez, hx, sm.hn[pb][0][ly][lx], zlo, zhiZ, wz0, wz1);
+          float d1 = ghost<Metric>(p, mex, hz, sm.hn[hb][2][ly][lx - 1], xlo, xhi, wx0, wx1);
           if (cpml) {
             d0 = cpml_correct<0>(p.et[2], d0, k, j, i, true);
             d1 = cpml_correct<2>(p.et[3], d1, k, j, i, true);
@@ -369,8 +391,8 @@ __global__ void __launch_bounds__(32 * NW) lean_step_kernel(Step3D p) {
         }
         // Ez: dHy/dx - dHx/dy
         if (zZ && yY1 && xX1) {
-          float d0 = ghost<Metric>(p, 2, i, hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1);
-          float d1 = ghost<Metric>(p, 1, j, hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1);
+          float d0 = ghost<Metric>(p, mex, hy, sm.hn[hb][1][ly][lx - 1], xlo, xhi, wx0, wx1);
+          float d1 = ghost<Metric>(p, mey[r], hx, sm.hn[hb][0][ly - 1][lx], ylo, yhi, wy0, wy1);
           if (cpml) {
             d0 = cpml_correct<2>(p.et[4], d0, k, j, i, true);
             d1 = cpml_correct<1>(p.et[5], d1, k, j, i, true);

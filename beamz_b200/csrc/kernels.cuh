@@ -44,6 +44,14 @@ __device__ __forceinline__ float dh(const Step3D& p, int axis, int c, float diff
   return div_rn(diff, p.div_bs, p.div_rs);
 }
 
+// dh / de with the coordinate's inverse distance already loaded (kernels that
+// hoist the metric out of their loops), or divided by the cell size.
+template <bool Metric>
+__device__ __forceinline__ float dm(const Step3D& p, float diff, float m) {
+  if constexpr (Metric) return diff * m;
+  return div_rn(diff, p.div_bs, p.div_rs);
+}
+
 // A backward difference of H along `axis` at E coordinate `c` (0..n_axis).
 template <bool Metric>
 __device__ __forceinline__ float de(const Step3D& p, int axis, int c, float diff) {
