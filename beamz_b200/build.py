@@ -7,7 +7,8 @@ with PyTorch, so torch-allocated pointers and torch streams are valid in it.
 
 ``-fmad=false`` keeps every product and sum separately rounded, in source
 order, which is the rounding contract the kernels rely on for parity with
-beamz's float32 path; explicit ``fmaf`` calls still emit FFMA.
+beamz's float32 path; explicit ``fmaf`` calls (the opt-in tolerance arithmetic
+of the class step) still emit FFMA.
 """
 
 from __future__ import annotations
@@ -20,7 +21,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_fdtd_b200.so")
-SOURCES = ("phase.cu", "fused.cu", "fused3d.cu", "fused_tma.cu", "io.cu", "adjoint.cu", "diag.cu", "planner.cu", "analysis.cu", "recorder.cu", "program.cu")
+SOURCES = ("phase.cu", "fused.cu", "fused3d.cu", "fused_tma.cu", "fast_tma.cu", "io.cu", "adjoint.cu", "diag.cu", "planner.cu", "analysis.cu", "recorder.cu", "program.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

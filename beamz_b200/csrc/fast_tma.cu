@@ -1,0 +1,871 @@
+// Tolerance-mode 3D leapfrog step on the pitched field layout (FDTD_FLAG_CLASSES).
+//
+// Same schedule as the bit-exact kernel in fused_tma.cu (one launch per step,
+// z-marching CTAs, TMA-staged planes on an mbarrier ring, recomputed H halo),
+// re-shaped so that a thread does four cells per plane instead of one:
+//
+//  * a CTA of NW warps owns a 128 x NW tile of (x, y) lattice points; lane l of
+//    warp w owns x = i0 + 4l .. 4l + 3 on row j = j0 + w, so every shared and
+//    global access of a cell group is one 16-byte vector;
+//  * x neighbours come from the adjacent lane by shuffle (the tile edges from
+//    the staged box); the y neighbour of the H update is the next staged row,
+//    that of the E update the row above in the new-H plane; H of the previous
+//    plane stays in registers;
+//  * every spatial difference is left unscaled: 1/dx is folded into the update
+//    coefficients (dt/(mu0 dx) for H, dt/(eps0 eps dx) per material class for
+//    E) and into the CPML 'a' coefficient, and products are contracted into
+//    FMAs.  Relative to beamz's float32 path (divide each difference by dx,
+//    then scale) this rounds differently within a few ulp per step; parity is
+//    a tolerance (fields 1e-5 relative L2 after the run), not bit equality;
+//  * the electric material is one uint8 class id per lattice point (the class
+//    being the (Ex, Ey, Ez) coefficient triple), 1 byte per cell instead of a
+//    4-byte codebook word, with the class table in shared memory.
+//
+// Tile-planes that touch a high domain face, a z face, an H source or a
+// partial tile run a general per-cell path with every validity, ghost and PEC
+// rule; the rest run one of six straight bodies chosen by the absorber axes
+// they touch (as the exact kernel).  ψ of the CPML terms is read and written
+// with plain loads; the H-term memories are double-banked (the halo
+// recomputation reads them), the E-term ones updated in place.
+//
+// Operation order otherwise follows beamz/simulation/kernels.py:458-626 (H
+// from E with CPML, H sources, H PEC; E from ghost-padded H with CPML, E PEC)
+// and beamz/simulation/execute.py:467-522.
+
+#include <cuda.h>
+
+#include <type_traits>
+
+#include "kernels.cuh"
+#include "tma_util.cuh"
+
+namespace fdtd {
+
+namespace {
+
+constexpr int kSlots = 32;  // CPML coefficient slots staged per term
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int NW>
+struct FastTile {
+  static constexpr int TX = 128, TY = NW, NT = 32 * NW;
+  static constexpr int BX = TX + 8;  // staged row: x from i0-4 to i0+131 (16-byte aligned start)
+  static constexpr int EH = TY + 2;  // E rows j0-1 .. j0+TY
+  static constexpr int HH = TY + 1;  // H rows j0-1 .. j0+TY-1
+  static constexpr int EBOX = ((EH * BX + 31) / 32) * 32;  // floats; every box starts on 128 B
+  static constexpr int HBOX = ((HH * BX + 31) / 32) * 32;
+  static constexpr int IBOX = TY * TX;  // class ids (bytes), rows j0 .. j0+TY-1, x i0 .. i0+127
+  static constexpr int XC = 4 + TX;     // box column of x = i0 + 128 (column X of the last tile)
+  struct Smem {
+    alignas(128) float e[3][3][EBOX];  // E ring: plane slot, component (TMA boxes start on 128 B)
+    alignas(128) float h[2][3][HBOX];  // H (old) ring
+    alignas(128) uint8_t ids[2][IBOX];
+    alignas(16) float hn[3][HH][BX];   // H (new) of this plane: own rows + halo row, own columns + halo column
+    float4 cls[256];                   // per class: dt/(eps0 eps dx) of Ex, Ey, Ez
+    float4 cc[12][kSlots];  // CPML (a/dx, b, 1/kappa): H terms 0-5, E terms 6-11
+    float amp[kMaxFusedSources];
+    unsigned long long bar[2];
+  };
+};
+
+struct FastMaps {
+  CUtensorMap e[3];
+  CUtensorMap h[3];
+  CUtensorMap ids;
+};
+
+// ---- float4 helpers ----------------------------------------------------------
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 sub4(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+// (v.y, v.z, v.w, n): the x+1 neighbours of a lane's four cells.
+__device__ __forceinline__ float4 next4(float4 v, float n) { return make_float4(v.y, v.z, v.w, n); }
+// (p, v.x, v.y, v.z): the x-1 neighbours.
+__device__ __forceinline__ float4 prev4(float p, float4 v) { return make_float4(p, v.x, v.y, v.z); }
+__device__ __forceinline__ float get(const float4& v, int q) { return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w)); }
+__device__ __forceinline__ void put(float4& v, int q, float s) {
+  if (q == 0) v.x = s;
+  else if (q == 1) v.y = s;
+  else if (q == 2) v.z = s;
+  else v.w = s;
+}
+
+// ---- arithmetic ------------------------------------------------------------
+// Exact: beamz's float32 order (kernels.py:458-626): every difference divided
+// by the cell size (correctly rounded, div_rn), every product and sum rounded
+// separately (this file is compiled with -fmad=false).  Otherwise the
+// tolerance form: differences left unscaled (1/dx folded into the
+// coefficients) and explicit fused multiply-adds.
+template <bool Exact>
+__device__ __forceinline__ float dv(float diff, float bs, float rs) {
+  if constexpr (Exact) return div_rn(diff, bs, rs);
+  return diff;
+}
+
+template <bool Exact>
+__device__ __forceinline__ float4 dv4(float4 d, float bs, float rs) {
+  return make_float4(dv<Exact>(d.x, bs, rs), dv<Exact>(d.y, bs, rs), dv<Exact>(d.z, bs, rs), dv<Exact>(d.w, bs, rs));
+}
+
+// H <- dec H - s (d0 - d1).
+template <bool Exact>
+__device__ __forceinline__ float h1(float h, float dec, float s, float d0, float d1) {
+  if constexpr (Exact) return dec * h - s * (d0 - d1);
+  return fmaf(-s, d0 - d1, dec * h);
+}
+
+template <bool Exact>
+__device__ __forceinline__ float4 h4(float4 h, float dec, float s, float4 d0, float4 d1) {
+  return make_float4(h1<Exact>(h.x, dec, s, d0.x, d1.x), h1<Exact>(h.y, dec, s, d0.y, d1.y),
+                     h1<Exact>(h.z, dec, s, d0.z, d1.z), h1<Exact>(h.w, dec, s, d0.w, d1.w));
+}
+
+// E <- E + c (d0 - d1).
+template <bool Exact>
+__device__ __forceinline__ float e_upd(float e, float c, float d0, float d1) {
+  if constexpr (Exact) return e + c * (d0 - d1);
+  return fmaf(c, d0 - d1, e);
+}
+
+// ---- CPML --------------------------------------------------------------------
+// psi <- b psi + a d and the corrected derivative d' = d / kappa + psi
+// (beamz/simulation/kernels.py:257-264), c = (a, b, 1/kappa).  In the
+// tolerance form d is the raw difference D = d dx, `a` is staged as a/dx and
+// the result is scaled by dx (D' = D/kappa + dx psi), so the update's
+// coefficient over dx applies to D' as to a plain difference.
+template <bool Exact>
+__device__ __forceinline__ float cpml_d(float4 c, float res, float psi_old, float d, float* psi_new) {
+  if constexpr (Exact) {
+    const float psi = c.y * psi_old + c.x * d;
+    *psi_new = psi;
+    return d * c.z + psi;
+  }
+  const float psi = fmaf(c.y, psi_old, c.x * d);
+  *psi_new = psi;
+  return fmaf(c.z, d, res * psi);
+}
+
+// Packed slab coordinate, -1 outside (fdtd_common.cuh's cpml_slot).
+__device__ __forceinline__ int slot_of(const CpmlTermDev& t, int coord) { return cpml_slot(t, coord); }
+
+// Offset of (k, j, i) in a term's packed slab, with the term axis coordinate
+// replaced by `slot`.
+template <int Axis>
+__device__ __forceinline__ int psi_off(const CpmlTermDev& t, int slot, int k, int j, int i) {
+  const int pk = Axis == 0 ? slot : k;
+  const int pj = Axis == 1 ? slot : j;
+  const int pi = Axis == 2 ? slot : i;
+  return (pk * t.pdy + pj) * t.pdx + pi;  // slabs hold < 2^31 elements (validated)
+}
+
+// A term whose slot is uniform over a lane's four cells (y terms on a row, z
+// terms on a plane): psi of the four cells is fetched ahead of its use (the
+// offset is recomputed when applying, to keep registers free).
+template <int Axis>
+__device__ __forceinline__ float4 psi4_fetch(const CpmlTermDev& t, int slot, int k, int j, int i) {
+  if (slot < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+  const float* s = t.psi_in + psi_off<Axis>(t, slot, k, j, i);
+  return make_float4(s[0], s[1], s[2], s[3]);
+}
+
+template <bool Exact, int Axis>
+__device__ __forceinline__ float4 psi4_apply(const CpmlTermDev& t, const float4* cc, int slot, float4 v, int k, int j,
+                                             int i, float res, float4 d, bool write) {
+  if (slot < 0) return d;
+  const float4 c = cc[slot];
+  float4 n;
+  float4 r;
+  r.x = cpml_d<Exact>(c, res, v.x, d.x, &n.x);
+  r.y = cpml_d<Exact>(c, res, v.y, d.y, &n.y);
+  r.z = cpml_d<Exact>(c, res, v.z, d.z, &n.z);
+  r.w = cpml_d<Exact>(c, res, v.w, d.w, &n.w);
+  if (write) {
+    float* o = t.psi_out + psi_off<Axis>(t, slot, k, j, i);
+    o[0] = n.x;
+    o[1] = n.y;
+    o[2] = n.z;
+    o[3] = n.w;
+  }
+  return r;
+}
+
+// An x term: the slot differs per cell.
+__device__ __forceinline__ float4 psix_fetch(const CpmlTermDev& t, int k, int j, int i) {
+  float v[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int slot = slot_of(t, i + c);
+    v[c] = slot >= 0 ? t.psi_in[psi_off<2>(t, slot, k, j, i + c)] : 0.0f;
+  }
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+template <bool Exact>
+__device__ __forceinline__ float4 psix_apply(const CpmlTermDev& t, const float4* cc, float4 v, int k, int j, int i,
+                                             float res, float4 d, bool write) {
+  float r[4] = {d.x, d.y, d.z, d.w};
+  const float pv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int slot = slot_of(t, i + c);
+    if (slot < 0) continue;
+    float n;
+    r[c] = cpml_d<Exact>(cc[slot], res, pv[c], r[c], &n);
+    if (write) t.psi_out[psi_off<2>(t, slot, k, j, i + c)] = n;
+  }
+  return make_float4(r[0], r[1], r[2], r[3]);
+}
+
+// One scalar cell of a term: psi fetched ahead (0 outside the slab), then applied.
+template <int Axis>
+__device__ __forceinline__ float psi1_fetch(const CpmlTermDev& t, int k, int j, int i) {
+  const int slot = slot_of(t, Axis == 0 ? k : (Axis == 1 ? j : i));
+  return slot >= 0 ? t.psi_in[psi_off<Axis>(t, slot, k, j, i)] : 0.0f;
+}
+
+template <bool Exact, int Axis>
+__device__ __forceinline__ float psi1_apply(const CpmlTermDev& t, const float4* cc, float v, int k, int j, int i,
+                                            float res, float d, bool write) {
+  const int slot = slot_of(t, Axis == 0 ? k : (Axis == 1 ? j : i));
+  if (slot < 0) return d;
+  float n;
+  const float r = cpml_d<Exact>(cc[slot], res, v, d, &n);
+  if (write) t.psi_out[psi_off<Axis>(t, slot, k, j, i)] = n;
+  return r;
+}
+
+// One scalar cell of a term fetched and applied at once (general path).
+template <bool Exact, int Axis>
+__device__ __forceinline__ float cpml1(const CpmlTermDev& t, const float4* cc, bool cc_smem, float res, int k, int j,
+                                       int i, float d, bool write) {
+  const int coord = Axis == 0 ? k : (Axis == 1 ? j : i);
+  const int slot = slot_of(t, coord);
+  if (slot < 0) return d;
+  const int off = psi_off<Axis>(t, slot, k, j, i);
+  const float a = Exact ? __ldg(t.a + slot) : __ldg(t.a + slot) * (1.0f / res);
+  const float4 c = cc_smem ? cc[slot] : make_float4(a, __ldg(t.b + slot), __ldg(t.k + slot), 0.0f);
+  float n;
+  const float r = cpml_d<Exact>(c, res, t.psi_in[off], d, &n);
+  if (write) t.psi_out[off] = n;
+  return r;
+}
+
+__device__ __forceinline__ void l2_prefetch(const void* ptr) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(ptr));
+}
+
+// L2 prefetch of the psi a term needs at (k, j, i..i+3), if any cell is in its slab.
+template <int Axis>
+__device__ __forceinline__ void psi_prefetch(const CpmlTermDev& t, int k, int j, int i) {
+  if (t.psi_in == nullptr) return;
+  if (Axis == 2) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int slot = slot_of(t, i + c);
+      if (slot >= 0) {
+        l2_prefetch(t.psi_in + psi_off<2>(t, slot, k, j, i + c));
+        return;
+      }
+    }
+    return;
+  }
+  const int slot = slot_of(t, Axis == 0 ? k : j);
+  if (slot >= 0) l2_prefetch(t.psi_in + psi_off<Axis>(t, slot, k, j, i));
+}
+
+__device__ __forceinline__ float h_sources_at(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
+  for (int s = 0; s < p.n_hsrc; ++s) {
+    const SourceDev& src = p.hsrc[s];
+    const int z = k - src.z0, y = j - src.y0, x = i - src.x0;
+    if (src.component != c || z < 0 || y < 0 || x < 0 || z >= src.ez || y >= src.ey || x >= src.ex) continue;
+    h = h + src.coeff[(static_cast<int64_t>(z) * src.ey + y) * src.ex + x] * amp[s];
+  }
+  return h;
+}
+
+__device__ __forceinline__ bool sources_touch(const Step3D& p, int k, int jlo, int jhi, int ilo, int ihi) {
+  for (int s = 0; s < p.n_hsrc; ++s) {
+    const SourceDev& src = p.hsrc[s];
+    if (k >= src.z0 && k < src.z0 + src.ez && jhi >= src.y0 && jlo < src.y0 + src.ey && ihi >= src.x0 &&
+        ilo < src.x0 + src.ex)
+      return true;
+  }
+  return false;
+}
+
+// Ghost-padded backward difference along one axis at E coordinate v of an
+// axis with n H samples (beamz/lattice.py:523-551): beyond a metallic wall the
+// ghost is zero, else a copy of the edge sample (the difference vanishes).
+__device__ __forceinline__ float ghost_diff(float center, float below, int v, int n, bool low_wall, bool high_wall) {
+  if (v == 0) return low_wall ? center : 0.0f;
+  if (v == n) return high_wall ? 0.0f - below : 0.0f;
+  return center - below;
+}
+
+// 8-warp CTAs: two per SM (shared memory), 128 registers; 4-warp CTAs: four.
+template <int NW, bool Cpml, bool Exact>
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
+    fast_step_kernel(const __grid_constant__ FastMaps maps, const __grid_constant__ Step3D p) {
+  using T = FastTile<NW>;
+  using S = typename T::Smem;
+  constexpr int BX = T::BX, TX = T::TX, TY = T::TY, XC = T::XC;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  S& sm = *reinterpret_cast<S*>(smem_raw);
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int tid = warp * 32 + lane;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int Z = p.Z, Y = p.Y, X = p.X;
+  const int k0 = blockIdx.z * p.z_chunk;
+  const int k1 = min(k0 + p.z_chunk, Z + 1);
+  const int kstart = k0 > 0 ? k0 - 1 : 0;
+  const int P = p.pitch, PL = (Y + 1) * p.pitch;
+  const float res = p.res, inv_res = p.inv_res;
+  const unsigned long long wait_ns = p.wait_ns;
+
+  // Bundle q: E(q+1) (and E(q) when `first`), H(q), class ids(q).  x starts at
+  // i0 - 4 (fields) or i0 (ids), i0 a multiple of 128: 16-byte aligned.
+  auto issue = [&](int q, int slot, bool first) {
+    const int ne = (first ? 1 : 0) + (q + 1 <= Z ? 1 : 0);
+    const unsigned bytes = ne * 3 * T::EH * BX * 4 + 3 * T::HH * BX * 4 + T::IBOX;
+    unsigned long long* b = &sm.bar[slot];
+    tma::bar_expect(b, bytes);
+    if (p.test_stall) return;  // test-only: the barrier is armed, no copy is issued, nothing is in flight
+    if (first)
+      for (int c = 0; c < 3; ++c) tma::load_3d(sm.e[q % 3][c], &maps.e[c], i0 - 4, j0 - 1, q, b);
+    if (q + 1 <= Z)
+      for (int c = 0; c < 3; ++c) tma::load_3d(sm.e[(q + 1) % 3][c], &maps.e[c], i0 - 4, j0 - 1, q + 1, b);
+    for (int c = 0; c < 3; ++c) tma::load_3d(sm.h[q % 2][c], &maps.h[c], i0 - 4, j0 - 1, q, b);
+    tma::load_3d(sm.ids[q % 2], &maps.ids, i0, j0, q, b);
+  };
+
+  if (tid == 0) {
+    tma::bar_init(&sm.bar[0], 1);
+    tma::bar_init(&sm.bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    issue(kstart, 0, true);
+  }
+  for (int e = tid; e < 256; e += T::NT) sm.cls[e] = p.class_coef[e];
+  bool cc_smem = true;
+  if (Cpml) {
+#pragma unroll
+    for (int t = 0; t < 12; ++t) {
+      const CpmlTermDev& d = t < 6 ? p.ht[t] : p.et[t - 6];
+      const int w = d.low + d.high;
+      cc_smem = cc_smem && w <= kSlots;
+      for (int e = tid; e < w && e < kSlots; e += T::NT)
+        sm.cc[t][e] = make_float4(Exact ? d.a[e] : d.a[e] * inv_res, d.b[e], d.k[e], 0.0f);
+    }
+  }
+  if (tid < p.n_hsrc) sm.amp[tid] = source_amplitude(p.hsrc[tid], p.step_counter[0] + p.step_offset);
+  __syncthreads();
+
+  const bool wz0 = wall(p.metallic, 0, false), wz1 = wall(p.metallic, 0, true);
+  const bool wy0 = wall(p.metallic, 1, false), wy1 = wall(p.metallic, 1, true);
+  const bool wx0 = wall(p.metallic, 2, false), wx1 = wall(p.metallic, 2, true);
+  // Uniform H coefficients (the pitched layout carries no per-site H).
+  const float dec0 = p.hm.decay[0][0], dec1 = p.hm.decay[1][0], dec2 = p.hm.decay[2][0];
+  // The tolerance form folds 1/dx into the H coefficient (the class table carries E's).
+  const float hsc = Exact ? 1.0f : inv_res;
+  const float s0 = p.hm.source[0][0] * hsc, s1 = p.hm.source[1][0] * hsc, s2 = p.hm.source[2][0] * hsc;
+  const float dbs = p.div_bs, drs = p.div_rs;  // div_rn's scaled cell size and reciprocal
+  auto D1 = [&](float v) { return dv<Exact>(v, dbs, drs); };
+  auto D4 = [&](float4 v) { return dv4<Exact>(v, dbs, drs); };
+
+  const int r = 1 + warp;              // own row in the staged boxes and hn
+  const int j = j0 + warp;             // its lattice row
+  const int c0 = 4 + 4 * lane;         // own first column in the boxes and hn
+  const int i = i0 + 4 * lane;         // its lattice x
+  const int rc = r * BX + c0;
+  // When X is a multiple of 128 the last tile also owns column X (Hx, Ey, Ez
+  // there), done by lane 31, so no CTA is spent on one column.
+  const bool xcol = X % TX == 0 && i0 + TX == X;
+  const bool xl = xcol && lane == 31;
+  const int xe = xcol ? 1 : 0;
+  const bool fast_ok = j0 + TY <= Y && i0 + TX <= X && cc_smem;
+  const bool xface = i0 == 0, yface = j0 == 0;
+  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
+  const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
+
+  // H of the previous plane on the own cells (the z-backward differences of E).
+  float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
+  float hxXp = 0.0f;
+
+  int e0 = kstart % 3, e1 = (kstart + 1) % 3, hs = kstart & 1;
+  for (int k = kstart; k < k1; ++k) {
+    const int n = k - kstart;
+    const bool emit = k >= k0;
+    const bool arrived = tma::bar_wait(&sm.bar[n & 1], (n >> 1) & 1, wait_ns);
+    if (__syncthreads_or(!arrived)) {  // CTA-uniform: every thread leaves together
+      if (tid == 0) {
+        if (p.status) atomicExch(p.status, 1);
+        if (!p.test_stall) tma::bar_wait(&sm.bar[n & 1], (n >> 1) & 1, wait_ns);  // the bundle in flight
+      }
+      __syncthreads();
+      return;
+    }
+    if (tid == 0 && k + 1 < k1) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      issue(k + 1, (n + 1) & 1, false);
+    }
+    const float* E0x = sm.e[e0][0];
+    const float* E0y = sm.e[e0][1];
+    const float* E0z = sm.e[e0][2];
+    const float* E1x = sm.e[e1][0];
+    const float* E1y = sm.e[e1][1];
+    const float* HOx = sm.h[hs][0];
+    const float* HOy = sm.h[hs][1];
+    const float* HOz = sm.h[hs][2];
+    const uint8_t* IDS = sm.ids[hs];
+    const bool src = p.n_hsrc > 0 && sources_touch(p, k, j0 - 1, j0 + TY, i0 - 1, i0 + TX);
+
+    if (fast_ok && !src && k >= 1 && k < Z) {
+      // ---- straight tile-plane: every own and halo cell valid ----------------
+      auto body = [&](auto axc, auto ayc, auto azc, auto fc) {
+        constexpr bool AX = decltype(axc)::value, AY = decltype(ayc)::value, AZ = decltype(azc)::value;
+        constexpr bool FC = decltype(fc)::value;  // the tile may touch x = 0 / y = 0
+        const bool at_x0 = FC && xface, at_y0 = FC && yface;
+        const int jh = j0 - 1, ih = i0 - 1;  // the halo row and column
+        // Which warps recompute a halo this plane (never on a pre-plane).
+        const bool halo_row_x = emit && warp == 0 && !at_y0;              // Hx on row j0-1
+        const bool halo_row_z = emit && warp == 1 && !at_y0;              // Hz on row j0-1
+        const bool halo_col = emit && warp == 2 && lane < TY && !at_x0;   // Hy, Hz on column i0-1
+        const int jc = j0 + lane;                                         // halo_col's row
+        // ---- every global load of the plane goes out first ----
+        // Class id of column X (lane 31 of the last tile).
+        const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
+        // psi of the H terms: own cells, halos, column X.
+        float4 qh0, qh1, qh2, qh3, qh4, qh5, qa, qb;
+        float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f, qX0 = 0.f, qX1 = 0.f, qR0 = 0.f, qR1 = 0.f;
+        if constexpr (AY) {
+          qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
+          qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
+        }
+        if constexpr (AZ) {
+          qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
+          qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
+        }
+        if constexpr (AX) {
+          qh3 = psix_fetch(p.ht[3], k, j, i);
+          qh4 = psix_fetch(p.ht[4], k, j, i);
+        }
+        if constexpr (AX || AY || AZ) {
+          if (halo_row_x) {
+            if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
+            if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
+            if (xl) {
+              if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
+              if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
+            }
+          } else if (halo_row_z) {
+            if constexpr (AX) qa = psix_fetch(p.ht[4], k, jh, i);
+            if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
+          } else if (halo_col) {
+            if constexpr (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
+            if constexpr (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
+            if constexpr (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
+            if constexpr (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
+          }
+          if (xl) {
+            if constexpr (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
+            if constexpr (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
+          }
+        }
+        // Next plane's psi (and column X's class id) into L2, a plane ahead of use.
+        if (k + 1 < k1) {
+          const int kn = k + 1;
+          if (xl) l2_prefetch(p.site_class + (kn * (Y + 1) + j) * p.pitch8 + X);
+          if constexpr (Cpml) {
+            psi_prefetch<0>(p.ht[1], kn, j, i);
+            psi_prefetch<0>(p.ht[2], kn, j, i);
+            psi_prefetch<0>(p.et[1], kn, j, i);
+            psi_prefetch<0>(p.et[2], kn, j, i);
+            if constexpr (AY) {
+              psi_prefetch<1>(p.ht[0], kn, j, i);
+              psi_prefetch<1>(p.ht[5], kn, j, i);
+              psi_prefetch<1>(p.et[0], kn, j, i);
+              psi_prefetch<1>(p.et[5], kn, j, i);
+            }
+            if constexpr (AX) {
+              psi_prefetch<2>(p.ht[3], kn, j, i);
+              psi_prefetch<2>(p.ht[4], kn, j, i);
+              psi_prefetch<2>(p.et[3], kn, j, i);
+              psi_prefetch<2>(p.et[4], kn, j, i);
+            }
+          }
+        }
+        // ---- H on the own row ----
+        const float4 ez = ld4(E0z + rc), ezy = ld4(E0z + rc + BX);
+        const float4 ey = ld4(E0y + rc), eyz = ld4(E1y + rc);
+        const float4 ex = ld4(E0x + rc), exz = ld4(E1x + rc), exy = ld4(E0x + rc + BX);
+        float ez4 = __shfl_down_sync(kFull, ez.x, 1), ey4 = __shfl_down_sync(kFull, ey.x, 1);
+        if (lane == 31) {
+          ez4 = E0z[rc + 4];
+          ey4 = E0y[rc + 4];
+        }
+        float4 dx0 = D4(sub4(ezy, ez)), dx1 = D4(sub4(eyz, ey));              // Hx: dEz/dy, dEy/dz
+        float4 dy0 = D4(sub4(exz, ex)), dy1 = D4(sub4(next4(ez, ez4), ez));   // Hy: dEx/dz, dEz/dx
+        float4 dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(exy, ex));   // Hz: dEy/dx, dEx/dy
+        if constexpr (AY) {
+          dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit);
+          dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit);
+        }
+        if constexpr (AZ) {
+          dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit);
+          dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
+        }
+        if constexpr (AX) {
+          dy1 = psix_apply<Exact>(p.ht[3], sm.cc[3], qh3, k, j, i, res, dy1, emit);
+          dz0 = psix_apply<Exact>(p.ht[4], sm.cc[4], qh4, k, j, i, res, dz0, emit);
+        }
+        float4 hx = h4<Exact>(ld4(HOx + rc), dec0, s0, dx0, dx1);
+        float4 hy = h4<Exact>(ld4(HOy + rc), dec1, s1, dy0, dy1);
+        const float4 hz = h4<Exact>(ld4(HOz + rc), dec2, s2, dz0, dz1);
+        if (at_x0 && lane == 0 && wx0) hx.x = 0.0f;  // PEC: normal H on the x = 0 wall
+        if (at_y0 && warp == 0 && wy0) hy = make_float4(0.f, 0.f, 0.f, 0.f);
+        st4(&sm.hn[0][r][c0], hx);
+        st4(&sm.hn[1][r][c0], hy);
+        st4(&sm.hn[2][r][c0], hz);
+        const int o = k * PL + j * P + i;
+        if (emit) {
+          st4(p.hout[0] + o, hx);
+          st4(p.hout[1] + o, hy);
+          st4(p.hout[2] + o, hz);
+        }
+        // Hx on column X (lane 31 of the last tile).
+        float hxX = 0.0f;
+        if (xl) {
+          const int b = rc + 4;
+          float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
+          if constexpr (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit);
+          if constexpr (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit);
+          hxX = wx1 ? 0.0f : h1<Exact>(HOx[b], dec0, s0, d0, d1);
+          sm.hn[0][r][XC] = hxX;
+          if (emit) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
+        }
+        // psi of the E terms, in flight during the halo and the barrier.
+        float4 qe0, qe1, qe2, qe3, qe4, qe5;
+        float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
+        if (emit) {
+          if constexpr (AY) {
+            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
+            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
+          }
+          if constexpr (AZ) {
+            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
+            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
+          }
+          if constexpr (AX) {
+            qe3 = psix_fetch(p.et[3], k, j, i);
+            qe4 = psix_fetch(p.et[4], k, j, i);
+          }
+          if (xl) {
+            if constexpr (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
+            if constexpr (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
+            if constexpr (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
+            if constexpr (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
+          }
+        }
+        // ---- recomputed halo: row j0-1 (Hx by warp 0, Hz by warp 1) and
+        //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
+        if (halo_row_x) {
+          const int b = c0;
+          float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
+          if constexpr (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
+          if constexpr (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
+          float4 h = h4<Exact>(ld4(HOx + b), dec0, s0, d0, d1);
+          if (at_x0 && lane == 0 && wx0) h.x = 0.0f;
+          st4(&sm.hn[0][0][b], h);
+          if (xl) {
+            const int bb = XC;
+            float e0v = D1(E0z[bb + BX] - E0z[bb]), e1v = D1(E1y[bb] - E0y[bb]);
+            if constexpr (AY) e0v = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qR0, k, jh, X, res, e0v, false);
+            if constexpr (AZ) e1v = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qR1, k, jh, X, res, e1v, false);
+            sm.hn[0][0][XC] = wx1 ? 0.0f : h1<Exact>(HOx[bb], dec0, s0, e0v, e1v);
+          }
+        } else if (halo_row_z) {
+          const int b = c0;
+          const float4 eyh = ld4(E0y + b);
+          float e4 = __shfl_down_sync(kFull, eyh.x, 1);
+          if (lane == 31) e4 = E0y[b + 4];
+          float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
+          if constexpr (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], qa, k, jh, i, res, d0, false);
+          if constexpr (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false);
+          st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), dec2, s2, d0, d1));
+        } else if (halo_col) {
+          const int rr = 1 + lane, b = rr * BX + 3;
+          float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
+          if constexpr (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
+          if constexpr (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
+          float hyv = h1<Exact>(HOy[b], dec1, s1, d0, d1);
+          if (at_y0 && jc == 0 && wy0) hyv = 0.0f;
+          float f0 = D1(E0y[b + 1] - E0y[b]), f1 = D1(E0x[b + BX] - E0x[b]);  // Hz: dEy/dx, dEx/dy
+          if constexpr (AX) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
+          if constexpr (AY) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
+          sm.hn[1][rr][3] = hyv;
+          sm.hn[2][rr][3] = h1<Exact>(HOz[b], dec2, s2, f0, f1);
+        }
+        __syncthreads();
+        if (!emit) {
+          hxp = hx;
+          hyp = hy;
+          hxXp = hxX;
+          return;
+        }
+        // ---- E on the own row ----
+        float4 hzy = ld4(&sm.hn[2][r - 1][c0]), hxy = ld4(&sm.hn[0][r - 1][c0]);
+        float hzl = __shfl_up_sync(kFull, hz.w, 1), hyl = __shfl_up_sync(kFull, hy.w, 1);
+        if (lane == 0) {
+          hzl = sm.hn[2][r][3];
+          hyl = sm.hn[1][r][3];
+          if (at_x0) {  // ghost beyond x = 0: zero on a metallic wall, else the edge value
+            hzl = wx0 ? 0.0f : hz.x;
+            hyl = wx0 ? 0.0f : hy.x;
+          }
+        }
+        if (at_y0 && warp == 0) {  // ghost beyond y = 0
+          hzy = wy0 ? make_float4(0.f, 0.f, 0.f, 0.f) : hz;
+          hxy = wy0 ? make_float4(0.f, 0.f, 0.f, 0.f) : hx;
+        }
+        float4 fx0 = D4(sub4(hz, hzy)), fx1 = D4(sub4(hy, hyp));              // Ex: dHz/dy, dHy/dz
+        float4 fy0 = D4(sub4(hx, hxp)), fy1 = D4(sub4(hz, prev4(hzl, hz)));   // Ey: dHx/dz, dHz/dx
+        float4 fz0 = D4(sub4(hy, prev4(hyl, hy))), fz1 = D4(sub4(hx, hxy));   // Ez: dHy/dx, dHx/dy
+        if constexpr (AY) {
+          fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, true);
+          fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, true);
+        }
+        if constexpr (AZ) {
+          fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, true);
+          fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
+        }
+        if constexpr (AX) {
+          fy1 = psix_apply<Exact>(p.et[3], sm.cc[9], qe3, k, j, i, res, fy1, true);
+          fz0 = psix_apply<Exact>(p.et[4], sm.cc[10], qe4, k, j, i, res, fz0, true);
+        }
+        const uint32_t w4 = *reinterpret_cast<const uint32_t*>(IDS + warp * TX + 4 * lane);
+        const float4 t0 = sm.cls[w4 & 0xffu], t1 = sm.cls[(w4 >> 8) & 0xffu];
+        const float4 t2 = sm.cls[(w4 >> 16) & 0xffu], t3 = sm.cls[w4 >> 24];
+        float4 nx = make_float4(e_upd<Exact>(ex.x, t0.x, fx0.x, fx1.x), e_upd<Exact>(ex.y, t1.x, fx0.y, fx1.y),
+                                e_upd<Exact>(ex.z, t2.x, fx0.z, fx1.z), e_upd<Exact>(ex.w, t3.x, fx0.w, fx1.w));
+        float4 ny = make_float4(e_upd<Exact>(ey.x, t0.y, fy0.x, fy1.x), e_upd<Exact>(ey.y, t1.y, fy0.y, fy1.y),
+                                e_upd<Exact>(ey.z, t2.y, fy0.z, fy1.z), e_upd<Exact>(ey.w, t3.y, fy0.w, fy1.w));
+        float4 nz = make_float4(e_upd<Exact>(ez.x, t0.z, fz0.x, fz1.x), e_upd<Exact>(ez.y, t1.z, fz0.y, fz1.y),
+                                e_upd<Exact>(ez.z, t2.z, fz0.z, fz1.z), e_upd<Exact>(ez.w, t3.z, fz0.w, fz1.w));
+        if (at_y0 && warp == 0 && wy0) {  // PEC: Ex, Ez on the y = 0 wall
+          nx = make_float4(0.f, 0.f, 0.f, 0.f);
+          nz = nx;
+        }
+        if (at_x0 && lane == 0 && wx0) {  // Ey, Ez on the x = 0 wall
+          ny.x = 0.0f;
+          nz.x = 0.0f;
+        }
+        st4(p.eout[0] + o, nx);
+        st4(p.eout[1] + o, ny);
+        st4(p.eout[2] + o, nz);
+        if (xl) {  // Ey, Ez on column X
+          const int b = rc + 4, oX = o + 4;
+          float hxy_X = sm.hn[0][r - 1][XC];
+          if (at_y0 && warp == 0) hxy_X = wy0 ? 0.0f : hxX;
+          // The Hz / Hy ghosts beyond x = X: zero on a metallic wall, else the edge value.
+          float g0 = D1(hxX - hxXp), g1 = D1(wx1 ? 0.0f - hz.w : 0.0f);   // Ey: dHx/dz, dHz/dx
+          float h0 = D1(wx1 ? 0.0f - hy.w : 0.0f), h1v = D1(hxX - hxy_X);  // Ez: dHy/dx, dHx/dy
+          if constexpr (AZ) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
+          if constexpr (AX) {
+            g1 = psi1_apply<Exact, 2>(p.et[3], sm.cc[9], qY3, k, j, X, res, g1, true);
+            h0 = psi1_apply<Exact, 2>(p.et[4], sm.cc[10], qY4, k, j, X, res, h0, true);
+          }
+          if constexpr (AY) h1v = psi1_apply<Exact, 1>(p.et[5], sm.cc[11], qY5, k, j, X, res, h1v, true);
+          const float4 t = sm.cls[cidX];
+          const float ny_ = e_upd<Exact>(E0y[b], t.y, g0, g1);
+          const float nz_ = e_upd<Exact>(E0z[b], t.z, h0, h1v);
+          p.eout[1][oX] = wx1 ? 0.0f : ny_;
+          p.eout[2][oX] = (wx1 || (at_y0 && warp == 0 && wy0)) ? 0.0f : nz_;
+        }
+        hxp = hx;
+        hyp = hy;
+        hxXp = hxX;
+      };
+      if constexpr (!Cpml) {
+        if (xface || yface) body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{});
+        else body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{});
+      } else {
+        const bool az = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
+        const int v = (ax ? 4 : 0) | (ay ? 2 : 0) | (az ? 1 : 0);
+        switch (v == 3 || v == 5 || v == 6 ? 7 : (v == 0 && !(xface || yface) ? 8 : v)) {
+          case 8: body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{}); break;
+          case 0: body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{}); break;
+          case 1: body(std::false_type{}, std::false_type{}, std::true_type{}, std::true_type{}); break;
+          case 2: body(std::false_type{}, std::true_type{}, std::false_type{}, std::true_type{}); break;
+          case 4: body(std::true_type{}, std::false_type{}, std::false_type{}, std::true_type{}); break;
+          default: body(std::true_type{}, std::true_type{}, std::true_type{}, std::true_type{}); break;
+        }
+      }
+    } else {
+      // ---- general tile-plane: per cell, every validity / ghost / PEC rule ---
+      const bool cpml = Cpml;
+      // H of one lattice point at box (rr, cc) = (j0-1+rr, i0-4+cc); `which`
+      // bit 0 Hx, 1 Hy, 2 Hz; `own` stores it (and its psi).
+      auto h_cell = [&](int rr, int cc, int which, bool own) {
+        const int jj = j0 - 1 + rr, ii = i0 - 4 + cc, b = rr * BX + cc;
+        const int o = k * PL + jj * P + ii;
+        const bool zZ = k < Z, yY = jj >= 0 && jj < Y, yY1 = jj >= 0 && jj <= Y;
+        const bool iX = ii >= 0 && ii < X, iX1 = ii >= 0 && ii <= X;
+        if ((which & 1) && zZ && yY && iX1) {  // Hx: dEz/dy - dEy/dz
+          float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
+          if (cpml) {
+            d0 = cpml1<Exact, 1>(p.ht[0], sm.cc[0], cc_smem, res, k, jj, ii, d0, own);
+            d1 = cpml1<Exact, 0>(p.ht[1], sm.cc[1], cc_smem, res, k, jj, ii, d1, own);
+          }
+          float h = h1<Exact>(HOx[b], dec0, s0, d0, d1);
+          if (src) h = h_sources_at(p, sm.amp, 3, k, jj, ii, h);
+          if ((ii == 0 && wx0) || (ii == X && wx1)) h = 0.0f;
+          sm.hn[0][rr][cc] = h;
+          if (own) p.hout[0][o] = h;
+        }
+        if ((which & 2) && zZ && yY1 && iX) {  // Hy: dEx/dz - dEz/dx
+          float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);
+          if (cpml) {
+            d0 = cpml1<Exact, 0>(p.ht[2], sm.cc[2], cc_smem, res, k, jj, ii, d0, own);
+            d1 = cpml1<Exact, 2>(p.ht[3], sm.cc[3], cc_smem, res, k, jj, ii, d1, own);
+          }
+          float h = h1<Exact>(HOy[b], dec1, s1, d0, d1);
+          if (src) h = h_sources_at(p, sm.amp, 4, k, jj, ii, h);
+          if ((jj == 0 && wy0) || (jj == Y && wy1)) h = 0.0f;
+          sm.hn[1][rr][cc] = h;
+          if (own) p.hout[1][o] = h;
+        }
+        if ((which & 4) && yY && iX) {  // Hz: dEy/dx - dEx/dy
+          float d0 = D1(E0y[b + 1] - E0y[b]), d1 = D1(E0x[b + BX] - E0x[b]);
+          if (cpml) {
+            d0 = cpml1<Exact, 2>(p.ht[4], sm.cc[4], cc_smem, res, k, jj, ii, d0, own);
+            d1 = cpml1<Exact, 1>(p.ht[5], sm.cc[5], cc_smem, res, k, jj, ii, d1, own);
+          }
+          float h = h1<Exact>(HOz[b], dec2, s2, d0, d1);
+          if (src) h = h_sources_at(p, sm.amp, 5, k, jj, ii, h);
+          if ((k == 0 && wz0) || (k == Z && wz1)) h = 0.0f;
+          sm.hn[2][rr][cc] = h;
+          if (own) p.hout[2][o] = h;
+        }
+      };
+      // E of one own lattice point at box (rr, cc), with H of the previous
+      // plane there (hxz, hyz).
+      auto e_cell = [&](int rr, int cc, float hxz, float hyz) {
+        const int jj = j0 - 1 + rr, ii = i0 - 4 + cc, b = rr * BX + cc;
+        if (jj > Y || ii > X) return;
+        const int o = k * PL + jj * P + ii;
+        const float hx = sm.hn[0][rr][cc], hy = sm.hn[1][rr][cc], hz = sm.hn[2][rr][cc];
+        const float hz_y = sm.hn[2][rr - 1][cc], hx_y = sm.hn[0][rr - 1][cc];
+        const float hz_x = sm.hn[2][rr][cc - 1], hy_x = sm.hn[1][rr][cc - 1];
+        const bool in_box = cc >= 4 && cc < 4 + TX && rr >= 1 && rr <= TY;
+        const float4 t = sm.cls[in_box ? IDS[(rr - 1) * TX + cc - 4] : p.site_class[(k * (Y + 1) + jj) * p.pitch8 + ii]];
+        if (ii < X) {  // Ex: dHz/dy - dHy/dz
+          float d0 = D1(ghost_diff(hz, hz_y, jj, Y, wy0, wy1)), d1 = D1(ghost_diff(hy, hyz, k, Z, wz0, wz1));
+          if (cpml) {
+            d0 = cpml1<Exact, 1>(p.et[0], sm.cc[6], cc_smem, res, k, jj, ii, d0, true);
+            d1 = cpml1<Exact, 0>(p.et[1], sm.cc[7], cc_smem, res, k, jj, ii, d1, true);
+          }
+          float e = e_upd<Exact>(E0x[b], t.x, d0, d1);
+          if ((k == 0 && wz0) || (k == Z && wz1) || (jj == 0 && wy0) || (jj == Y && wy1)) e = 0.0f;
+          p.eout[0][o] = e;
+        }
+        if (jj < Y) {  // Ey: dHx/dz - dHz/dx
+          float d0 = D1(ghost_diff(hx, hxz, k, Z, wz0, wz1)), d1 = D1(ghost_diff(hz, hz_x, ii, X, wx0, wx1));
+          if (cpml) {
+            d0 = cpml1<Exact, 0>(p.et[2], sm.cc[8], cc_smem, res, k, jj, ii, d0, true);
+            d1 = cpml1<Exact, 2>(p.et[3], sm.cc[9], cc_smem, res, k, jj, ii, d1, true);
+          }
+          float e = e_upd<Exact>(E0y[b], t.y, d0, d1);
+          if ((k == 0 && wz0) || (k == Z && wz1) || (ii == 0 && wx0) || (ii == X && wx1)) e = 0.0f;
+          p.eout[1][o] = e;
+        }
+        if (k < Z) {  // Ez: dHy/dx - dHx/dy
+          float d0 = D1(ghost_diff(hy, hy_x, ii, X, wx0, wx1)), d1 = D1(ghost_diff(hx, hx_y, jj, Y, wy0, wy1));
+          if (cpml) {
+            d0 = cpml1<Exact, 2>(p.et[4], sm.cc[10], cc_smem, res, k, jj, ii, d0, true);
+            d1 = cpml1<Exact, 1>(p.et[5], sm.cc[11], cc_smem, res, k, jj, ii, d1, true);
+          }
+          float e = e_upd<Exact>(E0z[b], t.z, d0, d1);
+          if ((jj == 0 && wy0) || (jj == Y && wy1) || (ii == 0 && wx0) || (ii == X && wx1)) e = 0.0f;
+          p.eout[2][o] = e;
+        }
+      };
+#pragma unroll 1
+      for (int q = 0; q < 4; ++q) h_cell(r, c0 + q, 7, emit);
+      if (xl) h_cell(r, XC, 1, emit);
+      if (emit) {
+        if (warp == 0 && j0 > 0) {
+#pragma unroll 1
+          for (int q = 0; q < 4; ++q) h_cell(0, c0 + q, 1 | 4, false);
+          if (xl) h_cell(0, XC, 1, false);
+        } else if (warp == 2 && lane < TY && i0 > 0) {
+          h_cell(1 + lane, 3, 2 | 4, false);
+        }
+      }
+      __syncthreads();
+      if (emit) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e_cell(r, c0 + q, get(hxp, q), get(hyp, q));
+        if (xl) e_cell(r, XC, hxXp, 0.0f);
+      }
+      hxp = ld4(&sm.hn[0][r][c0]);
+      hyp = ld4(&sm.hn[1][r][c0]);
+      if (xl) hxXp = sm.hn[0][r][XC];
+    }
+    e0 = e1;
+    e1 = e1 == 2 ? 0 : e1 + 1;
+    hs ^= 1;
+  }
+}
+
+template <int NW, bool Cpml, bool Exact>
+cudaError_t launch_fast_t(cudaStream_t s, const FastMaps& maps, const Step3D& p) {
+  using T = FastTile<NW>;
+  const size_t smem = sizeof(typename T::Smem);
+  auto kern = fast_step_kernel<NW, Cpml, Exact>;
+  int device = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err != cudaSuccess) return err;
+  // The dynamic shared-memory limit is a per-device function attribute: set it
+  // on every launch (cheap) rather than once per process.
+  err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  const int kmax = p.Z + 1;
+  const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
+  const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;  // a multiple of 128 leaves column X to lane 31
+  const dim3 grid(gx, (p.Y + 1 + T::TY - 1) / T::TY, (kmax + zc - 1) / zc);
+  Step3D q = p;
+  q.z_chunk = zc;
+  kern<<<grid, dim3(32, NW, 1), smem, s>>>(maps, q);
+  return cudaPeekAtLastError();
+}
+
+template <int NW>
+cudaError_t launch_fast_shape(cudaStream_t s, const Step3D& p) {
+  using T = FastTile<NW>;
+  FastMaps maps;
+  const int64_t P = p.pitch, rowb = P * 4, planeb = static_cast<int64_t>(p.Y + 1) * P * 4;
+  for (int c = 0; c < 3; ++c) {
+    const Dims de = component_dims(c, p.Z, p.Y, p.X), dh = component_dims(c + 3, p.Z, p.Y, p.X);
+    if (!tma::encode(&maps.e[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.ein[c], de.x, de.y, de.z, rowb, planeb, T::BX,
+                     T::EH) ||
+        !tma::encode(&maps.h[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, p.hin[c], dh.x, dh.y, dh.z, rowb, planeb, T::BX,
+                     T::HH))
+      return cudaErrorInvalidValue;
+  }
+  const int64_t P8 = p.pitch8;
+  if (!tma::encode(&maps.ids, CU_TENSOR_MAP_DATA_TYPE_UINT8, p.site_class, p.X + 1, p.Y + 1, p.Z + 1, P8,
+                   P8 * (p.Y + 1), T::TX, T::TY))
+    return cudaErrorInvalidValue;
+  if (p.fast_math) return p.cpml ? launch_fast_t<NW, true, false>(s, maps, p) : launch_fast_t<NW, false, false>(s, maps, p);
+  return p.cpml ? launch_fast_t<NW, true, true>(s, maps, p) : launch_fast_t<NW, false, true>(s, maps, p);
+}
+
+}  // namespace
+
+// tile_y: 8 (8 warps, 128 x 8 tiles) or 4 (4 warps, 128 x 4 tiles).
+cudaError_t launch_fast_tma(cudaStream_t s, const Step3D& p, int tile_y) {
+  return tile_y == 4 ? launch_fast_shape<4>(s, p) : launch_fast_shape<8>(s, p);
+}
+
+}  // namespace fdtd

@@ -59,6 +59,14 @@ struct Step3D {
   // FDTD_LAYOUT_PITCHED: floats per row of every field and site-id array.
   int pitch;
   int* status;  // optional error word for expired bounded waits
+  unsigned long long wait_ns;  // bound of every mbarrier wait (device time)
+  int test_stall;              // test-only: arm the first bundle's barrier without issuing its copies
+  // FDTD_FLAG_FAST pitched step: uint8 material class per lattice point
+  // (rows of pitch8 bytes) and the class table (Ex, Ey, Ez coefficients over dx).
+  const uint8_t* site_class;
+  int pitch8;
+  const float4* class_coef;
+  int fast_math;  // tolerance arithmetic in the class step (1/dx folded, fused multiply-adds)
   // Derivative metrics per axis (z, y, x), or null (isotropic: divide by res).
   const float* metric_h[3];  // [n_axis]: forward differences feeding H
   const float* metric_e[3];  // [n_axis + 1]: backward differences feeding E

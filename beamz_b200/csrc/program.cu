@@ -156,6 +156,23 @@ int validate(const FdtdProgram& p) {
       return kInvalid;
     if (!is_f32(p.site_coef) || elements(p.site_coef) != 3 * 256 || p.site_coef.data == nullptr) return kInvalid;
   }
+  if (p.flags & FDTD_FLAG_CLASSES) {
+    // The class step: uint8 classes on 16-byte rows, a
+    // 256-entry class table.
+    if (!pitched) return kInvalid;
+    const FdtdBuffer& cls = p.site_class;
+    if (cls.element_type != FDTD_U8 || cls.rank != 3 || cls.dims[0] != L.Z + 1 || cls.dims[1] != L.Y + 1 ||
+        cls.dims[2] < L.X + 1 || cls.dims[2] % 16 != 0 || cls.data == nullptr ||
+        (reinterpret_cast<uintptr_t>(cls.data) & 15) != 0)
+      return kInvalid;
+    if (static_cast<int64_t>(L.Z + 1) * (L.Y + 1) * cls.dims[2] >= (int64_t{1} << 31)) return kInvalid;
+    if (!is_f32(p.class_coef) || elements(p.class_coef) != 4 * 256 || p.class_coef.data == nullptr ||
+        (reinterpret_cast<uintptr_t>(p.class_coef.data) & 15) != 0)
+      return kInvalid;
+  }
+  if ((p.flags & FDTD_FLAG_FAST_MATH) && !(p.flags & FDTD_FLAG_CLASSES)) return kInvalid;
+  if ((p.flags & FDTD_FLAG_TEST_STALL) && !pitched) return kInvalid;
+  if (p.wait_limit_ns < 0) return kInvalid;
   if (p.cpml) {
     const int nterms = p.ndim == 3 ? 6 : 2;
     for (int h = 0; h < 2; ++h) {
@@ -380,6 +397,14 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
   s.z_chunk = p.z_chunk;
   s.pitch = static_cast<int>(p.pitch);
   s.status = static_cast<int*>(p.status.data);
+  s.wait_ns = p.wait_limit_ns > 0 ? static_cast<unsigned long long>(p.wait_limit_ns) : 200000000ull;
+  s.test_stall = (p.flags & FDTD_FLAG_TEST_STALL) ? 1 : 0;
+  if (p.flags & FDTD_FLAG_CLASSES) {
+    s.fast_math = (p.flags & FDTD_FLAG_FAST_MATH) ? 1 : 0;
+    s.site_class = static_cast<const uint8_t*>(p.site_class.data);
+    s.pitch8 = static_cast<int>(p.site_class.dims[2]);
+    s.class_coef = static_cast<const float4*>(p.class_coef.data);
+  }
   for (int a = 0; a < 3; ++a) {
     s.metric_h[a] = static_cast<const float*>(p.metric_h[a].data);
     s.metric_e[a] = static_cast<const float*>(p.metric_e[a].data);
@@ -580,7 +605,9 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
       for (int i = 0; i < n_hsrc; ++i) sp.hsrc[i] = hsrc[i];
       sp.n_esrc = n_esrc;
       for (int i = 0; i < n_esrc; ++i) sp.esrc[i] = esrc[i];
-      if (p.layout == FDTD_LAYOUT_PITCHED) {
+      if (p.layout == FDTD_LAYOUT_PITCHED && (p.flags & FDTD_FLAG_CLASSES)) {
+        err = launch_fast_tma(s, sp, p.tile_y);
+      } else if (p.layout == FDTD_LAYOUT_PITCHED) {
         err = launch_fused_tma(s, sp, p.tile_y);
       } else if (L.active == kActive3D) {
         err = launch_fused_lean(s, sp, p.material_kind, p.tile_y);

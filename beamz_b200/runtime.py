@@ -109,6 +109,44 @@ def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, 
     return words, torch.as_tensor(coef, device=device)
 
 
+class ClassOverflow(ValueError):
+    """More than 256 distinct (Ex, Ey, Ez) coefficient triples: no uint8 class ids."""
+
+
+def device_site_classes(words, coef, res: float, nx: int, z_block: int = 64, over_dx: bool = False):
+    """uint8 material classes of the codebook words (each distinct (Ex, Ey, Ez)
+    id triple one class, numbered in increasing word order) on rows of a
+    16-byte multiple, and the (256, 4) float32 table of each class's Ex, Ey,
+    Ez coefficients: the codebook's own values, or with ``over_dx`` divided by
+    the cell size (rounded once from float64) for the tolerance arithmetic.
+    Raises :class:`ClassOverflow` above 256 classes."""
+    torch = _torch()
+    dev = words.device
+    nz1, ny1, _ = (int(v) for v in words.shape)
+    pitch8 = -(-(nx + 1) // 16) * 16
+    present = torch.zeros(1 << 24, dtype=torch.int32, device=dev)
+    for k0 in range(0, nz1, z_block):
+        w = words[k0:k0 + z_block, :, : nx + 1].reshape(-1).long()
+        present += torch.bincount(w, minlength=1 << 24).to(torch.int32)[: 1 << 24].clamp_(max=1)
+        present.clamp_(max=1)
+    keys = torch.nonzero(present, as_tuple=False).reshape(-1)
+    if keys.numel() > 256:
+        raise ClassOverflow(f"{keys.numel()} distinct E coefficient triples (> 256)")
+    lut = torch.zeros(1 << 24, dtype=torch.uint8, device=dev)
+    lut[keys] = torch.arange(keys.numel(), device=dev, dtype=torch.int32).to(torch.uint8)
+    classes = torch.zeros((nz1, ny1, pitch8), dtype=torch.uint8, device=dev)
+    for k0 in range(0, nz1, z_block):
+        w = words[k0:k0 + z_block, :, : nx + 1].long()
+        classes[k0:k0 + z_block, :, : nx + 1] = lut[w]
+    k = keys.cpu().numpy().astype(np.int64)
+    c64 = np.asarray(coef.cpu().numpy() if hasattr(coef, "cpu") else coef, np.float64)
+    table = np.zeros((256, 4), np.float32)
+    for n in range(3):
+        v = c64[n, (k >> (8 * n)) & 0xFF]
+        table[: k.size, n] = (v / np.float64(np.float32(res)) if over_dx else v).astype(np.float32)
+    return classes, torch.as_tensor(table, device=dev)
+
+
 @dataclass
 class DftArena:
     """Device buffers of the packed monitor plan (beamz/simulation/cuda/runtime.py:530-618)."""
@@ -237,7 +275,9 @@ class DeviceProgram:
     """A compiled program: every static input of the step, resident on the device."""
 
     def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
-                 graphs=True, layout="auto", dft_batch: int = 16, dft_overlap: bool = True):
+                 graphs=True, layout="auto", dft_batch: int = 16, dft_overlap: bool = True,
+                 arithmetic: str = "exact", step_kernel: str = "codebook", wait_limit_ns: int = 0,
+                 test_stall: bool = False):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
         torch = _torch()
@@ -275,9 +315,38 @@ class DeviceProgram:
         elif layout == "auto":
             layout = "dense"
         self.layout = layout
+        # The pitched 3D step: the class step (uint8 material classes, 128-wide
+        # tiles) unless the scene has more than 256 distinct E coefficient
+        # triples or the codebook step is asked for.  Its arithmetic is
+        # beamz's float32 order; "fast" opts into the tolerance form.
+        if arithmetic not in ("fast", "exact"):
+            raise ValueError("arithmetic is 'fast' or 'exact'")
+        if step_kernel not in ("classes", "codebook"):
+            raise ValueError("step_kernel is 'classes' or 'codebook'")
+        self.site_class = self.class_coef = None
+        if layout == "pitched" and step_kernel == "classes":
+            try:
+                self.site_class, self.class_coef = device_site_classes(
+                    self.site_ids, self.site_coef, float(spec.resolution), int(spec.grid_shape[2]),
+                    over_dx=arithmetic == "fast")
+            except ClassOverflow:
+                step_kernel = "codebook"
+        if layout != "pitched":
+            step_kernel = "dense"
+        if step_kernel != "classes":
+            arithmetic = "exact"
+        self.step_kernel = step_kernel
+        self.arithmetic = arithmetic
         s = abi.FdtdProgram()
         s.abi_version = abi.FDTD_ABI_VERSION
         s.flags = abi.FDTD_FLAG_GRAPH_CACHE if graphs else 0
+        if step_kernel == "classes":
+            s.flags |= abi.FDTD_FLAG_CLASSES
+            if arithmetic == "fast":
+                s.flags |= abi.FDTD_FLAG_FAST_MATH
+        s.wait_limit_ns = int(wait_limit_ns)
+        if test_stall:  # test only: the pitched step's first wait runs out (nothing in flight)
+            s.flags |= abi.FDTD_FLAG_TEST_STALL
         s.ndim = spec.ndim
         s.polarization = 0 if spec.polarization == "tm" else 1
         s.schedule = self.schedule
@@ -318,6 +387,9 @@ class DeviceProgram:
             s.material_kind = abi.FDTD_MATERIAL_CODEBOOK
             s.site_ids = buf(self.site_ids)
             s.site_coef = buf(self.site_coef)
+            if self.site_class is not None:
+                s.site_class = buf(self.site_class)
+                s.class_coef = buf(self.class_coef)
         elif spec.voxel_ids is not None:
             s.material_kind = abi.FDTD_MATERIAL_VOXEL
             ids = np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8)

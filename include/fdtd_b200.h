@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 10
+#define FDTD_ABI_VERSION 11
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -43,6 +43,24 @@ enum {
  * a monitor: a pre-E source writes the bank that the previous step's sample
  * reads.  One host thread per caller stream. */
 #define FDTD_FLAG_DFT_OVERLAP (1 << 16)
+/* Class step (no counterpart in beamz): the 3D step of a PITCHED program reads
+ * its E material as one uint8 class per lattice point (site_class /
+ * class_coef below, 1 byte per cell instead of a 4-byte codebook word) and
+ * runs 128-wide tiles with four cells per thread.  Its arithmetic is beamz's
+ * float32 order, bit for bit, unless FDTD_FLAG_FAST_MATH is set too. */
+#define FDTD_FLAG_CLASSES (1 << 17)
+/* Tolerance arithmetic in the class step: 1/dx folded into the coefficients
+ * (class_coef then holds dt / (eps0 eps dx)), products contracted into fused
+ * multiply-adds.  Each step rounds within a few ulp of beamz's float32 path;
+ * after long runs whose fields decay (absorbed pulses) the difference grows
+ * to the float32 noise floor of the run itself (that of float32 against
+ * float64), so parity with the float32 path is a tolerance, not equality. */
+#define FDTD_FLAG_FAST_MATH (1 << 19)
+/* Test only: the pitched step arms its first copy barrier without issuing the
+ * copies, so its bounded wait runs out after wait_limit_ns with nothing in
+ * flight, and the kernel returns after setting `status` -- the expiry path,
+ * exercised without a fault or a hang. */
+#define FDTD_FLAG_TEST_STALL (1 << 18)
 
 /* Step schedules. */
 enum {
@@ -214,7 +232,7 @@ typedef struct FdtdProgram {
   int32_t z_chunk;        /* fused-kernel z planes per CTA (0 = whole axis) */
   int32_t layout;         /* FDTD_LAYOUT_* */
   int64_t pitch;          /* PITCHED: floats per row of every field array */
-  int64_t reserved64;
+  int64_t wait_limit_ns;  /* bound of every device-side wait of the pitched step (0 = 200 ms) */
   FdtdBuffer fields[6];     /* bank A (in/out) */
   FdtdBuffer fields_alt[6]; /* bank B (FDTD_SCHEDULE_FUSED only) */
   /* FDTD_MATERIAL_SITE: e_decay[c], e_source[c] are rank-0 or full E-component
@@ -254,6 +272,14 @@ typedef struct FdtdProgram {
   int32_t recorder_count;
   int32_t reserved_recorders;
   FdtdRecorder recorders[FDTD_MAX_RECORDERS];
+  /* FDTD_FLAG_CLASSES with FDTD_MATERIAL_CODEBOOK: U8 [Z+1, Y+1, pitch8]
+   * material class of every lattice point (pitch8 = dims[2], a multiple of 16
+   * >= X+1) and F32 [256, 4] per class the Ex, Ey, Ez update coefficients
+   * fl(fl(dt)/fl(eps0) * fl(1/eps_site)) -- over dx with FDTD_FLAG_FAST_MATH
+   * -- (the fourth column unused).  A class is one distinct (Ex, Ey, Ez)
+   * coefficient triple of the codebook. */
+  FdtdBuffer site_class;
+  FdtdBuffer class_coef;
 } FdtdProgram;
 
 /* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */

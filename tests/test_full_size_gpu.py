@@ -2,8 +2,10 @@
 x-normal DFT planes) at full size, through properties that do not need the
 numpy oracle to finish: agreement with the C restatement of the reference
 (accuracy bound: 1e-5 relative L2 for fields, 1e-4 for the DFT), bitwise
-agreement of the pitched TMA kernel with the dense kernel, exact linearity
-under a power-of-two scaling, and run-to-run determinism."""
+agreement of the exact pitched TMA kernel with the dense kernel (both bit for
+bit the float32 restatement), the full 1000-step run of the tolerance-mode
+step against the exact step, exact linearity under a power-of-two scaling,
+and run-to-run determinism."""
 
 from __future__ import annotations
 
@@ -45,7 +47,8 @@ def test_config2_matches_the_c_restatement(scene):
 
 def test_config2_pitched_and_dense_kernels_agree_bitwise(scene):
     spec, fields = scene
-    pitched = R.compile_program(spec)
+    pitched = R.compile_program(spec, step_kernel="classes")
+    assert pitched.step_kernel == "classes"
     a = R.run_steps(R.initial_state(pitched, fields=fields), pitched, STEPS).numpy()
     del pitched
     torch.cuda.empty_cache()
@@ -76,3 +79,26 @@ def test_config2_is_linear_and_deterministic(scene):
         np.testing.assert_array_equal(again[k], one[k])
         np.testing.assert_array_equal(two[k], 2 * one[k])
     np.testing.assert_array_equal(two["dft_w"], one["dft_w"])
+
+
+def test_config2_full_run_of_the_class_step_matches_the_codebook_step():
+    """All 1000 steps of the workload from zero fields (the dipole pulse and
+    the 4 x 5 DFT planes): the class step (the hot path) against the codebook
+    step, which equals the float32 restatement of the reference bit for bit
+    (the 3-step test above pins that at this size; the oracle tests at every
+    small size), bit for bit over the whole run."""
+    spec = W.scene_3d_512(total_steps=1000)
+    a_prog = R.compile_program(spec, step_kernel="classes")
+    assert a_prog.step_kernel == "classes"
+    a = R.run_steps(R.initial_state(a_prog), a_prog, 1000).numpy()
+    del a_prog
+    torch.cuda.empty_cache()
+    b_prog = R.compile_program(spec, step_kernel="codebook")
+    b = R.run_steps(R.initial_state(b_prog), b_prog, 1000).numpy()
+    del b_prog
+    torch.cuda.empty_cache()
+    for c in P.COMPONENTS:
+        assert np.linalg.norm(b[c]) > 0, c
+        np.testing.assert_array_equal(a[c], b[c], err_msg=c)
+    for k in ("dft_re", "dft_im", "dft_w"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)

@@ -126,14 +126,15 @@ def test_random_3d_against_oracle(case, schedule):
     _compare(state.numpy(), st, P.COMPONENTS)
 
 
+@pytest.mark.parametrize("step_kernel", ["classes", "codebook"])
 @pytest.mark.parametrize("tile", [(32, 4), (32, 8), (32, 16), (64, 4), (64, 8)])
 @pytest.mark.parametrize("z_chunk", [0, 3])
-def test_fused_tiles_and_z_chunks_are_bitwise_identical(tile, z_chunk):
+def test_fused_tiles_and_z_chunks_are_bitwise_identical(tile, z_chunk, step_kernel):
     spec = scenario_3d(grid=(11, 21, 70), seed=4, nsteps=6, metallic=("front",))
     fields = random_initial_fields(spec, seed=5)
     ref_prog = R.compile_program(spec, schedule="phases")
     ref = R.run_steps(R.initial_state(ref_prog, fields=fields), ref_prog, 6).numpy()
-    prog = R.compile_program(spec, schedule="fused", tile=tile, z_chunk=z_chunk)
+    prog = R.compile_program(spec, schedule="fused", tile=tile, z_chunk=z_chunk, step_kernel=step_kernel)
     out = R.run_steps(R.initial_state(prog, fields=fields), prog, 6).numpy()
     for c in P.COMPONENTS:
         np.testing.assert_array_equal(out[c], ref[c], err_msg=c)
