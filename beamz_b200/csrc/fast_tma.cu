@@ -191,29 +191,52 @@ __device__ __forceinline__ float4 psi4_apply(const CpmlTermDev& t, const float4*
   return r;
 }
 
-// An x term: the slot differs per cell.
-__device__ __forceinline__ float4 psix_fetch(const CpmlTermDev& t, int k, int j, int i) {
-  float v[4];
+// An x term on a lane's four cells: which cells lie in the term's slab (bits
+// 0-3) and the slot of cell 0, packed as mask | slot0 << 4; the slots of a
+// contiguous slab are consecutive.  Tile-constant, so computed once per CTA.
+__device__ __forceinline__ int xslab_of(const CpmlTermDev& t, int i) {
+  int mask = 0, base = 0;
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
+  for (int c = 3; c >= 0; --c) {
     const int slot = slot_of(t, i + c);
-    v[c] = slot >= 0 ? t.psi_in[psi_off<2>(t, slot, k, j, i + c)] : 0.0f;
+    if (slot >= 0) {
+      mask |= 1 << c;
+      base = slot - c;
+    }
+  }
+  return mask | (base << 4);
+}
+
+// psi of an x term on the own cells of row (k, j): the row offset of slot 0.
+__device__ __forceinline__ int xrow(const CpmlTermDev& t, int xs, int k, int j) {
+  return (k * t.pdy + j) * t.pdx + (xs >> 4);
+}
+
+__device__ __forceinline__ float4 psix_fetch(const CpmlTermDev& t, int xs, int k, int j) {
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  if (xs & 15) {
+    const float* row = t.psi_in + xrow(t, xs, k, j);
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (xs & (1 << c)) v[c] = row[c];
   }
   return make_float4(v[0], v[1], v[2], v[3]);
 }
 
 template <bool Exact>
-__device__ __forceinline__ float4 psix_apply(const CpmlTermDev& t, const float4* cc, float4 v, int k, int j, int i,
+__device__ __forceinline__ float4 psix_apply(const CpmlTermDev& t, const float4* cc, int xs, float4 v, int k, int j,
                                              float res, float4 d, bool write) {
+  if (!(xs & 15)) return d;
   float r[4] = {d.x, d.y, d.z, d.w};
   const float pv[4] = {v.x, v.y, v.z, v.w};
+  const int base = xs >> 4;
+  float* row = t.psi_out + xrow(t, xs, k, j);
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const int slot = slot_of(t, i + c);
-    if (slot < 0) continue;
+    if (!(xs & (1 << c))) continue;
     float n;
-    r[c] = cpml_d<Exact>(cc[slot], res, pv[c], r[c], &n);
-    if (write) t.psi_out[psi_off<2>(t, slot, k, j, i + c)] = n;
+    r[c] = cpml_d<Exact>(cc[base + c], res, pv[c], r[c], &n);
+    if (write) row[c] = n;
   }
   return make_float4(r[0], r[1], r[2], r[3]);
 }
@@ -256,23 +279,17 @@ __device__ __forceinline__ void l2_prefetch(const void* ptr) {
   asm volatile("prefetch.global.L2 [%0];\n" ::"l"(ptr));
 }
 
-// L2 prefetch of the psi a term needs at (k, j, i..i+3), if any cell is in its slab.
+// L2 prefetch of the psi a y or z term needs at (k, j, i..i+3), if in its slab.
 template <int Axis>
 __device__ __forceinline__ void psi_prefetch(const CpmlTermDev& t, int k, int j, int i) {
   if (t.psi_in == nullptr) return;
-  if (Axis == 2) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int slot = slot_of(t, i + c);
-      if (slot >= 0) {
-        l2_prefetch(t.psi_in + psi_off<2>(t, slot, k, j, i + c));
-        return;
-      }
-    }
-    return;
-  }
   const int slot = slot_of(t, Axis == 0 ? k : j);
   if (slot >= 0) l2_prefetch(t.psi_in + psi_off<Axis>(t, slot, k, j, i));
+}
+
+// ... and of an x term through its lane mask.
+__device__ __forceinline__ void psix_prefetch(const CpmlTermDev& t, int xs, int k, int j) {
+  if (xs & 15) l2_prefetch(t.psi_in + xrow(t, xs, k, j));
 }
 
 __device__ __forceinline__ float h_sources_at(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
@@ -388,6 +405,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
 
+  // x-slab masks of the own cells for Hyx, Hzx, Eyx, Ezx (tile-constant).
+  int xs3 = 0, xs4 = 0, xe3 = 0, xe4 = 0;
+  if (ax) {
+    xs3 = xslab_of(p.ht[3], i);
+    xs4 = xslab_of(p.ht[4], i);
+    xe3 = xslab_of(p.et[3], i);
+    xe4 = xslab_of(p.et[4], i);
+  }
+
   // H of the previous plane on the own cells (the z-backward differences of E).
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
   float hxXp = 0.0f;
@@ -436,8 +462,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         // Class id of column X (lane 31 of the last tile).
         const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
         // psi of the H terms: own cells, halos, column X.
-        float4 qh0, qh1, qh2, qh3, qh4, qh5, qa, qb;
-        float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f, qX0 = 0.f, qX1 = 0.f, qR0 = 0.f, qR1 = 0.f;
+        float4 qh0, qh1, qh2, qh3, qh4, qh5;
         if constexpr (AY) {
           qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
           qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
@@ -447,30 +472,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
         if constexpr (AX) {
-          qh3 = psix_fetch(p.ht[3], k, j, i);
-          qh4 = psix_fetch(p.ht[4], k, j, i);
-        }
-        if constexpr (AX || AY || AZ) {
-          if (halo_row_x) {
-            if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
-            if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
-            if (xl) {
-              if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
-              if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
-            }
-          } else if (halo_row_z) {
-            if constexpr (AX) qa = psix_fetch(p.ht[4], k, jh, i);
-            if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
-          } else if (halo_col) {
-            if constexpr (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
-            if constexpr (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
-            if constexpr (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
-            if constexpr (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
-          }
-          if (xl) {
-            if constexpr (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
-            if constexpr (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
-          }
+          qh3 = psix_fetch(p.ht[3], xs3, k, j);
+          qh4 = psix_fetch(p.ht[4], xs4, k, j);
         }
         // Next plane's psi (and column X's class id) into L2, a plane ahead of use.
         if (k + 1 < k1) {
@@ -488,25 +491,34 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               psi_prefetch<1>(p.et[5], kn, j, i);
             }
             if constexpr (AX) {
-              psi_prefetch<2>(p.ht[3], kn, j, i);
-              psi_prefetch<2>(p.ht[4], kn, j, i);
-              psi_prefetch<2>(p.et[3], kn, j, i);
-              psi_prefetch<2>(p.et[4], kn, j, i);
+              psix_prefetch(p.ht[3], xs3, kn, j);
+              psix_prefetch(p.ht[4], xs4, kn, j);
+              psix_prefetch(p.et[3], xe3, kn, j);
+              psix_prefetch(p.et[4], xe4, kn, j);
+            }
+            // The halos' (read-only) psi of the next plane.
+            if (warp == 0 && !at_y0) {
+              if constexpr (AY) psi_prefetch<1>(p.ht[0], kn, jh, i);
+              psi_prefetch<0>(p.ht[1], kn, jh, i);
+            } else if (warp == 1 && !at_y0) {
+              if constexpr (AX) psix_prefetch(p.ht[4], xs4, kn, jh);
+              if constexpr (AY) psi_prefetch<1>(p.ht[5], kn, jh, i);
             }
           }
         }
         // ---- H on the own row ----
-        const float4 ez = ld4(E0z + rc), ezy = ld4(E0z + rc + BX);
-        const float4 ey = ld4(E0y + rc), eyz = ld4(E1y + rc);
-        const float4 ex = ld4(E0x + rc), exz = ld4(E1x + rc), exy = ld4(E0x + rc + BX);
-        float ez4 = __shfl_down_sync(kFull, ez.x, 1), ey4 = __shfl_down_sync(kFull, ey.x, 1);
-        if (lane == 31) {
-          ez4 = E0z[rc + 4];
-          ey4 = E0y[rc + 4];
+        float4 dx0, dx1, dy0, dy1, dz0, dz1;
+        {
+          const float4 ez = ld4(E0z + rc), ey = ld4(E0y + rc), ex = ld4(E0x + rc);
+          float ez4 = __shfl_down_sync(kFull, ez.x, 1), ey4 = __shfl_down_sync(kFull, ey.x, 1);
+          if (lane == 31) {
+            ez4 = E0z[rc + 4];
+            ey4 = E0y[rc + 4];
+          }
+          dx0 = D4(sub4(ld4(E0z + rc + BX), ez)), dx1 = D4(sub4(ld4(E1y + rc), ey));   // Hx: dEz/dy, dEy/dz
+          dy0 = D4(sub4(ld4(E1x + rc), ex)), dy1 = D4(sub4(next4(ez, ez4), ez));       // Hy: dEx/dz, dEz/dx
+          dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(ld4(E0x + rc + BX), ex));  // Hz: dEy/dx, dEx/dy
         }
-        float4 dx0 = D4(sub4(ezy, ez)), dx1 = D4(sub4(eyz, ey));              // Hx: dEz/dy, dEy/dz
-        float4 dy0 = D4(sub4(exz, ex)), dy1 = D4(sub4(next4(ez, ez4), ez));   // Hy: dEx/dz, dEz/dx
-        float4 dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(exy, ex));   // Hz: dEy/dx, dEx/dy
         if constexpr (AY) {
           dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit);
           dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit);
@@ -516,8 +528,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
         }
         if constexpr (AX) {
-          dy1 = psix_apply<Exact>(p.ht[3], sm.cc[3], qh3, k, j, i, res, dy1, emit);
-          dz0 = psix_apply<Exact>(p.ht[4], sm.cc[4], qh4, k, j, i, res, dz0, emit);
+          dy1 = psix_apply<Exact>(p.ht[3], sm.cc[3], xs3, qh3, k, j, res, dy1, emit);
+          dz0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qh4, k, j, res, dz0, emit);
         }
         float4 hx = h4<Exact>(ld4(HOx + rc), dec0, s0, dx0, dx1);
         float4 hy = h4<Exact>(ld4(HOy + rc), dec1, s1, dy0, dy1);
@@ -537,6 +549,9 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         float hxX = 0.0f;
         if (xl) {
           const int b = rc + 4;
+          float qX0 = 0.f, qX1 = 0.f;
+          if constexpr (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
+          if constexpr (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
           float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
           if constexpr (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit);
           if constexpr (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit);
@@ -544,33 +559,18 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           sm.hn[0][r][XC] = hxX;
           if (emit) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
         }
-        // psi of the E terms, in flight during the halo and the barrier.
-        float4 qe0, qe1, qe2, qe3, qe4, qe5;
-        float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
-        if (emit) {
-          if constexpr (AY) {
-            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
-            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
-          }
-          if constexpr (AZ) {
-            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
-            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
-          }
-          if constexpr (AX) {
-            qe3 = psix_fetch(p.et[3], k, j, i);
-            qe4 = psix_fetch(p.et[4], k, j, i);
-          }
-          if (xl) {
-            if constexpr (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
-            if constexpr (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
-            if constexpr (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
-            if constexpr (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
-          }
-        }
         // ---- recomputed halo: row j0-1 (Hx by warp 0, Hz by warp 1) and
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
         if (halo_row_x) {
           const int b = c0;
+          float4 qa, qb;
+          float qR0 = 0.f, qR1 = 0.f;
+          if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
+          if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
+          if (xl) {
+            if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
+            if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
+          }
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
           if constexpr (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
           if constexpr (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
@@ -586,15 +586,23 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           }
         } else if (halo_row_z) {
           const int b = c0;
+          float4 qa, qb;
+          if constexpr (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
+          if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
           if (lane == 31) e4 = E0y[b + 4];
           float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
-          if constexpr (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], qa, k, jh, i, res, d0, false);
+          if constexpr (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
           if constexpr (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false);
           st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), dec2, s2, d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
+          float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f;
+          if constexpr (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
+          if constexpr (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
+          if constexpr (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
+          if constexpr (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
           float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
           if constexpr (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
           if constexpr (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
@@ -605,6 +613,29 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if constexpr (AY) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
           sm.hn[1][rr][3] = hyv;
           sm.hn[2][rr][3] = h1<Exact>(HOz[b], dec2, s2, f0, f1);
+        }
+        // psi of the E terms, in flight during the barrier.
+        float4 qe0, qe1, qe2, qe3, qe4, qe5;
+        float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
+        if (emit) {
+          if constexpr (AY) {
+            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
+            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
+          }
+          if constexpr (AZ) {
+            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
+            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
+          }
+          if constexpr (AX) {
+            qe3 = psix_fetch(p.et[3], xe3, k, j);
+            qe4 = psix_fetch(p.et[4], xe4, k, j);
+          }
+          if (xl) {
+            if constexpr (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
+            if constexpr (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
+            if constexpr (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
+            if constexpr (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
+          }
         }
         __syncthreads();
         if (!emit) {
@@ -640,9 +671,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
         }
         if constexpr (AX) {
-          fy1 = psix_apply<Exact>(p.et[3], sm.cc[9], qe3, k, j, i, res, fy1, true);
-          fz0 = psix_apply<Exact>(p.et[4], sm.cc[10], qe4, k, j, i, res, fz0, true);
+          fy1 = psix_apply<Exact>(p.et[3], sm.cc[9], xe3, qe3, k, j, res, fy1, true);
+          fz0 = psix_apply<Exact>(p.et[4], sm.cc[10], xe4, qe4, k, j, res, fz0, true);
         }
+        const float4 ex = ld4(E0x + rc), ey = ld4(E0y + rc), ez = ld4(E0z + rc);  // E(k) of the own cells
         const uint32_t w4 = *reinterpret_cast<const uint32_t*>(IDS + warp * TX + 4 * lane);
         const float4 t0 = sm.cls[w4 & 0xffu], t1 = sm.cls[(w4 >> 8) & 0xffu];
         const float4 t2 = sm.cls[(w4 >> 16) & 0xffu], t3 = sm.cls[w4 >> 24];

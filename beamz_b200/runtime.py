@@ -109,6 +109,49 @@ def device_site_codebook(voxel_ids, eps_table, dt_over_eps, pitch: int, device, 
     return words, torch.as_tensor(coef, device=device)
 
 
+def lossless_site_sources(spec: ProgramSpec):
+    """The per-site E sources of a 3D program whose E decay is exactly 1
+    everywhere (beamz's lossless material: E <- E + source * curl), else None."""
+    if spec.ndim != 3 or spec.e_site is None or spec.voxel_ids is not None:
+        return None
+    out = {}
+    for c in ("Ex", "Ey", "Ez"):
+        if c not in spec.e_site:
+            return None
+        dec, src = spec.e_site[c]
+        if np.any(np.asarray(dec, np.float32) != np.float32(1.0)):
+            return None
+        out[c] = src
+    return out
+
+
+def device_codebook_from_sites(sources: dict, shapes: dict, pitch: int, dt: float, device):
+    """Codebook words (Z+1, Y+1, pitch) int32 and (3, 256) tables from per-site
+    lossless E sources: per component the distinct source values (at most 256,
+    in increasing order) and each site's index among them -- beamz packs its
+    lossless CUDA coefficients the same way (compile.py:146-187) -- plus the
+    relative permittivity dt / (eps0 source) of each table entry (energy
+    diagnostics).  Raises :class:`CodebookOverflow` above 256 values."""
+    torch = _torch()
+    ez = shapes["Ex"]  # (Z+1, Y+1, X): the lattice's z and y extents
+    words = torch.zeros((int(ez[0]), int(ez[1]), pitch), dtype=torch.int32, device=device)
+    coef = np.zeros((3, 256), np.float32)
+    eps = np.ones((3, 256), np.float32)
+    for n, c in enumerate(("Ex", "Ey", "Ez")):
+        src = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(sources[c], np.float32), shapes[c])),
+                              device=device)
+        table, ids = torch.unique(src, return_inverse=True)
+        if table.numel() > 256:
+            raise CodebookOverflow(f"{c}: {table.numel()} distinct E-site coefficients (> 256)")
+        dz, dy, dx = (int(v) for v in shapes[c])
+        words[:dz, :dy, :dx] |= ids.to(torch.int32) << (8 * n)
+        t = table.cpu().numpy()
+        coef[n, : t.size] = t
+        with np.errstate(divide="ignore"):
+            eps[n, : t.size] = np.where(t != 0, np.float64(dt) / (EPS_0 * t.astype(np.float64)), 1.0)
+    return words, torch.as_tensor(coef, device=device), torch.as_tensor(eps, device=device)
+
+
 class ClassOverflow(ValueError):
     """More than 256 distinct (Ex, Ey, Ez) coefficient triples: no uint8 class ids."""
 
@@ -289,8 +332,9 @@ class DeviceProgram:
         self.shapes = {c: component_shape(c, spec.grid_shape, spec.polarization) for c in COMPONENTS}
         dev = self.device
         h_uniform = all(np.ndim(d) == 0 and np.ndim(s_) == 0 for d, s_ in spec.h_coefficients().values())
-        pitched_ok = (spec.ndim == 3 and spec.voxel_ids is not None and schedule == "fused" and h_uniform
-                      and spec.metrics is None)
+        site_sources = lossless_site_sources(spec)
+        pitched_ok = (spec.ndim == 3 and (spec.voxel_ids is not None or site_sources is not None)
+                      and schedule == "fused" and h_uniform and spec.metrics is None)
         if layout == "pitched" and not pitched_ok:
             raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule, uniform H and an "
                              "isotropic grid")
@@ -303,10 +347,14 @@ class DeviceProgram:
             self.pitch = -(-(nx + 1) // 4) * 4
             self.bank_shape = (nz + 1, ny + 1, self.pitch)
             try:
-                ids = torch.as_tensor(np.ascontiguousarray(spec.voxel_ids, np.uint8), device=dev)
-                self.site_ids, self.site_coef, self.site_eps_table = device_site_codebook(
-                    spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev, with_eps=True, ids=ids,
-                    counts=voxel_histogram(ids, dev))
+                if spec.voxel_ids is not None:
+                    ids = torch.as_tensor(np.ascontiguousarray(spec.voxel_ids, np.uint8), device=dev)
+                    self.site_ids, self.site_coef, self.site_eps_table = device_site_codebook(
+                        spec.voxel_ids, spec.eps_table, dt_over_eps, self.pitch, dev, with_eps=True, ids=ids,
+                        counts=voxel_histogram(ids, dev))
+                else:
+                    self.site_ids, self.site_coef, self.site_eps_table = device_codebook_from_sites(
+                        site_sources, self.shapes, self.pitch, float(spec.dt), dev)
                 layout = "pitched"
             except CodebookOverflow:
                 if layout == "pitched":

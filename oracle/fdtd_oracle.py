@@ -616,7 +616,8 @@ def update_e_3d(fields, psi_e, e_terms, dt, resolution, material: Material3D, me
     )
     one = f(1.0)
     dt_over_eps = f(dt) / f(EPS_0)
-    inv = tuple(one / np.asarray(e, dtype) for e in material.eps)
+    # (per-site coefficient programs carry no material: only ``coeffs`` is read)
+    inv = tuple(one / np.asarray(e, dtype) for e in material.eps) if material is not None else (None,) * 3
     new_psi = list(psi_e) if psi_e else []
     if e_terms:
         corrected = []

@@ -40,7 +40,12 @@ def oracle_program(spec, dtype=np.float32) -> O.OracleProgram:
                            metrics=spec.metrics.as_dict() if spec.metrics is not None else None,
                            recorders=[O.FieldRecorder(r.components, r.interval, r.capacity, r.indices, r.weights,
                                                       r.signs) for r in spec.recorders])
-    if spec.ndim == 3:
+    if spec.ndim == 3 and spec.voxel_ids is None:
+        # Per-site coefficients (beamz's CUDA-path form, cuda/src/update.cu:392-410):
+        # E <- decay E + source curl, H <- decay H - source curl.
+        prog.e_coeffs = {c: (np.asarray(d, dtype), np.asarray(s, dtype)) for c, (d, s) in spec.e_site.items()}
+        prog.h_coeffs_3d = {c: (np.asarray(d, dtype), np.asarray(s, dtype)) for c, (d, s) in spec.h_coefficients().items()}
+    elif spec.ndim == 3:
         eps = np.asarray(spec.eps_table, np.float32)[spec.voxel_ids]
         prog.material = O.material_from_voxels(eps, dtype=dtype)
     else:

@@ -20,7 +20,13 @@ from typing import Any, NamedTuple
 
 from . import _jaxshim
 
-REFERENCE_ROOT = os.environ.get("BEAMZ_REFERENCE_ROOT", "/root/reference")
+
+def reference_root() -> str:
+    """The beamz source tree: BEAMZ_REFERENCE_ROOT (the scripts set it from --reference)."""
+    root = os.environ.get("BEAMZ_REFERENCE_ROOT")
+    if not root:
+        raise RuntimeError("set BEAMZ_REFERENCE_ROOT (or pass --reference) to the root of the beamz source tree")
+    return root
 
 
 def _package(name: str, path: str | None = None) -> types.ModuleType:
@@ -35,7 +41,7 @@ def _package(name: str, path: str | None = None) -> types.ModuleType:
 def _load(name: str, relpath: str) -> types.ModuleType:
     if name in sys.modules and getattr(sys.modules[name], "__file__", None):
         return sys.modules[name]
-    path = os.path.join(REFERENCE_ROOT, relpath)
+    path = os.path.join(reference_root(), relpath)
     spec = importlib.util.spec_from_file_location(name, path)
     module = importlib.util.module_from_spec(spec)
     sys.modules[name] = module
@@ -69,7 +75,7 @@ class CpmlTerm:
 def load_reference():
     """Return a namespace with the reference modules the fixtures exercise."""
     _jaxshim.install()
-    root = REFERENCE_ROOT
+    root = reference_root()
     _package("beamz", os.path.join(root, "beamz"))
     _package("beamz.simulation", os.path.join(root, "beamz/simulation"))
     _package("beamz.devices", os.path.join(root, "beamz/devices"))

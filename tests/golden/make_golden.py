@@ -429,10 +429,12 @@ def gen_steps3d(ref, nsteps=16):
 
 def main():
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default=None)
+    parser.add_argument("--reference", default=os.environ.get("BEAMZ_REFERENCE_ROOT"),
+                        help="root of the beamz source tree (or set BEAMZ_REFERENCE_ROOT)")
     args = parser.parse_args()
-    if args.reference:
-        os.environ["BEAMZ_REFERENCE_ROOT"] = args.reference
+    if not args.reference:
+        parser.error("--reference (or BEAMZ_REFERENCE_ROOT) is required")
+    os.environ["BEAMZ_REFERENCE_ROOT"] = args.reference
     from ._refload import load_reference
 
     ref = load_reference()

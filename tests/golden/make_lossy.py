@@ -31,9 +31,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("BEAMZ_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("BEAMZ_REFERENCE_ROOT"),
+                    help="root of the beamz source tree (or set BEAMZ_REFERENCE_ROOT)")
     ap.add_argument("--out", default=os.path.join(HERE, "lossy.npz"))
     args = ap.parse_args(argv)
+    if not args.reference:
+        ap.error("--reference (or BEAMZ_REFERENCE_ROOT) is required")
     os.environ["BEAMZ_REFERENCE_ROOT"] = args.reference
     from ._refload import load_reference
 

@@ -101,9 +101,12 @@ def diagnostics_case(fns, rng, grid, polarization, res, nan=False):
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("BEAMZ_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("BEAMZ_REFERENCE_ROOT"),
+                    help="root of the beamz source tree (or set BEAMZ_REFERENCE_ROOT)")
     ap.add_argument("--out", default=os.path.join(HERE, "termination.npz"))
     args = ap.parse_args(argv)
+    if not args.reference:
+        ap.error("--reference (or BEAMZ_REFERENCE_ROOT) is required")
     fns = load_functions(args.reference)
     rng = np.random.default_rng(2024)
     out = {}
