@@ -21,7 +21,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_fdtd_b200.so")
-SOURCES = ("phase.cu", "fused.cu", "fused3d.cu", "fused_tma.cu", "fast_tma.cu", "io.cu", "adjoint.cu", "diag.cu", "planner.cu", "analysis.cu", "recorder.cu", "program.cu")
+SOURCES = ("phase.cu", "fused.cu", "fused3d.cu", "fused_tma.cu", "class_step.cu", "io.cu", "adjoint.cu", "diag.cu", "planner.cu", "analysis.cu", "recorder.cu", "program.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

@@ -28,7 +28,6 @@
 // mu * curl'_n per E site over a design box, mu = the masked E adjoint and
 // curl'_n the forward curl recomputed from a checkpoint.
 
-#include <mutex>
 
 #include "kernels.cuh"
 
@@ -318,25 +317,15 @@ static __device__ __align__(256) float g_adjoint_scratch[FDTD_ADJOINT_NOALLOC_MA
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-
-// Device address of g_adjoint_scratch on the current device, looked up once
-// per device with that device current.
+// Device address of g_adjoint_scratch on the current device.  Looked up on
+// every call (a cheap runtime query) rather than cached, so that the address
+// stays right after the device's context is torn down and re-created (the
+// module, and with it the array, may then sit elsewhere).
 cudaError_t adjoint_scratch_address(float** out) {
-  static std::mutex mu;
-  static float* addr[kMaxDevices] = {};
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t err = cudaGetSymbolAddress(&p, g_adjoint_scratch);
   if (err != cudaSuccess) return err;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(mu);
-  if (addr[dev] == nullptr) {
-    void* p = nullptr;
-    err = cudaGetSymbolAddress(&p, g_adjoint_scratch);
-    if (err != cudaSuccess) return err;
-    addr[dev] = static_cast<float*>(p);
-  }
-  *out = addr[dev];
+  *out = static_cast<float*>(p);
   return cudaSuccess;
 }
 
@@ -346,6 +335,12 @@ int64_t adjoint_noalloc_span(int64_t floats) { return (floats + 63) / 64 * 64; }
 
 cudaError_t launch_adjoint_step_noalloc(cudaStream_t s, const Step3D& p, const DftDev* dft, AdjDev a, int active,
                                         int step, const int64_t e_len[6], const int64_t h_len[6]) {
+  int64_t need = 0;
+  for (int t = 0; t < 6; ++t) {
+    need += e_len[t] > 0 ? adjoint_noalloc_span(e_len[t]) : 0;
+    need += h_len[t] > 0 ? adjoint_noalloc_span(h_len[t]) : 0;
+  }
+  if (need > FDTD_ADJOINT_NOALLOC_MAX_FLOATS) return cudaErrorInvalidValue;  // before any work
   float* base = nullptr;
   const cudaError_t err = adjoint_scratch_address(&base);
   if (err != cudaSuccess) return err;
@@ -358,7 +353,6 @@ cudaError_t launch_adjoint_step_noalloc(cudaStream_t s, const Step3D& p, const D
     a.scratch_h[t] = h_len[t] > 0 ? base + off : nullptr;
     off += h_len[t] > 0 ? adjoint_noalloc_span(h_len[t]) : 0;
   }
-  if (off > FDTD_ADJOINT_NOALLOC_MAX_FLOATS) return cudaErrorInvalidValue;
   return launch_adjoint_step(s, p, dft, a, active, step);
 }
 

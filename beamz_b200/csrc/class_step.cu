@@ -1,8 +1,11 @@
-// Tolerance-mode 3D leapfrog step on the pitched field layout (FDTD_FLAG_CLASSES).
+// The class step: one launch per 3D leapfrog step on the pitched field layout,
+// with the E material as one uint8 class per lattice point
+// (FDTD_FLAG_CLASSES).  The engine's 3D hot path.
 //
-// Same schedule as the bit-exact kernel in fused_tma.cu (one launch per step,
-// z-marching CTAs, TMA-staged planes on an mbarrier ring, recomputed H halo),
-// re-shaped so that a thread does four cells per plane instead of one:
+// Same schedule as the codebook kernel in fused_tma.cu (z-marching CTAs,
+// TMA-staged planes on an mbarrier ring, a recomputed H halo so that no CTA
+// waits on another), re-shaped so that a thread updates four cells per plane
+// instead of one:
 //
 //  * a CTA of NW warps owns a 128 x NW tile of (x, y) lattice points; lane l of
 //    warp w owns x = i0 + 4l .. 4l + 3 on row j = j0 + w, so every shared and
@@ -11,26 +14,29 @@
 //    the staged box); the y neighbour of the H update is the next staged row,
 //    that of the E update the row above in the new-H plane; H of the previous
 //    plane stays in registers;
-//  * every spatial difference is left unscaled: 1/dx is folded into the update
-//    coefficients (dt/(mu0 dx) for H, dt/(eps0 eps dx) per material class for
-//    E) and into the CPML 'a' coefficient, and products are contracted into
-//    FMAs.  Relative to beamz's float32 path (divide each difference by dx,
-//    then scale) this rounds differently within a few ulp per step; parity is
-//    a tolerance (fields 1e-5 relative L2 after the run), not bit equality;
-//  * the electric material is one uint8 class id per lattice point (the class
-//    being the (Ex, Ey, Ez) coefficient triple), 1 byte per cell instead of a
-//    4-byte codebook word, with the class table in shared memory.
+//  * the E material is one uint8 class id per lattice point (a class is one
+//    (Ex, Ey, Ez) coefficient triple of the codebook), 1 byte per cell instead
+//    of a 4-byte codebook word, with the class table in shared memory;
+//  * the CPML memories of an x-slab are addressed through per-lane slab masks
+//    computed once per CTA, every psi load of a plane is issued before its
+//    first use, and the next plane's psi is prefetched into L2.
+//
+// Arithmetic: beamz's float32 order bit for bit (every difference divided by
+// the cell size with a correctly rounded quotient, every product and sum
+// rounded separately; this file is compiled with -fmad=false).  With
+// FDTD_FLAG_FAST_MATH instead the tolerance form: 1/dx folded into the
+// coefficients (dt/(mu0 dx) for H, dt/(eps0 eps dx) per class for E, a/dx for
+// the CPML) and explicit fused multiply-adds.
 //
 // Tile-planes that touch a high domain face, a z face, an H source or a
 // partial tile run a general per-cell path with every validity, ghost and PEC
 // rule; the rest run one of six straight bodies chosen by the absorber axes
-// they touch (as the exact kernel).  ψ of the CPML terms is read and written
-// with plain loads; the H-term memories are double-banked (the halo
+// they touch.  The H-term CPML memories are double-banked (the halo
 // recomputation reads them), the E-term ones updated in place.
 //
-// Operation order otherwise follows beamz/simulation/kernels.py:458-626 (H
-// from E with CPML, H sources, H PEC; E from ghost-padded H with CPML, E PEC)
-// and beamz/simulation/execute.py:467-522.
+// Operation order follows beamz/simulation/kernels.py:458-626 (H from E with
+// CPML, H sources, H PEC; E from ghost-padded H with CPML, E PEC) and
+// beamz/simulation/execute.py:467-522.
 
 #include <cuda.h>
 
@@ -47,7 +53,7 @@ constexpr int kSlots = 32;  // CPML coefficient slots staged per term
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int NW>
-struct FastTile {
+struct ClassTile {
   static constexpr int TX = 128, TY = NW, NT = 32 * NW;
   static constexpr int BX = TX + 8;  // staged row: x from i0-4 to i0+131 (16-byte aligned start)
   static constexpr int EH = TY + 2;  // E rows j0-1 .. j0+TY
@@ -62,13 +68,14 @@ struct FastTile {
     alignas(128) uint8_t ids[2][IBOX];
     alignas(16) float hn[3][HH][BX];   // H (new) of this plane: own rows + halo row, own columns + halo column
     float4 cls[256];                   // per class: dt/(eps0 eps dx) of Ex, Ey, Ez
-    float4 cc[12][kSlots];  // CPML (a/dx, b, 1/kappa): H terms 0-5, E terms 6-11
+    float4 cc[12][kSlots];  // CPML (a, b, 1/kappa) (a/dx in the tolerance form): H terms 0-5, E terms 6-11
+    float xd[2][TY][32];    // corrected x differences of a row's x-slab cells by slot (compact x work)
     float amp[kMaxFusedSources];
     unsigned long long bar[2];
   };
 };
 
-struct FastMaps {
+struct ClassMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
   CUtensorMap ids;
@@ -241,6 +248,57 @@ __device__ __forceinline__ float4 psix_apply(const CpmlTermDev& t, const float4*
   return make_float4(r[0], r[1], r[2], r[3]);
 }
 
+// The own cells' x differences with the slab cells replaced by their corrected
+// values from the compact x work (`slots`: the row's corrected differences by
+// slab slot; the slots of the own cells are consecutive from xs >> 4).
+__device__ __forceinline__ float4 xtake(float4 d, int xs, const float* slots) {
+  if (!(xs & 15)) return d;
+  float r[4] = {d.x, d.y, d.z, d.w};
+  const int base = xs >> 4;
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    if (xs & (1 << c)) r[c] = slots[base + c];
+  return make_float4(r[0], r[1], r[2], r[3]);
+}
+
+// The compact x work's items of one x term in a tile: its slab slots whose x
+// lies in [i0, i1) (at most two runs: the low and the high slab).  Item q maps
+// to a slot and an x; returns false past the last item.
+struct XItems {
+  int lo_n, hi_s, hi_n, hi_x;  // low run: slots [0.., lo_n) at x = slot + lo_x0
+  int lo_s, lo_x;
+  __device__ __forceinline__ bool item(int q, int* slot, int* x) const {
+    if (q < lo_n) {
+      *slot = lo_s + q;
+      *x = lo_x + q;
+      return true;
+    }
+    q -= lo_n;
+    if (q < hi_n) {
+      *slot = hi_s + q;
+      *x = hi_x + q;
+      return true;
+    }
+    return false;
+  }
+};
+
+__device__ __forceinline__ XItems x_items(const CpmlTermDev& t, int i0, int i1) {
+  XItems r{};
+  // low slab: x = slot in [0, low)
+  const int lb = max(0, i0), le = min(t.low, i1);
+  r.lo_n = max(0, le - lb);
+  r.lo_s = lb;
+  r.lo_x = lb;
+  // high slab: x in [n - high, n), slot = low + x - (n - high)
+  const int hx0 = t.n_axis - t.high;
+  const int hb = max(hx0, i0), he = min(t.n_axis, i1);
+  r.hi_n = t.high > 0 ? max(0, he - hb) : 0;
+  r.hi_s = t.low + hb - hx0;
+  r.hi_x = hb;
+  return r;
+}
+
 // One scalar cell of a term: psi fetched ahead (0 outside the slab), then applied.
 template <int Axis>
 __device__ __forceinline__ float psi1_fetch(const CpmlTermDev& t, int k, int j, int i) {
@@ -324,8 +382,8 @@ __device__ __forceinline__ float ghost_diff(float center, float below, int v, in
 // 8-warp CTAs: two per SM (shared memory), 128 registers; 4-warp CTAs: four.
 template <int NW, bool Cpml, bool Exact>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
-    fast_step_kernel(const __grid_constant__ FastMaps maps, const __grid_constant__ Step3D p) {
-  using T = FastTile<NW>;
+    class_step_kernel(const __grid_constant__ ClassMaps maps, const __grid_constant__ Step3D p) {
+  using T = ClassTile<NW>;
   using S = typename T::Smem;
   constexpr int BX = T::BX, TX = T::TX, TY = T::TY, XC = T::XC;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -400,7 +458,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const bool xcol = X % TX == 0 && i0 + TX == X;
   const bool xl = xcol && lane == 31;
   const int xe = xcol ? 1 : 0;
-  const bool fast_ok = j0 + TY <= Y && i0 + TX <= X && cc_smem;
+  const bool fast_ok0 = j0 + TY <= Y && i0 + TX <= X && cc_smem;
   const bool xface = i0 == 0, yface = j0 == 0;
   const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
@@ -413,6 +471,27 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     xe3 = xslab_of(p.et[3], i);
     xe4 = xslab_of(p.et[4], i);
   }
+
+  // Compact x work: in a tile that touches an x slab, the recurrences of a
+  // row's x-slab cells are shared by the row's warp -- lanes 0-15 take the
+  // first x term of the phase (Hyx, Eyx), lanes 16-31 the second (Hzx, Ezx),
+  // one cell each -- instead of falling on the few lanes that own slab cells;
+  // the corrected differences reach the owners through shared memory.  Per x
+  // term: the first slab x in this tile and the run length (one contiguous
+  // run of at most 16 cells; otherwise the owners' per-lane path runs).
+  // The compact x work covers slabs of at most 32 slots per term (wider ones
+  // take the general path); each lane takes items lane and lane + 32 of the
+  // row's (term, slot) list: the first x term's slots, then the second's.
+  const bool xcompact = ax && p.ht[3].low + p.ht[3].high <= 32 && p.ht[4].low + p.ht[4].high <= 32 &&
+                        p.et[3].low + p.et[3].high <= 32 && p.et[4].low + p.et[4].high <= 32;
+  // The lane's x-slab psi of the next plane, loaded a plane ahead (H and E
+  // terms, items lane and lane + 32).
+  float xq_h0 = 0.0f, xq_h1 = 0.0f, xq_e0 = 0.0f, xq_e1 = 0.0f;
+  int xq_kh = -1, xq_ke = -1;  // the planes they belong to
+
+  const bool fast_ok = fast_ok0 && (!ax || xcompact);
+  // Column X is lane 31's own work, so the items stop short of it.
+  const int xi1 = i0 + TX;
 
   // H of the previous plane on the own cells (the z-backward differences of E).
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
@@ -462,7 +541,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         // Class id of column X (lane 31 of the last tile).
         const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
         // psi of the H terms: own cells, halos, column X.
-        float4 qh0, qh1, qh2, qh3, qh4, qh5;
+        float4 qh0, qh1, qh2, qh5;
         if constexpr (AY) {
           qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
           qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
@@ -471,9 +550,28 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
-        if constexpr (AX) {
-          qh3 = psix_fetch(p.ht[3], xs3, k, j);
-          qh4 = psix_fetch(p.ht[4], xs4, k, j);
+        // The halos' psi (read only), in flight during the own-row H update:
+        // row j0-1 (warp 0: Hxy, Hxz, and column X's; warp 1: Hzx, Hzy) and
+        // column i0-1 (warp 2: Hyz, Hyx, Hzx, Hzy in qa.x-w).
+        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
+        float qR0 = 0.f, qR1 = 0.f;
+        if constexpr (AX || AY || AZ) {
+          if (halo_row_x) {
+            if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
+            if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
+            if (xl) {
+              if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
+              if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
+            }
+          } else if (halo_row_z) {
+            if constexpr (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
+            if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
+          } else if (halo_col) {
+            if constexpr (AZ) qa.x = psi1_fetch<0>(p.ht[2], k, jc, ih);
+            if constexpr (AX) qa.y = psi1_fetch<2>(p.ht[3], k, jc, ih);
+            if constexpr (AX) qa.z = psi1_fetch<2>(p.ht[4], k, jc, ih);
+            if constexpr (AY) qa.w = psi1_fetch<1>(p.ht[5], k, jc, ih);
+          }
         }
         // Next plane's psi (and column X's class id) into L2, a plane ahead of use.
         if (k + 1 < k1) {
@@ -490,12 +588,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               psi_prefetch<1>(p.et[0], kn, j, i);
               psi_prefetch<1>(p.et[5], kn, j, i);
             }
-            if constexpr (AX) {
-              psix_prefetch(p.ht[3], xs3, kn, j);
-              psix_prefetch(p.ht[4], xs4, kn, j);
-              psix_prefetch(p.et[3], xe3, kn, j);
-              psix_prefetch(p.et[4], xe4, kn, j);
-            }
             // The halos' (read-only) psi of the next plane.
             if (warp == 0 && !at_y0) {
               if constexpr (AY) psi_prefetch<1>(p.ht[0], kn, jh, i);
@@ -503,8 +595,40 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             } else if (warp == 1 && !at_y0) {
               if constexpr (AX) psix_prefetch(p.ht[4], xs4, kn, jh);
               if constexpr (AY) psi_prefetch<1>(p.ht[5], kn, jh, i);
+            } else if (warp == 2 && lane < TY && !at_x0) {
+              const int slot2 = slot_of(p.ht[2], kn);
+              if (slot2 >= 0) l2_prefetch(p.ht[2].psi_in + psi_off<0>(p.ht[2], slot2, kn, jc, ih));
+              if constexpr (AY) {
+                const int slot5 = slot_of(p.ht[5], jc);
+                if (slot5 >= 0) l2_prefetch(p.ht[5].psi_in + psi_off<1>(p.ht[5], slot5, kn, jc, ih));
+              }
             }
           }
+        }
+        // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
+        if constexpr (AX) {
+          const XItems it3 = x_items(p.ht[3], i0, xi1), it4 = x_items(p.ht[4], i0, xi1);
+          const int n3 = it3.lo_n + it3.hi_n;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int q = lane + 32 * h;
+            const bool second = q >= n3;  // Hzx (dEy/dx), else Hyx (dEz/dx)
+            int slot, x;
+            if ((second ? it4 : it3).item(second ? q - n3 : q, &slot, &x)) {
+              const CpmlTermDev& d = second ? p.ht[4] : p.ht[3];
+              const float* Erow = second ? E0y : E0z;
+              const int b = r * BX + 4 + (x - i0);
+              const int off = (k * d.pdy + j) * d.pdx + slot;
+              const float psi = xq_kh == k ? (h ? xq_h1 : xq_h0) : d.psi_in[off];
+              if (k + 1 < k1) (h ? xq_h1 : xq_h0) = d.psi_in[off + d.pdy * d.pdx];  // the next plane's, in flight
+              float nv;
+              const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
+              if (emit) d.psi_out[off] = nv;
+              sm.xd[second ? 1 : 0][warp][slot] = dp;
+            }
+          }
+          xq_kh = k + 1;
+          __syncwarp();
         }
         // ---- H on the own row ----
         float4 dx0, dx1, dy0, dy1, dz0, dz1;
@@ -528,8 +652,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
         }
         if constexpr (AX) {
-          dy1 = psix_apply<Exact>(p.ht[3], sm.cc[3], xs3, qh3, k, j, res, dy1, emit);
-          dz0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qh4, k, j, res, dz0, emit);
+          dy1 = xtake(dy1, xs3, sm.xd[0][warp]);
+          dz0 = xtake(dz0, xs4, sm.xd[1][warp]);
         }
         float4 hx = h4<Exact>(ld4(HOx + rc), dec0, s0, dx0, dx1);
         float4 hy = h4<Exact>(ld4(HOy + rc), dec1, s1, dy0, dy1);
@@ -563,14 +687,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
         if (halo_row_x) {
           const int b = c0;
-          float4 qa, qb;
-          float qR0 = 0.f, qR1 = 0.f;
-          if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
-          if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
-          if (xl) {
-            if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
-            if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
-          }
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
           if constexpr (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
           if constexpr (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
@@ -586,9 +702,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           }
         } else if (halo_row_z) {
           const int b = c0;
-          float4 qa, qb;
-          if constexpr (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
-          if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
           if (lane == 31) e4 = E0y[b + 4];
@@ -598,11 +711,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), dec2, s2, d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
-          float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f;
-          if constexpr (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
-          if constexpr (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
-          if constexpr (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
-          if constexpr (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
+          const float qc0 = qa.x, qc1 = qa.y, qc2 = qa.z, qc3 = qa.w;
           float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
           if constexpr (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
           if constexpr (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
@@ -615,7 +724,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           sm.hn[2][rr][3] = h1<Exact>(HOz[b], dec2, s2, f0, f1);
         }
         // psi of the E terms, in flight during the barrier.
-        float4 qe0, qe1, qe2, qe3, qe4, qe5;
+        float4 qe0, qe1, qe2, qe5;
         float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
         if (emit) {
           if constexpr (AY) {
@@ -625,10 +734,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if constexpr (AZ) {
             qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
             qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
-          }
-          if constexpr (AX) {
-            qe3 = psix_fetch(p.et[3], xe3, k, j);
-            qe4 = psix_fetch(p.et[4], xe4, k, j);
           }
           if (xl) {
             if constexpr (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
@@ -643,6 +748,33 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           hyp = hy;
           hxXp = hxX;
           return;
+        }
+        // ---- compact x work of the E terms (Eyx, Ezx) on this warp's row ----
+        if constexpr (AX) {
+          const XItems it3 = x_items(p.et[3], i0, xi1), it4 = x_items(p.et[4], i0, xi1);
+          const int n3 = it3.lo_n + it3.hi_n;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int q = lane + 32 * h;
+            const bool second = q >= n3;  // Ezx (dHy/dx), else Eyx (dHz/dx)
+            int slot, x;
+            if ((second ? it4 : it3).item(second ? q - n3 : q, &slot, &x)) {
+              const CpmlTermDev& d = second ? p.et[4] : p.et[3];
+              const float* Hrow = second ? sm.hn[1][r] : sm.hn[2][r];
+              const int c = 4 + (x - i0);
+              // Beyond x = 0 the ghost: zero on a metallic wall, else the edge value.
+              const float dv = (at_x0 && x == 0) ? (wx0 ? Hrow[c] : 0.0f) : Hrow[c] - Hrow[c - 1];
+              const int off = (k * d.pdy + j) * d.pdx + slot;
+              const float psi = xq_ke == k ? (h ? xq_e1 : xq_e0) : d.psi_in[off];
+              if (k + 1 < k1) (h ? xq_e1 : xq_e0) = d.psi_in[off + d.pdy * d.pdx];
+              float nv;
+              const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
+              d.psi_out[off] = nv;
+              sm.xd[second ? 1 : 0][warp][slot] = dp;
+            }
+          }
+          xq_ke = k + 1;
+          __syncwarp();
         }
         // ---- E on the own row ----
         float4 hzy = ld4(&sm.hn[2][r - 1][c0]), hxy = ld4(&sm.hn[0][r - 1][c0]);
@@ -671,8 +803,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
         }
         if constexpr (AX) {
-          fy1 = psix_apply<Exact>(p.et[3], sm.cc[9], xe3, qe3, k, j, res, fy1, true);
-          fz0 = psix_apply<Exact>(p.et[4], sm.cc[10], xe4, qe4, k, j, res, fz0, true);
+          fy1 = xtake(fy1, xe3, sm.xd[0][warp]);
+          fz0 = xtake(fz0, xe4, sm.xd[1][warp]);
         }
         const float4 ex = ld4(E0x + rc), ey = ld4(E0y + rc), ez = ld4(E0z + rc);  // E(k) of the own cells
         const uint32_t w4 = *reinterpret_cast<const uint32_t*>(IDS + warp * TX + 4 * lane);
@@ -851,10 +983,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 }
 
 template <int NW, bool Cpml, bool Exact>
-cudaError_t launch_fast_t(cudaStream_t s, const FastMaps& maps, const Step3D& p) {
-  using T = FastTile<NW>;
+cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
+  using T = ClassTile<NW>;
   const size_t smem = sizeof(typename T::Smem);
-  auto kern = fast_step_kernel<NW, Cpml, Exact>;
+  auto kern = class_step_kernel<NW, Cpml, Exact>;
   int device = 0;
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess) return err;
@@ -873,9 +1005,9 @@ cudaError_t launch_fast_t(cudaStream_t s, const FastMaps& maps, const Step3D& p)
 }
 
 template <int NW>
-cudaError_t launch_fast_shape(cudaStream_t s, const Step3D& p) {
-  using T = FastTile<NW>;
-  FastMaps maps;
+cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
+  using T = ClassTile<NW>;
+  ClassMaps maps;
   const int64_t P = p.pitch, rowb = P * 4, planeb = static_cast<int64_t>(p.Y + 1) * P * 4;
   for (int c = 0; c < 3; ++c) {
     const Dims de = component_dims(c, p.Z, p.Y, p.X), dh = component_dims(c + 3, p.Z, p.Y, p.X);
@@ -889,15 +1021,15 @@ cudaError_t launch_fast_shape(cudaStream_t s, const Step3D& p) {
   if (!tma::encode(&maps.ids, CU_TENSOR_MAP_DATA_TYPE_UINT8, p.site_class, p.X + 1, p.Y + 1, p.Z + 1, P8,
                    P8 * (p.Y + 1), T::TX, T::TY))
     return cudaErrorInvalidValue;
-  if (p.fast_math) return p.cpml ? launch_fast_t<NW, true, false>(s, maps, p) : launch_fast_t<NW, false, false>(s, maps, p);
-  return p.cpml ? launch_fast_t<NW, true, true>(s, maps, p) : launch_fast_t<NW, false, true>(s, maps, p);
+  if (p.fast_math) return p.cpml ? launch_class_t<NW, true, false>(s, maps, p) : launch_class_t<NW, false, false>(s, maps, p);
+  return p.cpml ? launch_class_t<NW, true, true>(s, maps, p) : launch_class_t<NW, false, true>(s, maps, p);
 }
 
 }  // namespace
 
 // tile_y: 8 (8 warps, 128 x 8 tiles) or 4 (4 warps, 128 x 4 tiles).
-cudaError_t launch_fast_tma(cudaStream_t s, const Step3D& p, int tile_y) {
-  return tile_y == 4 ? launch_fast_shape<4>(s, p) : launch_fast_shape<8>(s, p);
+cudaError_t launch_class_step(cudaStream_t s, const Step3D& p, int tile_y) {
+  return tile_y == 4 ? launch_class_shape<4>(s, p) : launch_class_shape<8>(s, p);
 }
 
 }  // namespace fdtd

@@ -132,7 +132,7 @@ cudaError_t launch_phase(cudaStream_t s, const Step3D& p, int phase, int mat, in
 cudaError_t launch_fused(cudaStream_t s, const Step3D& p, int mat, int active_mask, int tile_x, int tile_y);
 cudaError_t launch_fused_lean(cudaStream_t s, const Step3D& p, int mat, int tile_y);
 cudaError_t launch_fused_tma(cudaStream_t s, const Step3D& p, int tile_y);
-cudaError_t launch_fast_tma(cudaStream_t s, const Step3D& p, int tile_y);
+cudaError_t launch_class_step(cudaStream_t s, const Step3D& p, int tile_y);
 // `row`/`plane` are the target's element pitches (dense: dx and dy*dx).
 cudaError_t launch_source(cudaStream_t s, const SourceDev& src, float* target, Dims td, int64_t row,
                           int64_t plane, int timing, int metallic, const int* counter, int step_offset);

@@ -606,7 +606,7 @@ cudaError_t enqueue_program(cudaStream_t s, const FdtdProgram& p) {
       sp.n_esrc = n_esrc;
       for (int i = 0; i < n_esrc; ++i) sp.esrc[i] = esrc[i];
       if (p.layout == FDTD_LAYOUT_PITCHED && (p.flags & FDTD_FLAG_CLASSES)) {
-        err = launch_fast_tma(s, sp, p.tile_y);
+        err = launch_class_step(s, sp, p.tile_y);
       } else if (p.layout == FDTD_LAYOUT_PITCHED) {
         err = launch_fused_tma(s, sp, p.tile_y);
       } else if (L.active == kActive3D) {
@@ -888,6 +888,22 @@ int check_adjoint(const FdtdProgram& p, const FdtdAdjointStep& a, const Layout& 
   return 0;
 }
 
+// Elements of each derivative term's adjoint scratch (0 for a term between
+// inactive components): an E term's target E component, an H term's target H
+// component.  Both adjoint entry points size their scratch from this.
+void adjoint_term_lengths(const Layout& L, int64_t e_len[6], int64_t h_len[6]) {
+  for (int t = 0; t < 6; ++t) {
+    const int ec = kETermComp[t], hsrc = (t == 0 || t == 3) ? 5 : ((t == 1 || t == 4) ? 4 : 3);
+    e_len[t] = ((L.active >> ec) & 1) && ((L.active >> hsrc) & 1)
+                   ? dims_count(component_dims(ec, L.Z, L.Y, L.X))
+                   : 0;
+    const int hc = kHTermComp[t], esrc = (t == 0 || t == 3) ? 2 : ((t == 1 || t == 4) ? 1 : 0);
+    h_len[t] = ((L.active >> hc) & 1) && ((L.active >> esrc) & 1)
+                   ? dims_count(component_dims(hc, L.Z, L.Y, L.X))
+                   : 0;
+  }
+}
+
 AdjDev adjoint_dev(const FdtdProgram& p, const FdtdAdjointStep& a) {
   AdjDev d{};
   for (int c = 0; c < 6; ++c) d.lam[c] = static_cast<float*>(p.fields[c].data);
@@ -921,16 +937,12 @@ int fdtd_adjoint_step(void* stream, const FdtdProgram* adjoint, const FdtdAdjoin
   const int b = fdtd::check_adjoint(p, *a, L, false);
   if (b != 0) return b;
   // Every derivative term between two active components needs its scratch.
+  int64_t e_len[6], h_len[6];
+  fdtd::adjoint_term_lengths(L, e_len, h_len);
   for (int t = 0; t < 6; ++t) {
-    const int ec = fdtd::kETermComp[t], hsrc = (t == 0 || t == 3) ? 5 : ((t == 1 || t == 4) ? 4 : 3);
-    const bool e_live = ((L.active >> ec) & 1) && ((L.active >> hsrc) & 1);
-    if (e_live ? !fdtd::f32_sized(a->scratch_e[t], fdtd::dims_count(fdtd::component_dims(ec, L.Z, L.Y, L.X)))
-               : a->scratch_e[t].data != nullptr)
+    if (e_len[t] > 0 ? !fdtd::f32_sized(a->scratch_e[t], e_len[t]) : a->scratch_e[t].data != nullptr)
       return fdtd::kInvalid;
-    const int hc = fdtd::kHTermComp[t], esrc = (t == 0 || t == 3) ? 2 : ((t == 1 || t == 4) ? 1 : 0);
-    const bool h_live = ((L.active >> hc) & 1) && ((L.active >> esrc) & 1);
-    if (h_live ? !fdtd::f32_sized(a->scratch_h[t], fdtd::dims_count(fdtd::component_dims(hc, L.Z, L.Y, L.X)))
-               : a->scratch_h[t].data != nullptr)
+    if (h_len[t] > 0 ? !fdtd::f32_sized(a->scratch_h[t], h_len[t]) : a->scratch_h[t].data != nullptr)
       return fdtd::kInvalid;
   }
   const bool dft = p.dft.monitor_count > 0 && a->dft_grad_re.data != nullptr;
@@ -956,18 +968,11 @@ int fdtd_adjoint_step_noalloc(void* stream, const FdtdProgram* adjoint, const Fd
   fdtd::layout_of(p, &L);
   const int b = fdtd::check_adjoint(p, *a, L, false);
   if (b != 0) return b;
-  int64_t e_len[6] = {}, h_len[6] = {}, total = 0;
-  for (int t = 0; t < 6; ++t) {
+  int64_t e_len[6], h_len[6];
+  fdtd::adjoint_term_lengths(L, e_len, h_len);
+  for (int t = 0; t < 6; ++t)
     if (a->scratch_e[t].data != nullptr || a->scratch_h[t].data != nullptr) return fdtd::kInvalid;
-    const int ec = fdtd::kETermComp[t], hsrc = (t == 0 || t == 3) ? 5 : ((t == 1 || t == 4) ? 4 : 3);
-    if (((L.active >> ec) & 1) && ((L.active >> hsrc) & 1))
-      e_len[t] = fdtd::dims_count(fdtd::component_dims(ec, L.Z, L.Y, L.X));
-    const int hc = fdtd::kHTermComp[t], esrc = (t == 0 || t == 3) ? 2 : ((t == 1 || t == 4) ? 1 : 0);
-    if (((L.active >> hc) & 1) && ((L.active >> esrc) & 1))
-      h_len[t] = fdtd::dims_count(fdtd::component_dims(hc, L.Z, L.Y, L.X));
-    total += fdtd::adjoint_noalloc_span(e_len[t]) + fdtd::adjoint_noalloc_span(h_len[t]);
-  }
-  if (total > FDTD_ADJOINT_NOALLOC_MAX_FLOATS) return fdtd::kInvalid;
+  // The scratch bound is checked once, by the launcher, before any work is enqueued.
   const bool dft = p.dft.monitor_count > 0 && a->dft_grad_re.data != nullptr;
   fdtd::DftDev dd{};
   if (dft) {

@@ -41,7 +41,9 @@ def _dipole(component, site, eps_site, dt, total_steps, fwidth, offset, ndim=3):
 
 
 def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, monitors=True, sources=True,
-                 n_monitors=4, n_freqs=5):
+                 n_monitors=4, n_freqs=5, cpml_edges=None):
+    """``cpml_edges``: the faces with an absorber (default all six; an empty
+    tuple gives a closed box), for measuring the absorber's cost per axis."""
     nz, ny, nx = shape
     rng = np.random.default_rng(seed)
     dt = _dt(3, 0.99)
@@ -53,7 +55,10 @@ def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, 
         y0 = int(rng.integers(0, max(1, ny - sy)))
         x0 = int(rng.integers(0, max(1, nx - sx)))
         ids[z0:z0 + 11, y0:y0 + sy, x0:x0 + sx] = 1
-    h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells)
+    if cpml_edges is not None and len(cpml_edges) == 0:
+        h_terms, e_terms = [], []
+    else:
+        h_terms, e_terms = P.plan_cpml(shape, dt, RES, pml_cells=pml_cells, edges=cpml_edges)
     ids = P.extend_into_absorber(ids, P.absorber_edge_counts(shape, pml_cells, resolution=RES))
     table = np.ones(256, np.float32)
     table[0], table[1] = OXIDE, SI

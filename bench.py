@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--scene", default="3d_512", choices=["3d_512", "capacity", "2d_400"])
     ap.add_argument("--tile", default="32x8")
     ap.add_argument("--z-chunk", type=int, default=16)
+    ap.add_argument("--cpml-faces", choices=["all", "x", "y", "z", "none"], default="all",
+                    help="3d_512 only: the faces that carry the absorber (the absorber's cost per axis)")
+    ap.add_argument("--step-kernel", choices=["classes", "codebook"], default=None,
+                    help="pitched 3D step (default: the runtime's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel-steps", type=int, default=200)
@@ -53,6 +57,9 @@ def parse():
     ap.add_argument("--requests", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--adjoint", choices=["2d", "3d"], default=None, help="inverse design: forward + adjoint gradient")
+    ap.add_argument("--accuracy", choices=["reduced", "full"], default="reduced",
+                    help="accuracy key: a reduced copy of the scene against the FP32 and FP64 oracles (default), "
+                         "or the full 512x512x256 scene over all 1000 steps against the C restatement (minutes)")
     return ap.parse_args()
 
 
@@ -138,6 +145,15 @@ def cpu_sample(spec_fn, total_steps, budget_s, threads=0):
     return per_cell_step, nthreads
 
 
+def config_block(args, spec) -> dict:
+    """The workload description both arms print (the driver compares them)."""
+    scene = {"3d_512": "3d_512x512x256_cpml12_sibox_dipole_dft4x5", "capacity": "capacity_1536x1024x1024_cpml12",
+             "2d_400": "2d_400x400_tm_cpml20_strip_dft3"}[args.scene]
+    return {"workload": scene, "grid_zyx": [int(v) for v in spec.grid_shape], "cells": int(spec.cells),
+            "parallelism": f"replicas x{max(1, int(os.environ.get('WORLD_SIZE', '1')))}",
+            "l2": "inputs larger than L2 (two field banks of %.1f GB)" % (2 * 4 * 6 * spec.cells / 1e9)}
+
+
 def reference_arm(args, scene_fn, cells_full):
     """CPU restatement of the reference step: bounded z-slab samples per step."""
     from oracle import cpu_port
@@ -158,10 +174,9 @@ def reference_arm(args, scene_fn, cells_full):
         "impl": "reference", "metric": "GCUPS", "value": round(gcups, 4), "unit": "Gcell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "3d_512x512x256_cpml12_sibox_dipole_dft4x5", "cells": cells_full,
-                   "sample_cells": spec.cells, "threads": nthreads},
+        "config": config_block(args, scene_fn(total_steps=1, monitors=False, sources=False)),
         "cpu_baseline": {"value": round(gcups, 4), "unit": "Gcell-updates/s", "cores": nthreads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "sample_cells": spec.cells},
         "e2e": {"value": round(gcups, 4), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -328,6 +343,45 @@ def accuracy_report(dev) -> dict:
     return report
 
 
+def accuracy_full(dev, step_kernel: str) -> dict:
+    """The 512 x 512 x 256 workload over its full 1000 steps from zero fields
+    (the dipole pulse and the 4 x 5 DFT planes) against the C restatement of
+    the reference's float32 step on every host thread: the largest
+    per-component relative L2 error of the fields and of the DFT arena.  The
+    float64 error is the reduced case's (no float64 restatement runs this size
+    in bounded time)."""
+    from beamz_b200 import plan as P
+    from beamz_b200 import runtime as R
+    from beamz_b200 import workloads as W
+    from oracle import cpu_port
+    from oracle import fdtd_oracle as O
+
+    steps = 1000
+    spec = W.scene_3d_512(total_steps=steps)
+    prog = R.compile_program(spec, device=dev, step_kernel=step_kernel)
+    out = R.run_steps(R.initial_state(prog), prog, steps).numpy()
+    del prog
+    import torch
+
+    torch.cuda.empty_cache()
+    cpu_port.build()
+    t0 = time.perf_counter()
+    ref = cpu_port.HostRun(spec).run(steps, threads=0)
+    cpu_s = time.perf_counter() - t0
+    fields = {c: O.relative_l2(out[c], ref.fields[c]) for c in P.COMPONENTS}
+    report = {"case": "512x512x256 scene (CPML 12, Si boxes, Ey dipole pulse, 4 DFT planes x 5 f), "
+                      f"{steps} steps from zero fields, against the C restatement (float32)",
+              "steps": steps, "fields_rel_l2_fp32": float(max(fields.values())),
+              "fields_rel_l2_fp32_per_component": {c: float(v) for c, v in fields.items()},
+              "fields_bit_identical_fp32": bool(all(np.array_equal(out[c], ref.fields[c]) for c in P.COMPONENTS)),
+              "dft_rel_l2_fp32": float(max(O.relative_l2(out["dft_re"], ref.dft_re),
+                                           O.relative_l2(out["dft_im"], ref.dft_im))),
+              "dft_weights_equal": bool(np.array_equal(out["dft_w"], ref.dft_w)),
+              "reference_cpu_s": round(cpu_s, 1), "step_kernel": step_kernel}
+    report["reduced_fp64"] = accuracy_report(dev)
+    return report
+
+
 def main():
     args = parse()
     import torch
@@ -371,8 +425,12 @@ def main():
     primes = 1 if args.steps % 2 == 0 else 2
     total = args.warmup + (primes + 2) * args.steps
     shape_kw = {"shape": tuple(int(v) for v in args.shape.split("x"))} if args.shape else {}
+    if args.scene == "3d_512" and args.cpml_faces != "all":
+        shape_kw["cpml_edges"] = {"x": ("left", "right"), "y": ("bottom", "top"), "z": ("front", "back"),
+                                  "none": ()}[args.cpml_faces]
     spec = scene_fn(total_steps=total, **shape_kw)
-    prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
+    sk = {"step_kernel": args.step_kernel} if args.step_kernel else {}
+    prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
     state = R.initial_state(prog)
     stream = torch.cuda.current_stream(dev)
 
@@ -417,7 +475,7 @@ def main():
     # ---- dominant kernel alone: the fused step without sources or monitors ---
     if args.scene == "3d_512":
         kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw)
-        kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk)
+        kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
         kstate = R.initial_state(kprog)
     else:  # other scenes time their own step (a second copy of the 1.6 G-cell scene would not fit)
         kprog, kstate = prog, state
@@ -494,7 +552,7 @@ def main():
         cpu = {"value": round(cspec.cells * 5 / cdt / 1e9, 4), "unit": "Gcell-updates/s", "cores": nthreads,
                "kind": "port",
                "sample": f"5 steps of a {nz}x512x512 z-slab of the scene, C restatement (OpenMP, {nthreads} threads)"}
-        accuracy = accuracy_report(dev)
+        accuracy = accuracy_full(dev, prog.step_kernel) if args.accuracy == "full" else accuracy_report(dev)
 
     if rank == 0:
         line = {
@@ -502,13 +560,13 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded voxels, beamz-style workload)",
-            "config": {"workload": f"{args.scene}" + ("_cpml12_sibox_dipole_dft4x5" if args.scene == "3d_512" else ""),
-                       "grid_zyx": list(spec.grid_shape), "cells": cells, "schedule": "fused", "tile": list(tile),
-                       "z_chunk": args.z_chunk, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (two field banks of %.1f GB)" % (2 * 4 * 6 * cells / 1e9)},
+            "config": config_block(args, spec),
+            "launch": {"schedule": "fused", "step_kernel": prog.step_kernel, "arithmetic": prog.arithmetic,
+                       "tile": list(tile), "z_chunk": args.z_chunk},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "tma_step_kernel" if prog.layout == "pitched" else "fused step", "kernel_ms": round(kernel_ms, 4),
+                         "kernel": {"classes": "class_step_kernel", "codebook": "tma_step_kernel"}.get(
+                             prog.step_kernel, "fused step"), "kernel_ms": round(kernel_ms, 4),
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
             "peak_hbm_gb": round(peak_hbm / 1e9, 2),
             "accuracy": accuracy,

@@ -1,4 +1,6 @@
-"""fdtd_adjoint_step_noalloc against fdtd_adjoint_step (collected last)."""
+"""fdtd_adjoint_step_noalloc against fdtd_adjoint_step (collected last):
+bit for bit over two consecutive adjoint steps, on a 2D TM program and on a
+3D program with CPML on every face and a DFT plane."""
 
 from __future__ import annotations
 
@@ -45,15 +47,32 @@ def _step(prog, n, scratch, g):
     return a
 
 
-def test_noalloc_adjoint_step_matches_the_allocating_entry_point():
+def _spec(kind):
+    if kind == "2d":
+        spec = W.scene_2d(total_steps=64, seed=9, shape=(72, 80), pml_cells=6, n_monitors=2)
+        return dataclasses.replace(spec, metallic_edges=frozenset({"bottom", "right"}))
+    # 3D: all twelve derivative terms live, CPML on every axis (psi transposed
+    # on all three), Ex/Ey/Ez of different extents, a DFT plane.
+    import torch
+
+    from beamz_b200 import adjoint as AD
+
+    spec = W.scene_3d_512(total_steps=64, seed=3, shape=(22, 24, 26), pml_cells=4, n_monitors=1, n_freqs=3)
+    eps = torch.as_tensor(np.asarray(spec.eps_table, np.float32)[spec.voxel_ids])
+    coefs = AD.eps_to_coefficients_3d(eps, spec.dt, P.EPS_0)
+    spec = AD.site_spec(spec, {c: v.cpu().numpy() for c, v in zip(("Ex", "Ey", "Ez"), coefs)})
+    return dataclasses.replace(spec, metallic_edges=frozenset({"front"}))
+
+
+@pytest.mark.parametrize("kind", ["2d", "3d"])
+def test_noalloc_adjoint_step_matches_the_allocating_entry_point(kind):
     import torch
 
     from beamz_b200 import runtime as R
 
-    spec = W.scene_2d(total_steps=64, seed=9, shape=(72, 80), pml_cells=6, n_monitors=2)
-    spec = dataclasses.replace(spec, metallic_edges=frozenset({"bottom", "right"}))
+    spec = _spec(kind)
     prog = R.compile_program(spec, schedule="phases", layout="dense")
-    active = P.active_components(2, "tm")
+    active = P.active_components(spec.ndim, spec.polarization)
     scratch = {"e": {}, "h": {}}
     for t in range(6):
         ec, hs = P.COMPONENTS[t // 2], P.COMPONENTS[_E_SRC[t]]
