@@ -17,9 +17,9 @@
 //  * the E material is one uint8 class id per lattice point (a class is one
 //    (Ex, Ey, Ez) coefficient triple of the codebook), 1 byte per cell instead
 //    of a 4-byte codebook word, with the class table in shared memory;
-//  * the CPML memories of an x-slab are addressed through per-lane slab masks
-//    computed once per CTA, every psi load of a plane is issued before its
-//    first use, and the next plane's psi is prefetched into L2.
+//  * the CPML recurrences of a row's x-slab cells are shared by the row's warp
+//    (one cell per lane) instead of falling on the few lanes that own them,
+//    and every psi load of a plane is issued ahead of its first use.
 //
 // Arithmetic: beamz's float32 order bit for bit (every difference divided by
 // the cell size with a correctly rounded quotient, every product and sum
@@ -30,8 +30,8 @@
 //
 // Tile-planes that touch a high domain face, a z face, an H source or a
 // partial tile run a general per-cell path with every validity, ghost and PEC
-// rule; the rest run one of six straight bodies chosen by the absorber axes
-// they touch.  The H-term CPML memories are double-banked (the halo
+// rule; the rest run one of three straight bodies: the interior, the x = 0 /
+// y = 0 faces, and the absorber shell (its axes plane-uniform run-time flags).  The H-term CPML memories are double-banked (the halo
 // recomputation reads them), the E-term ones updated in place.
 //
 // Operation order follows beamz/simulation/kernels.py:458-626 (H from E with
@@ -70,6 +70,8 @@ struct ClassTile {
     float4 cls[256];                   // per class: dt/(eps0 eps dx) of Ex, Ey, Ez
     float4 cc[12][kSlots];  // CPML (a, b, 1/kappa) (a/dx in the tolerance form): H terms 0-5, E terms 6-11
     float xd[2][TY][32];    // corrected x differences of a row's x-slab cells by slot (compact x work)
+    float xpf[2][2][NT];    // the x work's psi of the next plane: [plane parity][H, E][thread]
+    float hcoef[6];         // uniform H decay (Hx, Hy, Hz) and source (over dx in the tolerance form)
     float amp[kMaxFusedSources];
     unsigned long long bar[2];
   };
@@ -299,6 +301,15 @@ __device__ __forceinline__ XItems x_items(const CpmlTermDev& t, int i0, int i1) 
   return r;
 }
 
+// A 4-byte global -> shared copy that holds no register while in flight
+// (cp.async, waited on by the issuing thread before it reads the slot).
+__device__ __forceinline__ void async_copy4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tma::smem_u32(dst)), "l"(src) : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One scalar cell of a term: psi fetched ahead (0 outside the slab), then applied.
 template <int Axis>
 __device__ __forceinline__ float psi1_fetch(const CpmlTermDev& t, int k, int j, int i) {
@@ -331,23 +342,6 @@ __device__ __forceinline__ float cpml1(const CpmlTermDev& t, const float4* cc, b
   const float r = cpml_d<Exact>(c, res, t.psi_in[off], d, &n);
   if (write) t.psi_out[off] = n;
   return r;
-}
-
-__device__ __forceinline__ void l2_prefetch(const void* ptr) {
-  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(ptr));
-}
-
-// L2 prefetch of the psi a y or z term needs at (k, j, i..i+3), if in its slab.
-template <int Axis>
-__device__ __forceinline__ void psi_prefetch(const CpmlTermDev& t, int k, int j, int i) {
-  if (t.psi_in == nullptr) return;
-  const int slot = slot_of(t, Axis == 0 ? k : j);
-  if (slot >= 0) l2_prefetch(t.psi_in + psi_off<Axis>(t, slot, k, j, i));
-}
-
-// ... and of an x term through its lane mask.
-__device__ __forceinline__ void psix_prefetch(const CpmlTermDev& t, int xs, int k, int j) {
-  if (xs & 15) l2_prefetch(t.psi_in + xrow(t, xs, k, j));
 }
 
 __device__ __forceinline__ float h_sources_at(const Step3D& p, const float* amp, int c, int k, int j, int i, float h) {
@@ -434,16 +428,20 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     }
   }
   if (tid < p.n_hsrc) sm.amp[tid] = source_amplitude(p.hsrc[tid], p.step_counter[0] + p.step_offset);
+  // The uniform H coefficients live in shared memory (read where used) rather
+  // than in six registers for the whole kernel.  The tolerance form folds 1/dx
+  // into the source (the class table carries E's).
+  if (tid < 3) {
+    sm.hcoef[tid] = p.hm.decay[tid][0];
+    sm.hcoef[3 + tid] = p.hm.source[tid][0] * (Exact ? 1.0f : inv_res);
+  }
   __syncthreads();
 
   const bool wz0 = wall(p.metallic, 0, false), wz1 = wall(p.metallic, 0, true);
   const bool wy0 = wall(p.metallic, 1, false), wy1 = wall(p.metallic, 1, true);
   const bool wx0 = wall(p.metallic, 2, false), wx1 = wall(p.metallic, 2, true);
   // Uniform H coefficients (the pitched layout carries no per-site H).
-  const float dec0 = p.hm.decay[0][0], dec1 = p.hm.decay[1][0], dec2 = p.hm.decay[2][0];
-  // The tolerance form folds 1/dx into the H coefficient (the class table carries E's).
-  const float hsc = Exact ? 1.0f : inv_res;
-  const float s0 = p.hm.source[0][0] * hsc, s1 = p.hm.source[1][0] * hsc, s2 = p.hm.source[2][0] * hsc;
+
   const float dbs = p.div_bs, drs = p.div_rs;  // div_rn's scaled cell size and reciprocal
   auto D1 = [&](float v) { return dv<Exact>(v, dbs, drs); };
   auto D4 = [&](float4 v) { return dv4<Exact>(v, dbs, drs); };
@@ -484,14 +482,34 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   // row's (term, slot) list: the first x term's slots, then the second's.
   const bool xcompact = ax && p.ht[3].low + p.ht[3].high <= 32 && p.ht[4].low + p.ht[4].high <= 32 &&
                         p.et[3].low + p.et[3].high <= 32 && p.et[4].low + p.et[4].high <= 32;
-  // The lane's x-slab psi of the next plane, loaded a plane ahead (H and E
-  // terms, items lane and lane + 32).
-  float xq_h0 = 0.0f, xq_h1 = 0.0f, xq_e0 = 0.0f, xq_e1 = 0.0f;
-  int xq_kh = -1, xq_ke = -1;  // the planes they belong to
 
   const bool fast_ok = fast_ok0 && (!ax || xcompact);
-  // Column X is lane 31's own work, so the items stop short of it.
-  const int xi1 = i0 + TX;
+  const bool shell_x = ax, shell_y = ay;  // the tile's absorber axes (z is per plane)
+  // The psi of this lane's first x item in the next plane is copied a plane
+  // ahead into shared memory (the x work sits at the head of its phase, so a
+  // load there would stall the whole warp); the planes the H and the E copies
+  // belong to.
+  int xq_kh = -1, xq_ke = -1;
+  bool shell_z = false;
+  // This lane's compact x items (tile-constant), packed as valid | second term
+  // << 1 | slot << 2 | (x - i0) << 8: items lane and lane + 32 of the H terms'
+  // list (xi_h0, xi_h1) and of the E terms' (xi_e0, xi_e1).  Column X is lane
+  // 31's own work, so the items stop short of it.
+  int xi_h0 = 0, xi_h1 = 0, xi_e0 = 0, xi_e1 = 0;
+  if (xcompact) {
+    auto pack = [&](const CpmlTermDev& t3, const CpmlTermDev& t4, int q) {
+      const XItems a3 = x_items(t3, i0, i0 + TX), a4 = x_items(t4, i0, i0 + TX);
+      const int n3 = a3.lo_n + a3.hi_n;
+      const bool second = q >= n3;
+      int slot = 0, x = 0;
+      if (!(second ? a4 : a3).item(second ? q - n3 : q, &slot, &x)) return 0;
+      return 1 | (second ? 2 : 0) | (slot << 2) | ((x - i0) << 8);
+    };
+    xi_h0 = pack(p.ht[3], p.ht[4], lane);
+    xi_h1 = pack(p.ht[3], p.ht[4], lane + 32);
+    xi_e0 = pack(p.et[3], p.et[4], lane);
+    xi_e1 = pack(p.et[3], p.et[4], lane + 32);
+  }
 
   // H of the previous plane on the own cells (the z-backward differences of E).
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
@@ -528,8 +546,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     if (fast_ok && !src && k >= 1 && k < Z) {
       // ---- straight tile-plane: every own and halo cell valid ----------------
       auto body = [&](auto axc, auto ayc, auto azc, auto fc) {
-        constexpr bool AX = decltype(axc)::value, AY = decltype(ayc)::value, AZ = decltype(azc)::value;
+        // CPML axes: compile-time off in the interior and face bodies; in the
+        // shell body (all on) the plane's own axes decide at run time
+        // (plane-uniform branches), so one body serves every absorber tile.
+        constexpr bool SX = decltype(axc)::value, SY = decltype(ayc)::value, SZ = decltype(azc)::value;
         constexpr bool FC = decltype(fc)::value;  // the tile may touch x = 0 / y = 0
+        const bool AX = SX && shell_x, AY = SY && shell_y, AZ = SZ && shell_z;
         const bool at_x0 = FC && xface, at_y0 = FC && yface;
         const int jh = j0 - 1, ih = i0 - 1;  // the halo row and column
         // Which warps recompute a halo this plane (never on a pre-plane).
@@ -542,85 +564,38 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
         // psi of the H terms: own cells, halos, column X.
         float4 qh0, qh1, qh2, qh5;
-        if constexpr (AY) {
+        if (AY) {
           qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
           qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
         }
-        if constexpr (AZ) {
+        if (AZ) {
           qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
-        // The halos' psi (read only), in flight during the own-row H update:
-        // row j0-1 (warp 0: Hxy, Hxz, and column X's; warp 1: Hzx, Hzy) and
-        // column i0-1 (warp 2: Hyz, Hyx, Hzx, Hzy in qa.x-w).
-        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
-        float qR0 = 0.f, qR1 = 0.f;
-        if constexpr (AX || AY || AZ) {
-          if (halo_row_x) {
-            if constexpr (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
-            if constexpr (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
-            if (xl) {
-              if constexpr (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
-              if constexpr (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
-            }
-          } else if (halo_row_z) {
-            if constexpr (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
-            if constexpr (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
-          } else if (halo_col) {
-            if constexpr (AZ) qa.x = psi1_fetch<0>(p.ht[2], k, jc, ih);
-            if constexpr (AX) qa.y = psi1_fetch<2>(p.ht[3], k, jc, ih);
-            if constexpr (AX) qa.z = psi1_fetch<2>(p.ht[4], k, jc, ih);
-            if constexpr (AY) qa.w = psi1_fetch<1>(p.ht[5], k, jc, ih);
-          }
-        }
-        // Next plane's psi (and column X's class id) into L2, a plane ahead of use.
-        if (k + 1 < k1) {
-          const int kn = k + 1;
-          if (xl) l2_prefetch(p.site_class + (kn * (Y + 1) + j) * p.pitch8 + X);
-          if constexpr (Cpml) {
-            psi_prefetch<0>(p.ht[1], kn, j, i);
-            psi_prefetch<0>(p.ht[2], kn, j, i);
-            psi_prefetch<0>(p.et[1], kn, j, i);
-            psi_prefetch<0>(p.et[2], kn, j, i);
-            if constexpr (AY) {
-              psi_prefetch<1>(p.ht[0], kn, j, i);
-              psi_prefetch<1>(p.ht[5], kn, j, i);
-              psi_prefetch<1>(p.et[0], kn, j, i);
-              psi_prefetch<1>(p.et[5], kn, j, i);
-            }
-            // The halos' (read-only) psi of the next plane.
-            if (warp == 0 && !at_y0) {
-              if constexpr (AY) psi_prefetch<1>(p.ht[0], kn, jh, i);
-              psi_prefetch<0>(p.ht[1], kn, jh, i);
-            } else if (warp == 1 && !at_y0) {
-              if constexpr (AX) psix_prefetch(p.ht[4], xs4, kn, jh);
-              if constexpr (AY) psi_prefetch<1>(p.ht[5], kn, jh, i);
-            } else if (warp == 2 && lane < TY && !at_x0) {
-              const int slot2 = slot_of(p.ht[2], kn);
-              if (slot2 >= 0) l2_prefetch(p.ht[2].psi_in + psi_off<0>(p.ht[2], slot2, kn, jc, ih));
-              if constexpr (AY) {
-                const int slot5 = slot_of(p.ht[5], jc);
-                if (slot5 >= 0) l2_prefetch(p.ht[5].psi_in + psi_off<1>(p.ht[5], slot5, kn, jc, ih));
-              }
-            }
-          }
-        }
         // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
-        if constexpr (AX) {
-          const XItems it3 = x_items(p.ht[3], i0, xi1), it4 = x_items(p.ht[4], i0, xi1);
-          const int n3 = it3.lo_n + it3.hi_n;
+        if (AX) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const int q = lane + 32 * h;
-            const bool second = q >= n3;  // Hzx (dEy/dx), else Hyx (dEz/dx)
-            int slot, x;
-            if ((second ? it4 : it3).item(second ? q - n3 : q, &slot, &x)) {
+            const int w = h ? xi_h1 : xi_h0;
+            if (w & 1) {
+              const bool second = w & 2;  // Hzx (dEy/dx), else Hyx (dEz/dx)
+              const int slot = (w >> 2) & 63, xo = w >> 8;
               const CpmlTermDev& d = second ? p.ht[4] : p.ht[3];
               const float* Erow = second ? E0y : E0z;
-              const int b = r * BX + 4 + (x - i0);
+              const int b = r * BX + 4 + xo;
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              const float psi = xq_kh == k ? (h ? xq_h1 : xq_h0) : d.psi_in[off];
-              if (k + 1 < k1) (h ? xq_h1 : xq_h0) = d.psi_in[off + d.pdy * d.pdx];  // the next plane's, in flight
+              float psi;
+              if (h == 0) {
+                if (xq_kh == k) {
+                  async_wait_all();
+                  psi = sm.xpf[k & 1][0][tid];
+                } else {
+                  psi = d.psi_in[off];
+                }
+                if (k + 1 < k1) async_copy4(&sm.xpf[(k + 1) & 1][0][tid], d.psi_in + off + d.pdy * d.pdx);
+              } else {
+                psi = d.psi_in[off];
+              }
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
               if (emit) d.psi_out[off] = nv;
@@ -643,21 +618,21 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy0 = D4(sub4(ld4(E1x + rc), ex)), dy1 = D4(sub4(next4(ez, ez4), ez));       // Hy: dEx/dz, dEz/dx
           dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(ld4(E0x + rc + BX), ex));  // Hz: dEy/dx, dEx/dy
         }
-        if constexpr (AY) {
+        if (AY) {
           dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit);
           dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit);
         }
-        if constexpr (AZ) {
+        if (AZ) {
           dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit);
           dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
         }
-        if constexpr (AX) {
+        if (AX) {
           dy1 = xtake(dy1, xs3, sm.xd[0][warp]);
           dz0 = xtake(dz0, xs4, sm.xd[1][warp]);
         }
-        float4 hx = h4<Exact>(ld4(HOx + rc), dec0, s0, dx0, dx1);
-        float4 hy = h4<Exact>(ld4(HOy + rc), dec1, s1, dy0, dy1);
-        const float4 hz = h4<Exact>(ld4(HOz + rc), dec2, s2, dz0, dz1);
+        float4 hx = h4<Exact>(ld4(HOx + rc), sm.hcoef[0], sm.hcoef[3], dx0, dx1);
+        float4 hy = h4<Exact>(ld4(HOy + rc), sm.hcoef[1], sm.hcoef[4], dy0, dy1);
+        const float4 hz = h4<Exact>(ld4(HOz + rc), sm.hcoef[2], sm.hcoef[5], dz0, dz1);
         if (at_x0 && lane == 0 && wx0) hx.x = 0.0f;  // PEC: normal H on the x = 0 wall
         if (at_y0 && warp == 0 && wy0) hy = make_float4(0.f, 0.f, 0.f, 0.f);
         st4(&sm.hn[0][r][c0], hx);
@@ -674,12 +649,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         if (xl) {
           const int b = rc + 4;
           float qX0 = 0.f, qX1 = 0.f;
-          if constexpr (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
-          if constexpr (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
+          if (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
+          if (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
           float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
-          if constexpr (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit);
-          if constexpr (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit);
-          hxX = wx1 ? 0.0f : h1<Exact>(HOx[b], dec0, s0, d0, d1);
+          if (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit);
+          if (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit);
+          hxX = wx1 ? 0.0f : h1<Exact>(HOx[b], sm.hcoef[0], sm.hcoef[3], d0, d1);
           sm.hn[0][r][XC] = hxX;
           if (emit) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
         }
@@ -687,59 +662,74 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
         if (halo_row_x) {
           const int b = c0;
+          float4 qa, qb;
+          float qR0 = 0.f, qR1 = 0.f;
+          if (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
+          if (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
+          if (xl) {
+            if (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
+            if (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
+          }
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
-          if constexpr (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
-          if constexpr (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
-          float4 h = h4<Exact>(ld4(HOx + b), dec0, s0, d0, d1);
+          if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
+          if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
+          float4 h = h4<Exact>(ld4(HOx + b), sm.hcoef[0], sm.hcoef[3], d0, d1);
           if (at_x0 && lane == 0 && wx0) h.x = 0.0f;
           st4(&sm.hn[0][0][b], h);
           if (xl) {
             const int bb = XC;
             float e0v = D1(E0z[bb + BX] - E0z[bb]), e1v = D1(E1y[bb] - E0y[bb]);
-            if constexpr (AY) e0v = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qR0, k, jh, X, res, e0v, false);
-            if constexpr (AZ) e1v = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qR1, k, jh, X, res, e1v, false);
-            sm.hn[0][0][XC] = wx1 ? 0.0f : h1<Exact>(HOx[bb], dec0, s0, e0v, e1v);
+            if (AY) e0v = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qR0, k, jh, X, res, e0v, false);
+            if (AZ) e1v = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qR1, k, jh, X, res, e1v, false);
+            sm.hn[0][0][XC] = wx1 ? 0.0f : h1<Exact>(HOx[bb], sm.hcoef[0], sm.hcoef[3], e0v, e1v);
           }
         } else if (halo_row_z) {
           const int b = c0;
+          float4 qa, qb;
+          if (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
+          if (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
           if (lane == 31) e4 = E0y[b + 4];
           float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
-          if constexpr (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
-          if constexpr (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false);
-          st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), dec2, s2, d0, d1));
+          if (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
+          if (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false);
+          st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), sm.hcoef[2], sm.hcoef[5], d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
-          const float qc0 = qa.x, qc1 = qa.y, qc2 = qa.z, qc3 = qa.w;
+          float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f;
+          if (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
+          if (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
+          if (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
+          if (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
           float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
-          if constexpr (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
-          if constexpr (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
-          float hyv = h1<Exact>(HOy[b], dec1, s1, d0, d1);
+          if (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
+          if (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
+          float hyv = h1<Exact>(HOy[b], sm.hcoef[1], sm.hcoef[4], d0, d1);
           if (at_y0 && jc == 0 && wy0) hyv = 0.0f;
           float f0 = D1(E0y[b + 1] - E0y[b]), f1 = D1(E0x[b + BX] - E0x[b]);  // Hz: dEy/dx, dEx/dy
-          if constexpr (AX) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
-          if constexpr (AY) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
+          if (AX) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
+          if (AY) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
           sm.hn[1][rr][3] = hyv;
-          sm.hn[2][rr][3] = h1<Exact>(HOz[b], dec2, s2, f0, f1);
+          sm.hn[2][rr][3] = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], f0, f1);
         }
         // psi of the E terms, in flight during the barrier.
         float4 qe0, qe1, qe2, qe5;
         float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
         if (emit) {
-          if constexpr (AY) {
+          if (AY) {
             qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
             qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
           }
-          if constexpr (AZ) {
+          if (AZ) {
             qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
             qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
           }
           if (xl) {
-            if constexpr (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
-            if constexpr (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
-            if constexpr (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
-            if constexpr (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
+            if (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
+            if (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
+            if (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
+            if (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
           }
         }
         __syncthreads();
@@ -750,23 +740,31 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           return;
         }
         // ---- compact x work of the E terms (Eyx, Ezx) on this warp's row ----
-        if constexpr (AX) {
-          const XItems it3 = x_items(p.et[3], i0, xi1), it4 = x_items(p.et[4], i0, xi1);
-          const int n3 = it3.lo_n + it3.hi_n;
+        if (AX) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const int q = lane + 32 * h;
-            const bool second = q >= n3;  // Ezx (dHy/dx), else Eyx (dHz/dx)
-            int slot, x;
-            if ((second ? it4 : it3).item(second ? q - n3 : q, &slot, &x)) {
+            const int w = h ? xi_e1 : xi_e0;
+            if (w & 1) {
+              const bool second = w & 2;  // Ezx (dHy/dx), else Eyx (dHz/dx)
+              const int slot = (w >> 2) & 63, xo = w >> 8;
               const CpmlTermDev& d = second ? p.et[4] : p.et[3];
               const float* Hrow = second ? sm.hn[1][r] : sm.hn[2][r];
-              const int c = 4 + (x - i0);
+              const int c = 4 + xo;
               // Beyond x = 0 the ghost: zero on a metallic wall, else the edge value.
-              const float dv = (at_x0 && x == 0) ? (wx0 ? Hrow[c] : 0.0f) : Hrow[c] - Hrow[c - 1];
+              const float dv = (at_x0 && xo == 0) ? (wx0 ? Hrow[c] : 0.0f) : Hrow[c] - Hrow[c - 1];
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              const float psi = xq_ke == k ? (h ? xq_e1 : xq_e0) : d.psi_in[off];
-              if (k + 1 < k1) (h ? xq_e1 : xq_e0) = d.psi_in[off + d.pdy * d.pdx];
+              float psi;
+              if (h == 0) {
+                if (xq_ke == k) {
+                  async_wait_all();
+                  psi = sm.xpf[k & 1][1][tid];
+                } else {
+                  psi = d.psi_in[off];
+                }
+                if (k + 1 < k1) async_copy4(&sm.xpf[(k + 1) & 1][1][tid], d.psi_in + off + d.pdy * d.pdx);
+              } else {
+                psi = d.psi_in[off];
+              }
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
               d.psi_out[off] = nv;
@@ -794,15 +792,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         float4 fx0 = D4(sub4(hz, hzy)), fx1 = D4(sub4(hy, hyp));              // Ex: dHz/dy, dHy/dz
         float4 fy0 = D4(sub4(hx, hxp)), fy1 = D4(sub4(hz, prev4(hzl, hz)));   // Ey: dHx/dz, dHz/dx
         float4 fz0 = D4(sub4(hy, prev4(hyl, hy))), fz1 = D4(sub4(hx, hxy));   // Ez: dHy/dx, dHx/dy
-        if constexpr (AY) {
+        if (AY) {
           fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, true);
           fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, true);
         }
-        if constexpr (AZ) {
+        if (AZ) {
           fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, true);
           fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
         }
-        if constexpr (AX) {
+        if (AX) {
           fy1 = xtake(fy1, xe3, sm.xd[0][warp]);
           fz0 = xtake(fz0, xe4, sm.xd[1][warp]);
         }
@@ -834,12 +832,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           // The Hz / Hy ghosts beyond x = X: zero on a metallic wall, else the edge value.
           float g0 = D1(hxX - hxXp), g1 = D1(wx1 ? 0.0f - hz.w : 0.0f);   // Ey: dHx/dz, dHz/dx
           float h0 = D1(wx1 ? 0.0f - hy.w : 0.0f), h1v = D1(hxX - hxy_X);  // Ez: dHy/dx, dHx/dy
-          if constexpr (AZ) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
-          if constexpr (AX) {
+          if (AZ) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
+          if (AX) {
             g1 = psi1_apply<Exact, 2>(p.et[3], sm.cc[9], qY3, k, j, X, res, g1, true);
             h0 = psi1_apply<Exact, 2>(p.et[4], sm.cc[10], qY4, k, j, X, res, h0, true);
           }
-          if constexpr (AY) h1v = psi1_apply<Exact, 1>(p.et[5], sm.cc[11], qY5, k, j, X, res, h1v, true);
+          if (AY) h1v = psi1_apply<Exact, 1>(p.et[5], sm.cc[11], qY5, k, j, X, res, h1v, true);
           const float4 t = sm.cls[cidX];
           const float ny_ = e_upd<Exact>(E0y[b], t.y, g0, g1);
           const float nz_ = e_upd<Exact>(E0z[b], t.z, h0, h1v);
@@ -854,16 +852,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         if (xface || yface) body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{});
         else body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{});
       } else {
-        const bool az = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
-        const int v = (ax ? 4 : 0) | (ay ? 2 : 0) | (az ? 1 : 0);
-        switch (v == 3 || v == 5 || v == 6 ? 7 : (v == 0 && !(xface || yface) ? 8 : v)) {
-          case 8: body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{}); break;
-          case 0: body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{}); break;
-          case 1: body(std::false_type{}, std::false_type{}, std::true_type{}, std::true_type{}); break;
-          case 2: body(std::false_type{}, std::true_type{}, std::false_type{}, std::true_type{}); break;
-          case 4: body(std::true_type{}, std::false_type{}, std::false_type{}, std::true_type{}); break;
-          default: body(std::true_type{}, std::true_type{}, std::true_type{}, std::true_type{}); break;
-        }
+        shell_z = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
+        if (shell_x || shell_y || shell_z) body(std::true_type{}, std::true_type{}, std::true_type{}, std::true_type{});
+        else if (xface || yface) body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{});
+        else body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{});
       }
     } else {
       // ---- general tile-plane: per cell, every validity / ghost / PEC rule ---
@@ -881,7 +873,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 1>(p.ht[0], sm.cc[0], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 0>(p.ht[1], sm.cc[1], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOx[b], dec0, s0, d0, d1);
+          float h = h1<Exact>(HOx[b], sm.hcoef[0], sm.hcoef[3], d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 3, k, jj, ii, h);
           if ((ii == 0 && wx0) || (ii == X && wx1)) h = 0.0f;
           sm.hn[0][rr][cc] = h;
@@ -893,7 +885,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 0>(p.ht[2], sm.cc[2], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 2>(p.ht[3], sm.cc[3], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOy[b], dec1, s1, d0, d1);
+          float h = h1<Exact>(HOy[b], sm.hcoef[1], sm.hcoef[4], d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 4, k, jj, ii, h);
           if ((jj == 0 && wy0) || (jj == Y && wy1)) h = 0.0f;
           sm.hn[1][rr][cc] = h;
@@ -905,7 +897,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 2>(p.ht[4], sm.cc[4], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 1>(p.ht[5], sm.cc[5], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOz[b], dec2, s2, d0, d1);
+          float h = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 5, k, jj, ii, h);
           if ((k == 0 && wz0) || (k == Z && wz1)) h = 0.0f;
           sm.hn[2][rr][cc] = h;
@@ -968,7 +960,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       }
       __syncthreads();
       if (emit) {
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < 4; ++q) e_cell(r, c0 + q, get(hxp, q), get(hyp, q));
         if (xl) e_cell(r, XC, hxXp, 0.0f);
       }
