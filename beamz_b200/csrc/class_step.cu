@@ -71,6 +71,8 @@ struct ClassTile {
     float4 cc[12][kSlots];  // CPML (a, b, 1/kappa) (a/dx in the tolerance form): H terms 0-5, E terms 6-11
     float xd[2][TY][32];    // corrected x differences of a row's x-slab cells by slot (compact x work)
     float xpf[2][2][NT];    // the x work's psi of the next plane: [plane parity][H, E][thread]
+    float xph[2][4][32];    // the Hzx halo row's psi of the next plane (warp 1): [parity][cell][lane]
+    int xst[8][32];         // per lane: x-slab masks xs3, xs4, xe3, xe4 and compact items h0, h1, e0, e1
     float hcoef[6];         // uniform H decay (Hx, Hy, Hz) and source (over dx in the tolerance form)
     float amp[kMaxFusedSources];
     unsigned long long bar[2];
@@ -305,10 +307,14 @@ __device__ __forceinline__ XItems x_items(const CpmlTermDev& t, int i0, int i1) 
 // (cp.async, waited on by the issuing thread before it reads the slot).
 __device__ __forceinline__ void async_copy4(float* dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tma::smem_u32(dst)), "l"(src) : "memory");
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Wait for this thread's copy groups except the `newer` (0 or 1) most recent.
+__device__ __forceinline__ void async_wait(bool newer) {
+  if (newer) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 // One scalar cell of a term: psi fetched ahead (0 outside the slab), then applied.
 template <int Axis>
@@ -461,42 +467,24 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
 
-  // x-slab masks of the own cells for Hyx, Hzx, Eyx, Ezx (tile-constant).
-  int xs3 = 0, xs4 = 0, xe3 = 0, xe4 = 0;
-  if (ax) {
-    xs3 = xslab_of(p.ht[3], i);
-    xs4 = xslab_of(p.ht[4], i);
-    xe3 = xslab_of(p.et[3], i);
-    xe4 = xslab_of(p.et[4], i);
-  }
-
   // Compact x work: in a tile that touches an x slab, the recurrences of a
-  // row's x-slab cells are shared by the row's warp -- lanes 0-15 take the
-  // first x term of the phase (Hyx, Eyx), lanes 16-31 the second (Hzx, Ezx),
-  // one cell each -- instead of falling on the few lanes that own slab cells;
-  // the corrected differences reach the owners through shared memory.  Per x
-  // term: the first slab x in this tile and the run length (one contiguous
-  // run of at most 16 cells; otherwise the owners' per-lane path runs).
-  // The compact x work covers slabs of at most 32 slots per term (wider ones
-  // take the general path); each lane takes items lane and lane + 32 of the
-  // row's (term, slot) list: the first x term's slots, then the second's.
+  // row's x-slab cells are shared by the row's warp -- each lane takes items
+  // lane and lane + 32 of the row's (term, slot) list, the first x term's
+  // slots (Hyx, Eyx), then the second's (Hzx, Ezx) -- instead of falling on
+  // the few lanes that own slab cells; the corrected differences reach the
+  // owners through shared memory.  It covers slabs of at most 32 slots per
+  // term (wider ones take the general path).
   const bool xcompact = ax && p.ht[3].low + p.ht[3].high <= 32 && p.ht[4].low + p.ht[4].high <= 32 &&
                         p.et[3].low + p.et[3].high <= 32 && p.et[4].low + p.et[4].high <= 32;
-
   const bool fast_ok = fast_ok0 && (!ax || xcompact);
   const bool shell_x = ax, shell_y = ay;  // the tile's absorber axes (z is per plane)
-  // The psi of this lane's first x item in the next plane is copied a plane
-  // ahead into shared memory (the x work sits at the head of its phase, so a
-  // load there would stall the whole warp); the planes the H and the E copies
-  // belong to.
-  int xq_kh = -1, xq_ke = -1;
-  bool shell_z = false;
-  // This lane's compact x items (tile-constant), packed as valid | second term
-  // << 1 | slot << 2 | (x - i0) << 8: items lane and lane + 32 of the H terms'
-  // list (xi_h0, xi_h1) and of the E terms' (xi_e0, xi_e1).  Column X is lane
-  // 31's own work, so the items stop short of it.
-  int xi_h0 = 0, xi_h1 = 0, xi_e0 = 0, xi_e1 = 0;
-  if (xcompact) {
+  // Tile-constant x state per lane, in shared memory so that it holds no
+  // register outside the x work: the x-slab masks of the own cells for Hyx,
+  // Hzx, Eyx, Ezx (xslab_of) and the lane's compact items, packed as valid |
+  // second term << 1 | slot << 2 | (x - i0) << 8 (items lane and lane + 32 of
+  // the H terms' list, then of the E terms').  Column X is lane 31's own work,
+  // so the items stop short of it.
+  if (xcompact && warp == 0) {
     auto pack = [&](const CpmlTermDev& t3, const CpmlTermDev& t4, int q) {
       const XItems a3 = x_items(t3, i0, i0 + TX), a4 = x_items(t4, i0, i0 + TX);
       const int n3 = a3.lo_n + a3.hi_n;
@@ -505,11 +493,21 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       if (!(second ? a4 : a3).item(second ? q - n3 : q, &slot, &x)) return 0;
       return 1 | (second ? 2 : 0) | (slot << 2) | ((x - i0) << 8);
     };
-    xi_h0 = pack(p.ht[3], p.ht[4], lane);
-    xi_h1 = pack(p.ht[3], p.ht[4], lane + 32);
-    xi_e0 = pack(p.et[3], p.et[4], lane);
-    xi_e1 = pack(p.et[3], p.et[4], lane + 32);
+    sm.xst[0][lane] = xslab_of(p.ht[3], i);
+    sm.xst[1][lane] = xslab_of(p.ht[4], i);
+    sm.xst[2][lane] = xslab_of(p.et[3], i);
+    sm.xst[3][lane] = xslab_of(p.et[4], i);
+    sm.xst[4][lane] = pack(p.ht[3], p.ht[4], lane);
+    sm.xst[5][lane] = pack(p.ht[3], p.ht[4], lane + 32);
+    sm.xst[6][lane] = pack(p.et[3], p.et[4], lane);
+    sm.xst[7][lane] = pack(p.et[3], p.et[4], lane + 32);
   }
+  if (xcompact) __syncthreads();  // CTA-uniform
+  // The x work's psi is copied a plane ahead into shared memory (cp.async,
+  // one commit group per phase and thread, empty where the thread copies
+  // nothing): the plane of the last H group and of the last E group.
+  int xq_kh = -1, xq_ke = -1;
+  bool shell_z = false;
 
   // H of the previous plane on the own cells (the z-backward differences of E).
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
@@ -525,6 +523,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         if (p.status) atomicExch(p.status, 1);
         if (!p.test_stall) tma::bar_wait(&sm.bar[n & 1], (n >> 1) & 1, wait_ns);  // the bundle in flight
       }
+      if (Cpml) async_wait(false);  // this thread's x-work copies
       __syncthreads();
       return;
     }
@@ -573,10 +572,16 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
         // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
+        bool xh_have = false;  // this plane's x psi was copied ahead (items, warp 1's halo row)
         if (AX) {
+          xh_have = xq_kh == k;
+          // Pending: this plane's H group, then its E group (newest) when the
+          // previous plane ran its E work; anything else is waited out.
+          async_wait(xh_have && xq_ke == k);
+          const bool ahead = k + 1 < k1;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const int w = h ? xi_h1 : xi_h0;
+            const int w = sm.xst[4 + h][lane];
             if (w & 1) {
               const bool second = w & 2;  // Hzx (dEy/dx), else Hyx (dEz/dx)
               const int slot = (w >> 2) & 63, xo = w >> 8;
@@ -584,24 +589,24 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const float* Erow = second ? E0y : E0z;
               const int b = r * BX + 4 + xo;
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              float psi;
-              if (h == 0) {
-                if (xq_kh == k) {
-                  async_wait_all();
-                  psi = sm.xpf[k & 1][0][tid];
-                } else {
-                  psi = d.psi_in[off];
-                }
-                if (k + 1 < k1) async_copy4(&sm.xpf[(k + 1) & 1][0][tid], d.psi_in + off + d.pdy * d.pdx);
-              } else {
-                psi = d.psi_in[off];
-              }
+              const float psi = (h == 0 && xh_have) ? sm.xpf[k & 1][0][tid] : d.psi_in[off];
+              if (h == 0 && ahead) async_copy4(&sm.xpf[(k + 1) & 1][0][tid], d.psi_in + off + d.pdy * d.pdx);
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
               if (emit) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
+          if (ahead && warp == 1 && !at_y0) {  // Hzx on the halo row j0-1, next plane
+            const int xs = sm.xst[1][lane];
+            if (xs & 15) {
+              const float* row = p.ht[4].psi_in + xrow(p.ht[4], xs, k + 1, jh);
+#pragma unroll
+              for (int c = 0; c < 4; ++c)
+                if (xs & (1 << c)) async_copy4(&sm.xph[(k + 1) & 1][c][lane], row + c);
+            }
+          }
+          if (ahead) async_commit();
           xq_kh = k + 1;
           __syncwarp();
         }
@@ -627,8 +632,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
         }
         if (AX) {
-          dy1 = xtake(dy1, xs3, sm.xd[0][warp]);
-          dz0 = xtake(dz0, xs4, sm.xd[1][warp]);
+          dy1 = xtake(dy1, sm.xst[0][lane], sm.xd[0][warp]);
+          dz0 = xtake(dz0, sm.xst[1][lane], sm.xd[1][warp]);
         }
         float4 hx = h4<Exact>(ld4(HOx + rc), sm.hcoef[0], sm.hcoef[3], dx0, dx1);
         float4 hy = h4<Exact>(ld4(HOy + rc), sm.hcoef[1], sm.hcoef[4], dy0, dy1);
@@ -686,7 +691,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         } else if (halo_row_z) {
           const int b = c0;
           float4 qa, qb;
-          if (AX) qa = psix_fetch(p.ht[4], xs4, k, jh);
+          const int xs4 = AX ? sm.xst[1][lane] : 0;
+          if (AX) {
+            if (xh_have) {
+              const int q = k & 1;
+              qa = make_float4(sm.xph[q][0][lane], sm.xph[q][1][lane], sm.xph[q][2][lane], sm.xph[q][3][lane]);
+            } else {
+              qa = psix_fetch(p.ht[4], xs4, k, jh);
+            }
+          }
           if (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
@@ -741,9 +754,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         }
         // ---- compact x work of the E terms (Eyx, Ezx) on this warp's row ----
         if (AX) {
+          const bool have = xq_ke == k;
+          const bool ahead = k + 1 < k1;
+          // Pending: this plane's E group, then the next plane's H group (newest).
+          async_wait(have && ahead);
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const int w = h ? xi_e1 : xi_e0;
+            const int w = sm.xst[6 + h][lane];
             if (w & 1) {
               const bool second = w & 2;  // Ezx (dHy/dx), else Eyx (dHz/dx)
               const int slot = (w >> 2) & 63, xo = w >> 8;
@@ -753,24 +770,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               // Beyond x = 0 the ghost: zero on a metallic wall, else the edge value.
               const float dv = (at_x0 && xo == 0) ? (wx0 ? Hrow[c] : 0.0f) : Hrow[c] - Hrow[c - 1];
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              float psi;
-              if (h == 0) {
-                if (xq_ke == k) {
-                  async_wait_all();
-                  psi = sm.xpf[k & 1][1][tid];
-                } else {
-                  psi = d.psi_in[off];
-                }
-                if (k + 1 < k1) async_copy4(&sm.xpf[(k + 1) & 1][1][tid], d.psi_in + off + d.pdy * d.pdx);
-              } else {
-                psi = d.psi_in[off];
-              }
+              const float psi = (h == 0 && have) ? sm.xpf[k & 1][1][tid] : d.psi_in[off];
+              if (h == 0 && ahead) async_copy4(&sm.xpf[(k + 1) & 1][1][tid], d.psi_in + off + d.pdy * d.pdx);
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
               d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
+          if (ahead) async_commit();
           xq_ke = k + 1;
           __syncwarp();
         }
@@ -801,8 +809,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
         }
         if (AX) {
-          fy1 = xtake(fy1, xe3, sm.xd[0][warp]);
-          fz0 = xtake(fz0, xe4, sm.xd[1][warp]);
+          fy1 = xtake(fy1, sm.xst[2][lane], sm.xd[0][warp]);
+          fz0 = xtake(fz0, sm.xst[3][lane], sm.xd[1][warp]);
         }
         const float4 ex = ld4(E0x + rc), ey = ld4(E0y + rc), ez = ld4(E0z + rc);  // E(k) of the own cells
         const uint32_t w4 = *reinterpret_cast<const uint32_t*>(IDS + warp * TX + 4 * lane);
@@ -972,6 +980,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     e1 = e1 == 2 ? 0 : e1 + 1;
     hs ^= 1;
   }
+  if (Cpml) async_wait(false);  // no copy into shared memory outlives the CTA
 }
 
 template <int NW, bool Cpml, bool Exact>
