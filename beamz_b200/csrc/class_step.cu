@@ -40,6 +40,7 @@
 
 #include <cuda.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -62,6 +63,8 @@ struct ClassTile {
   static constexpr int HBOX = ((HH * BX + 31) / 32) * 32;
   static constexpr int IBOX = TY * TX;  // class ids (bytes), rows j0 .. j0+TY-1, x i0 .. i0+127
   static constexpr int XC = 4 + TX;     // box column of x = i0 + 128 (column X of the last tile)
+  static constexpr int XW = 16;         // staged x-psi window (slots)
+  static constexpr int XPS = ((HH * XW + 31) / 32) * 32;
   struct Smem {
     alignas(128) float e[3][3][EBOX];  // E ring: plane slot, component (TMA boxes start on 128 B)
     alignas(128) float h[2][3][HBOX];  // H (old) ring
@@ -70,8 +73,10 @@ struct ClassTile {
     float4 cls[256];                   // per class: dt/(eps0 eps dx) of Ex, Ey, Ez
     float4 cc[12][kSlots];  // CPML (a, b, 1/kappa) (a/dx in the tolerance form): H terms 0-5, E terms 6-11
     float xd[2][TY][32];    // corrected x differences of a row's x-slab cells by slot (compact x work)
-    float xpf[2][2][NT];    // the x work's psi of the next plane: [plane parity][H, E][thread]
-    float xph[2][4][32];    // the Hzx halo row's psi of the next plane (warp 1): [parity][cell][lane]
+    // x-term psi (Hyx, Hzx, Eyx, Ezx) of the bundle's plane, staged with it:
+    // rows j0-1 .. j0+TY-1, a 16-slot window of the tile's slab run.
+    alignas(128) float xps[2][4][XPS];
+    int xwin[4];            // each term's window start (slot)
     int xst[8][32];         // per lane: x-slab masks xs3, xs4, xe3, xe4 and compact items h0, h1, e0, e1
     float hcoef[6];         // uniform H decay (Hx, Hy, Hz) and source (over dx in the tolerance form)
     float amp[kMaxFusedSources];
@@ -83,7 +88,41 @@ struct ClassMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
   CUtensorMap ids;
+  CUtensorMap xpsi[4];  // x-term psi slabs (Hyx, Hzx, Eyx, Ezx), when Step3D::xstage
 };
+
+// CTA dispatch order, longest first: the CTAs of the absorber tile rows (every
+// z chunk), then the absorber z chunks of the other rows, then the rest, each
+// group x fastest.  Absorber CTAs take two to three times as long as interior
+// ones, so in launch order the last wave would otherwise be absorber-heavy
+// (the high z slab's chunks) and leave SMs idle at the end of the step.
+struct TileIdx {
+  int x, y, z;
+};
+__device__ __forceinline__ TileIdx tile_of(int L, int gx, int gy, int gz, const int* ord) {
+  const int ylo = ord[0], yhi = ord[1], zlo = ord[2], zhi = ord[3];
+  const int nys = ylo + (gy - yhi), nzs = zlo + (gz - zhi), nyi = gy - nys;
+  TileIdx t;
+  t.x = L % gx;
+  int q = L / gx;
+  auto row = [&](int r, bool shell) { return shell ? (r < ylo ? r : yhi + r - ylo) : ylo + r; };
+  auto chunk = [&](int c, bool shell) { return shell ? (c < zlo ? c : zhi + c - zlo) : zlo + c; };
+  if (q < nys * gz) {
+    t.y = row(q % nys, true);
+    t.z = q / nys;
+    return t;
+  }
+  q -= nys * gz;
+  if (q < nyi * nzs) {
+    t.y = row(q % nyi, false);
+    t.z = chunk(q / nyi, true);
+    return t;
+  }
+  q -= nyi * nzs;
+  t.y = row(q % nyi, false);
+  t.z = chunk(q / nyi, false);
+  return t;
+}
 
 // ---- float4 helpers ----------------------------------------------------------
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -303,19 +342,6 @@ __device__ __forceinline__ XItems x_items(const CpmlTermDev& t, int i0, int i1) 
   return r;
 }
 
-// A 4-byte global -> shared copy that holds no register while in flight
-// (cp.async, waited on by the issuing thread before it reads the slot).
-__device__ __forceinline__ void async_copy4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tma::smem_u32(dst)), "l"(src) : "memory");
-}
-
-__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// Wait for this thread's copy groups except the `newer` (0 or 1) most recent.
-__device__ __forceinline__ void async_wait(bool newer) {
-  if (newer) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-  else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
 // One scalar cell of a term: psi fetched ahead (0 outside the slab), then applied.
 template <int Axis>
 __device__ __forceinline__ float psi1_fetch(const CpmlTermDev& t, int k, int j, int i) {
@@ -390,20 +416,55 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   S& sm = *reinterpret_cast<S*>(smem_raw);
   const int lane = threadIdx.x, warp = threadIdx.y;
   const int tid = warp * 32 + lane;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int Z = p.Z, Y = p.Y, X = p.X;
-  const int k0 = blockIdx.z * p.z_chunk;
+  const int gx = X % TX == 0 ? X / TX : X / TX + 1, gy = (Y + TY) / TY, gz = (Z + p.z_chunk) / p.z_chunk;
+  const TileIdx tile = tile_of(blockIdx.x, gx, gy, gz, p.order);
+  const int i0 = tile.x * TX, j0 = tile.y * TY;
+  const int k0 = tile.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, Z + 1);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
   const int P = p.pitch, PL = (Y + 1) * p.pitch;
   const float res = p.res, inv_res = p.inv_res;
   const unsigned long long wait_ns = p.wait_ns;
 
-  // Bundle q: E(q+1) (and E(q) when `first`), H(q), class ids(q).  x starts at
-  // i0 - 4 (fields) or i0 (ids), i0 a multiple of 128: 16-byte aligned.
+  // When X is a multiple of 128 the last tile also owns column X (Hx, Ey, Ez
+  // there), done by lane 31, so no CTA is spent on one column.
+  const bool xcol = X % TX == 0 && i0 + TX == X;
+  const int xe = xcol ? 1 : 0;
+  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
+  // Compact x work: in a tile that touches an x slab, the recurrences of a
+  // row's x-slab cells are shared by the row's warp -- each lane takes items
+  // lane and lane + 32 of the row's (term, slot) list, the first x term's
+  // slots (Hyx, Eyx), then the second's (Hzx, Ezx) -- instead of falling on
+  // the few lanes that own slab cells; the corrected differences reach the
+  // owners through shared memory.  It covers slabs of at most 32 slots per
+  // term (wider ones take the general path).
+  const bool xcompact = ax && p.ht[3].low + p.ht[3].high <= 32 && p.ht[4].low + p.ht[4].high <= 32 &&
+                        p.et[3].low + p.et[3].high <= 32 && p.et[4].low + p.et[4].high <= 32;
+  // The x terms' psi rides in the plane's bundle when each term's run of
+  // slots in this tile fits one 16-slot window starting on a multiple of 4
+  // (16-byte TMA coordinate); otherwise the x work loads it directly.
+  int xwin[4] = {0, 0, 0, 0};
+  bool xstage = xcompact && p.xstage;
+  if (xstage) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const XItems a = x_items(t < 2 ? p.ht[3 + t] : p.et[1 + t], i0, i0 + TX);
+      if (a.lo_n + a.hi_n == 0) continue;
+      const int first = a.lo_n > 0 ? a.lo_s : a.hi_s;
+      const int last = a.hi_n > 0 ? a.hi_s + a.hi_n - 1 : a.lo_s + a.lo_n - 1;
+      xwin[t] = first & ~3;
+      if (last - xwin[t] >= T::XW) xstage = false;
+    }
+  }
+
+  // Bundle q: E(q+1) (and E(q) when `first`), H(q), class ids(q), and the x
+  // terms' psi of plane q.  x starts at i0 - 4 (fields), i0 (ids) or a
+  // multiple of 4 (psi): 16-byte aligned.
   auto issue = [&](int q, int slot, bool first) {
     const int ne = (first ? 1 : 0) + (q + 1 <= Z ? 1 : 0);
-    const unsigned bytes = ne * 3 * T::EH * BX * 4 + 3 * T::HH * BX * 4 + T::IBOX;
+    const unsigned bytes =
+        ne * 3 * T::EH * BX * 4 + 3 * T::HH * BX * 4 + T::IBOX + (xstage ? 4 * T::XW * T::HH * 4 : 0);
     unsigned long long* b = &sm.bar[slot];
     tma::bar_expect(b, bytes);
     if (p.test_stall) return;  // test-only: the barrier is armed, no copy is issued, nothing is in flight
@@ -413,9 +474,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       for (int c = 0; c < 3; ++c) tma::load_3d(sm.e[(q + 1) % 3][c], &maps.e[c], i0 - 4, j0 - 1, q + 1, b);
     for (int c = 0; c < 3; ++c) tma::load_3d(sm.h[q % 2][c], &maps.h[c], i0 - 4, j0 - 1, q, b);
     tma::load_3d(sm.ids[q % 2], &maps.ids, i0, j0, q, b);
+    if (xstage) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) tma::load_3d(sm.xps[q % 2][t], &maps.xpsi[t], xwin[t], j0 - 1, q, b);
+    }
   };
 
   if (tid == 0) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) sm.xwin[t] = xwin[t];
     tma::bar_init(&sm.bar[0], 1);
     tma::bar_init(&sm.bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -457,25 +524,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int c0 = 4 + 4 * lane;         // own first column in the boxes and hn
   const int i = i0 + 4 * lane;         // its lattice x
   const int rc = r * BX + c0;
-  // When X is a multiple of 128 the last tile also owns column X (Hx, Ey, Ez
-  // there), done by lane 31, so no CTA is spent on one column.
-  const bool xcol = X % TX == 0 && i0 + TX == X;
   const bool xl = xcol && lane == 31;
-  const int xe = xcol ? 1 : 0;
   const bool fast_ok0 = j0 + TY <= Y && i0 + TX <= X && cc_smem;
   const bool xface = i0 == 0, yface = j0 == 0;
-  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
-
-  // Compact x work: in a tile that touches an x slab, the recurrences of a
-  // row's x-slab cells are shared by the row's warp -- each lane takes items
-  // lane and lane + 32 of the row's (term, slot) list, the first x term's
-  // slots (Hyx, Eyx), then the second's (Hzx, Ezx) -- instead of falling on
-  // the few lanes that own slab cells; the corrected differences reach the
-  // owners through shared memory.  It covers slabs of at most 32 slots per
-  // term (wider ones take the general path).
-  const bool xcompact = ax && p.ht[3].low + p.ht[3].high <= 32 && p.ht[4].low + p.ht[4].high <= 32 &&
-                        p.et[3].low + p.et[3].high <= 32 && p.et[4].low + p.et[4].high <= 32;
   const bool fast_ok = fast_ok0 && (!ax || xcompact);
   const bool shell_x = ax, shell_y = ay;  // the tile's absorber axes (z is per plane)
   // Tile-constant x state per lane, in shared memory so that it holds no
@@ -503,10 +555,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     sm.xst[7][lane] = pack(p.et[3], p.et[4], lane + 32);
   }
   if (xcompact) __syncthreads();  // CTA-uniform
-  // The x work's psi is copied a plane ahead into shared memory (cp.async,
-  // one commit group per phase and thread, empty where the thread copies
-  // nothing): the plane of the last H group and of the last E group.
-  int xq_kh = -1, xq_ke = -1;
   bool shell_z = false;
 
   // H of the previous plane on the own cells (the z-backward differences of E).
@@ -523,7 +571,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         if (p.status) atomicExch(p.status, 1);
         if (!p.test_stall) tma::bar_wait(&sm.bar[n & 1], (n >> 1) & 1, wait_ns);  // the bundle in flight
       }
-      if (Cpml) async_wait(false);  // this thread's x-work copies
       __syncthreads();
       return;
     }
@@ -544,13 +591,15 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 
     if (fast_ok && !src && k >= 1 && k < Z) {
       // ---- straight tile-plane: every own and halo cell valid ----------------
-      auto body = [&](auto axc, auto ayc, auto azc, auto fc) {
-        // CPML axes: compile-time off in the interior and face bodies; in the
-        // shell body (all on) the plane's own axes decide at run time
-        // (plane-uniform branches), so one body serves every absorber tile.
-        constexpr bool SX = decltype(axc)::value, SY = decltype(ayc)::value, SZ = decltype(azc)::value;
-        constexpr bool FC = decltype(fc)::value;  // the tile may touch x = 0 / y = 0
-        const bool AX = SX && shell_x, AY = SY && shell_y, AZ = SZ && shell_z;
+      auto body = [&](auto mode) {
+        // The body's CPML axes (bits 0-2: x, y, z) and whether the tile may
+        // touch x = 0 / y = 0 (bit 3) are compile-time, so that a tile-plane
+        // runs code holding only its own absorber work; with bit 4 the axes
+        // are upper bounds and the plane's own flags decide at run time (the
+        // rare combinations share that body).
+        constexpr int M = decltype(mode)::value;
+        constexpr bool SX = M & 1, SY = M & 2, SZ = M & 4, FC = M & 8, RT = M & 16;
+        const bool AX = SX && (!RT || shell_x), AY = SY && (!RT || shell_y), AZ = SZ && (!RT || shell_z);
         const bool at_x0 = FC && xface, at_y0 = FC && yface;
         const int jh = j0 - 1, ih = i0 - 1;  // the halo row and column
         // Which warps recompute a halo this plane (never on a pre-plane).
@@ -571,14 +620,20 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
+        // psi of the E terms too: in flight through the whole H phase.
+        float4 qe0, qe1, qe2, qe5;
+        if (emit) {
+          if (AY) {
+            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
+            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
+          }
+          if (AZ) {
+            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
+            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
+          }
+        }
         // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
-        bool xh_have = false;  // this plane's x psi was copied ahead (items, warp 1's halo row)
         if (AX) {
-          xh_have = xq_kh == k;
-          // Pending: this plane's H group, then its E group (newest) when the
-          // previous plane ran its E work; anything else is waited out.
-          async_wait(xh_have && xq_ke == k);
-          const bool ahead = k + 1 < k1;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int w = sm.xst[4 + h][lane];
@@ -589,25 +644,14 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const float* Erow = second ? E0y : E0z;
               const int b = r * BX + 4 + xo;
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              const float psi = (h == 0 && xh_have) ? sm.xpf[k & 1][0][tid] : d.psi_in[off];
-              if (h == 0 && ahead) async_copy4(&sm.xpf[(k + 1) & 1][0][tid], d.psi_in + off + d.pdy * d.pdx);
+              const int t = second ? 1 : 0;
+              const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
               if (emit) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
-          if (ahead && warp == 1 && !at_y0) {  // Hzx on the halo row j0-1, next plane
-            const int xs = sm.xst[1][lane];
-            if (xs & 15) {
-              const float* row = p.ht[4].psi_in + xrow(p.ht[4], xs, k + 1, jh);
-#pragma unroll
-              for (int c = 0; c < 4; ++c)
-                if (xs & (1 << c)) async_copy4(&sm.xph[(k + 1) & 1][c][lane], row + c);
-            }
-          }
-          if (ahead) async_commit();
-          xq_kh = k + 1;
           __syncwarp();
         }
         // ---- H on the own row ----
@@ -693,9 +737,9 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           float4 qa, qb;
           const int xs4 = AX ? sm.xst[1][lane] : 0;
           if (AX) {
-            if (xh_have) {
-              const int q = k & 1;
-              qa = make_float4(sm.xph[q][0][lane], sm.xph[q][1][lane], sm.xph[q][2][lane], sm.xph[q][3][lane]);
+            if (xstage) {  // row j0-1 of the staged Hzx box (cells outside the slab are not read)
+              const float* q = &sm.xps[hs][1][(xs4 >> 4) - sm.xwin[1]];
+              qa = make_float4(q[0], q[1], q[2], q[3]);
             } else {
               qa = psix_fetch(p.ht[4], xs4, k, jh);
             }
@@ -726,18 +770,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           sm.hn[1][rr][3] = hyv;
           sm.hn[2][rr][3] = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], f0, f1);
         }
-        // psi of the E terms, in flight during the barrier.
-        float4 qe0, qe1, qe2, qe5;
         float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
         if (emit) {
-          if (AY) {
-            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
-            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
-          }
-          if (AZ) {
-            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
-            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
-          }
           if (xl) {
             if (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
             if (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
@@ -754,10 +788,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         }
         // ---- compact x work of the E terms (Eyx, Ezx) on this warp's row ----
         if (AX) {
-          const bool have = xq_ke == k;
-          const bool ahead = k + 1 < k1;
-          // Pending: this plane's E group, then the next plane's H group (newest).
-          async_wait(have && ahead);
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int w = sm.xst[6 + h][lane];
@@ -770,16 +800,14 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               // Beyond x = 0 the ghost: zero on a metallic wall, else the edge value.
               const float dv = (at_x0 && xo == 0) ? (wx0 ? Hrow[c] : 0.0f) : Hrow[c] - Hrow[c - 1];
               const int off = (k * d.pdy + j) * d.pdx + slot;
-              const float psi = (h == 0 && have) ? sm.xpf[k & 1][1][tid] : d.psi_in[off];
-              if (h == 0 && ahead) async_copy4(&sm.xpf[(k + 1) & 1][1][tid], d.psi_in + off + d.pdy * d.pdx);
+              const int t = second ? 3 : 2;
+              const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
               d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
-          if (ahead) async_commit();
-          xq_ke = k + 1;
           __syncwarp();
         }
         // ---- E on the own row ----
@@ -856,14 +884,16 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         hyp = hy;
         hxXp = hxX;
       };
+      using std::integral_constant;
       if constexpr (!Cpml) {
-        if (xface || yface) body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{});
-        else body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{});
+        if (xface || yface) body(integral_constant<int, 8>{});
+        else body(integral_constant<int, 0>{});
       } else {
         shell_z = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
-        if (shell_x || shell_y || shell_z) body(std::true_type{}, std::true_type{}, std::true_type{}, std::true_type{});
-        else if (xface || yface) body(std::false_type{}, std::false_type{}, std::false_type{}, std::true_type{});
-        else body(std::false_type{}, std::false_type{}, std::false_type{}, std::false_type{});
+        if (shell_y || shell_z) body(integral_constant<int, 16 | 8 | 7>{});  // y / z slabs (and x)
+        else if (shell_x) body(integral_constant<int, 8 | 1>{});           // x slab tiles (about half)
+        else if (xface || yface) body(integral_constant<int, 8>{});
+        else body(integral_constant<int, 0>{});
       }
     } else {
       // ---- general tile-plane: per cell, every validity / ghost / PEC rule ---
@@ -980,7 +1010,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     e1 = e1 == 2 ? 0 : e1 + 1;
     hs ^= 1;
   }
-  if (Cpml) async_wait(false);  // no copy into shared memory outlives the CTA
 }
 
 template <int NW, bool Cpml, bool Exact>
@@ -998,10 +1027,31 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
   const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;  // a multiple of 128 leaves column X to lane 31
-  const dim3 grid(gx, (p.Y + 1 + T::TY - 1) / T::TY, (kmax + zc - 1) / zc);
+  const int gy = (p.Y + 1 + T::TY - 1) / T::TY, gz = (kmax + zc - 1) / zc;
   Step3D q = p;
   q.z_chunk = zc;
-  kern<<<grid, dim3(32, NW, 1), smem, s>>>(maps, q);
+  // Absorber rows and chunks at both ends (the tile test of the kernel's ay
+  // and per-plane shell_z): dispatched first.
+  auto row_shell = [&](int b) {
+    const int j0 = b * T::TY;
+    return p.cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + T::TY <= p.cpml_inner[1][1]);
+  };
+  auto chunk_shell = [&](int c) {
+    const int k0 = c * zc, k1 = std::min(k0 + zc, kmax);
+    return p.cpml && (k0 < p.cpml_inner[0][0] || k1 > p.cpml_inner[0][1]);
+  };
+  int ylo = 0, yhi = gy, zlo = 0, zhi = gz;
+  while (ylo < gy && row_shell(ylo)) ++ylo;
+  while (yhi > ylo && row_shell(yhi - 1)) --yhi;
+  while (zlo < gz && chunk_shell(zlo)) ++zlo;
+  while (zhi > zlo && chunk_shell(zhi - 1)) --zhi;
+  q.order[0] = ylo;
+  q.order[1] = yhi;
+  q.order[2] = zlo;
+  q.order[3] = zhi;
+  const long long ctas = static_cast<long long>(gx) * gy * gz;
+  if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  kern<<<dim3(static_cast<unsigned>(ctas), 1, 1), dim3(32, NW, 1), smem, s>>>(maps, q);
   return cudaPeekAtLastError();
 }
 
@@ -1022,8 +1072,27 @@ cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
   if (!tma::encode(&maps.ids, CU_TENSOR_MAP_DATA_TYPE_UINT8, p.site_class, p.X + 1, p.Y + 1, p.Z + 1, P8,
                    P8 * (p.Y + 1), T::TX, T::TY))
     return cudaErrorInvalidValue;
-  if (p.fast_math) return p.cpml ? launch_class_t<NW, true, false>(s, maps, p) : launch_class_t<NW, false, false>(s, maps, p);
-  return p.cpml ? launch_class_t<NW, true, true>(s, maps, p) : launch_class_t<NW, false, true>(s, maps, p);
+  // x-term psi slabs (Hyx, Hzx, Eyx, Ezx): (plane, row, slot) with rows of
+  // low + high slots.  Staged only when every row is a multiple of 16 bytes
+  // and every slab 16-byte aligned (TMA's stride and base rules).
+  Step3D q = p;
+  q.xstage = 0;
+  if (p.cpml) {
+    const CpmlTermDev* xt[4] = {&p.ht[3], &p.ht[4], &p.et[3], &p.et[4]};
+    const int comp[4] = {4, 5, 1, 2};  // Hy, Hz, Ey, Ez
+    bool ok = true;
+    for (int t = 0; t < 4 && ok; ++t) {
+      const CpmlTermDev& d = *xt[t];
+      const int w = d.low + d.high;
+      const Dims dc = component_dims(comp[t], p.Z, p.Y, p.X);
+      ok = w > 0 && w % 4 == 0 && d.pdx == w && (reinterpret_cast<uintptr_t>(d.psi_in) & 15) == 0 &&
+           tma::encode(&maps.xpsi[t], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d.psi_in, w, d.pdy, dc.z, int64_t(w) * 4,
+                       int64_t(w) * 4 * d.pdy, T::XW, T::HH);
+    }
+    q.xstage = ok ? 1 : 0;
+  }
+  if (q.fast_math) return q.cpml ? launch_class_t<NW, true, false>(s, maps, q) : launch_class_t<NW, false, false>(s, maps, q);
+  return q.cpml ? launch_class_t<NW, true, true>(s, maps, q) : launch_class_t<NW, false, true>(s, maps, q);
 }
 
 }  // namespace

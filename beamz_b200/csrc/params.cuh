@@ -67,6 +67,11 @@ struct Step3D {
   int pitch8;
   const float4* class_coef;
   int fast_math;  // tolerance arithmetic in the class step (1/dx folded, fused multiply-adds)
+  // Class step dispatch order (longest first): tile rows [0, order[0]) and
+  // [order[1], rows) and z chunks [0, order[2]) and [order[3], chunks) hold
+  // absorber cells; their CTAs are dispatched before the others.
+  int order[4];
+  int xstage;  // class step: the x-term psi slabs have tensor maps (staged with each plane's bundle)
   // Derivative metrics per axis (z, y, x), or null (isotropic: divide by res).
   const float* metric_h[3];  // [n_axis]: forward differences feeding H
   const float* metric_e[3];  // [n_axis + 1]: backward differences feeding E
