@@ -18,8 +18,12 @@
 //    (Ex, Ey, Ez) coefficient triple of the codebook), 1 byte per cell instead
 //    of a 4-byte codebook word, with the class table in shared memory;
 //  * the CPML recurrences of a row's x-slab cells are shared by the row's warp
-//    (one cell per lane) instead of falling on the few lanes that own them,
-//    and every psi load of a plane is issued ahead of its first use.
+//    (one cell per lane) instead of falling on the few lanes that own them;
+//    their psi rows ride in the plane's TMA bundle (a 16-slot window per x
+//    term), so an x-slab tile never waits on a psi load; the y / z terms' psi
+//    loads of a plane are all issued at its top;
+//  * CTAs are dispatched longest first (absorber tile rows, then absorber z
+//    chunks, then the interior), so that the last wave is not absorber-heavy.
 //
 // Arithmetic: beamz's float32 order bit for bit (every difference divided by
 // the cell size with a correctly rounded quotient, every product and sum
@@ -28,10 +32,14 @@
 // coefficients (dt/(mu0 dx) for H, dt/(eps0 eps dx) per class for E, a/dx for
 // the CPML) and explicit fused multiply-adds.
 //
-// Tile-planes that touch a high domain face, a z face, an H source or a
-// partial tile run a general per-cell path with every validity, ghost and PEC
-// rule; the rest run one of three straight bodies: the interior, the x = 0 /
-// y = 0 faces, and the absorber shell (its axes plane-uniform run-time flags).  The H-term CPML memories are double-banked (the halo
+// Tile-planes that touch a z face, an H source or a partial x tile run a
+// general per-cell path with every validity, ghost and PEC rule; the rest run
+// a straight body compiled for their case: the interior, the x = 0 / y = 0
+// faces, the x-slab tiles (about half of them on a 512-wide grid), the other
+// absorber tiles (axes as plane-uniform run-time flags), and the last tile
+// row, shifted down to end at row Y (where Hx, Hz and Ey do not exist and the
+// y = Y ghost applies) with its rows below the tile row before computed but
+// not stored.  The H-term CPML memories are double-banked (the halo
 // recomputation reads them), the E-term ones updated in place.
 //
 // Operation order follows beamz/simulation/kernels.py:458-626 (H from E with
@@ -419,7 +427,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int Z = p.Z, Y = p.Y, X = p.X;
   const int gx = X % TX == 0 ? X / TX : X / TX + 1, gy = (Y + TY) / TY, gz = (Z + p.z_chunk) / p.z_chunk;
   const TileIdx tile = tile_of(blockIdx.x, gx, gy, gz, p.order);
-  const int i0 = tile.x * TX, j0 = tile.y * TY;
+  // The last tile row, when it would hold rows past Y, is shifted down to
+  // end at row Y (j0 = Y + 1 - TY) so that it runs a straight body; its rows
+  // below jown belong to the tile row before and are computed, not stored.
+  const int jown = tile.y * TY;
+  const bool ylast = jown + TY > Y && Y + 1 >= TY;
+  const int i0 = tile.x * TX, j0 = ylast ? Y + 1 - TY : jown;
   const int k0 = tile.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, Z + 1);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
@@ -525,7 +538,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int i = i0 + 4 * lane;         // its lattice x
   const int rc = r * BX + c0;
   const bool xl = xcol && lane == 31;
-  const bool fast_ok0 = j0 + TY <= Y && i0 + TX <= X && cc_smem;
+  const bool fast_ok0 = (j0 + TY <= Y || ylast) && i0 + TX <= X && cc_smem;
+  const bool own = j >= jown;  // this warp's row is the tile's to store
   const bool xface = i0 == 0, yface = j0 == 0;
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
   const bool fast_ok = fast_ok0 && (!ax || xcompact);
@@ -599,6 +613,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         // rare combinations share that body).
         constexpr int M = decltype(mode)::value;
         constexpr bool SX = M & 1, SY = M & 2, SZ = M & 4, FC = M & 8, RT = M & 16;
+        // Bit 5, or the run-time body on the last tile row: own rows from
+        // jown, row Y in warp TY-1 (Hx, Hz and Ey do not exist there and the
+        // y = Y ghost applies).
+        constexpr bool LY = M & 32;
+        const bool lyr = LY || (RT && ylast);
+        const bool st = !lyr || own;       // this row is stored
+        const bool rowY = lyr && j == Y;   // row Y: Hx, Hz, Ey absent
         const bool AX = SX && (!RT || shell_x), AY = SY && (!RT || shell_y), AZ = SZ && (!RT || shell_z);
         const bool at_x0 = FC && xface, at_y0 = FC && yface;
         const int jh = j0 - 1, ih = i0 - 1;  // the halo row and column
@@ -612,12 +633,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
         // psi of the H terms: own cells, halos, column X.
         float4 qh0, qh1, qh2, qh5;
-        if (AY) {
+        if (AY && !rowY) {
           qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
           qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
         }
         if (AZ) {
-          qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
+          if (!rowY) qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
           qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
         }
         // psi of the E terms too: in flight through the whole H phase.
@@ -629,7 +650,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           }
           if (AZ) {
             qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
-            qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
+            if (!rowY) qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
           }
         }
         // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
@@ -637,7 +658,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int w = sm.xst[4 + h][lane];
-            if (w & 1) {
+            if ((w & 1) && !(rowY && (w & 2))) {
               const bool second = w & 2;  // Hzx (dEy/dx), else Hyx (dEz/dx)
               const int slot = (w >> 2) & 63, xo = w >> 8;
               const CpmlTermDev& d = second ? p.ht[4] : p.ht[3];
@@ -648,7 +669,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
-              if (emit) d.psi_out[off] = nv;
+              if (emit && st) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
@@ -667,13 +688,14 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy0 = D4(sub4(ld4(E1x + rc), ex)), dy1 = D4(sub4(next4(ez, ez4), ez));       // Hy: dEx/dz, dEz/dx
           dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(ld4(E0x + rc + BX), ex));  // Hz: dEy/dx, dEx/dy
         }
-        if (AY) {
-          dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit);
-          dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit);
+        if (AY && !rowY) {
+          dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit && st);
+          dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit && st);
         }
         if (AZ) {
-          dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit);
-          dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit);
+          if (!rowY)
+            dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit && st);
+          dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit && st);
         }
         if (AX) {
           dy1 = xtake(dy1, sm.xst[0][lane], sm.xd[0][warp]);
@@ -684,28 +706,29 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const float4 hz = h4<Exact>(ld4(HOz + rc), sm.hcoef[2], sm.hcoef[5], dz0, dz1);
         if (at_x0 && lane == 0 && wx0) hx.x = 0.0f;  // PEC: normal H on the x = 0 wall
         if (at_y0 && warp == 0 && wy0) hy = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rowY && wy1) hy = make_float4(0.f, 0.f, 0.f, 0.f);  // PEC: normal H on the y = Y wall
         st4(&sm.hn[0][r][c0], hx);
         st4(&sm.hn[1][r][c0], hy);
         st4(&sm.hn[2][r][c0], hz);
         const int o = k * PL + j * P + i;
-        if (emit) {
-          st4(p.hout[0] + o, hx);
+        if (emit && st) {
+          if (!rowY) st4(p.hout[0] + o, hx);
           st4(p.hout[1] + o, hy);
-          st4(p.hout[2] + o, hz);
+          if (!rowY) st4(p.hout[2] + o, hz);
         }
         // Hx on column X (lane 31 of the last tile).
         float hxX = 0.0f;
-        if (xl) {
+        if (xl && !rowY) {
           const int b = rc + 4;
           float qX0 = 0.f, qX1 = 0.f;
           if (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
           if (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
           float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
-          if (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit);
-          if (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit);
+          if (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit && st);
+          if (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit && st);
           hxX = wx1 ? 0.0f : h1<Exact>(HOx[b], sm.hcoef[0], sm.hcoef[3], d0, d1);
           sm.hn[0][r][XC] = hxX;
-          if (emit) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
+          if (emit && st) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
         }
         // ---- recomputed halo: row j0-1 (Hx by warp 0, Hz by warp 1) and
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
@@ -754,27 +777,28 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), sm.hcoef[2], sm.hcoef[5], d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
+          const bool hz_ok = !(lyr && jc == Y);  // Hz has no row Y
           float qc0 = 0.f, qc1 = 0.f, qc2 = 0.f, qc3 = 0.f;
           if (AZ) qc0 = psi1_fetch<0>(p.ht[2], k, jc, ih);
           if (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
-          if (AX) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
-          if (AY) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
+          if (AX && hz_ok) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
+          if (AY && hz_ok) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
           float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
           if (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
           if (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
           float hyv = h1<Exact>(HOy[b], sm.hcoef[1], sm.hcoef[4], d0, d1);
           if (at_y0 && jc == 0 && wy0) hyv = 0.0f;
           float f0 = D1(E0y[b + 1] - E0y[b]), f1 = D1(E0x[b + BX] - E0x[b]);  // Hz: dEy/dx, dEx/dy
-          if (AX) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
-          if (AY) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
+          if (AX && hz_ok) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
+          if (AY && hz_ok) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
           sm.hn[1][rr][3] = hyv;
           sm.hn[2][rr][3] = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], f0, f1);
         }
         float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
         if (emit) {
           if (xl) {
-            if (AZ) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
-            if (AX) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
+            if (AZ && !rowY) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
+            if (AX && !rowY) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
             if (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
             if (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
           }
@@ -791,7 +815,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int w = sm.xst[6 + h][lane];
-            if (w & 1) {
+            if ((w & 1) && !(rowY && !(w & 2))) {
               const bool second = w & 2;  // Ezx (dHy/dx), else Eyx (dHz/dx)
               const int slot = (w >> 2) & 63, xo = w >> 8;
               const CpmlTermDev& d = second ? p.et[4] : p.et[3];
@@ -804,7 +828,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
               const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
-              d.psi_out[off] = nv;
+              if (st) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
           }
@@ -828,13 +852,19 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         float4 fx0 = D4(sub4(hz, hzy)), fx1 = D4(sub4(hy, hyp));              // Ex: dHz/dy, dHy/dz
         float4 fy0 = D4(sub4(hx, hxp)), fy1 = D4(sub4(hz, prev4(hzl, hz)));   // Ey: dHx/dz, dHz/dx
         float4 fz0 = D4(sub4(hy, prev4(hyl, hy))), fz1 = D4(sub4(hx, hxy));   // Ez: dHy/dx, dHx/dy
+        if (rowY) {  // ghost beyond y = Y: zero on a metallic wall, else the edge value
+          const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+          fx0 = D4(wy1 ? sub4(z4, hzy) : z4);
+          fz1 = D4(wy1 ? sub4(z4, hxy) : z4);
+        }
         if (AY) {
-          fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, true);
-          fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, true);
+          fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, st);
+          fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, st);
         }
         if (AZ) {
-          fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, true);
-          fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, true);
+          fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, st);
+          if (!rowY)
+            fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, st);
         }
         if (AX) {
           fy1 = xtake(fy1, sm.xst[2][lane], sm.xd[0][warp]);
@@ -858,27 +888,34 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           ny.x = 0.0f;
           nz.x = 0.0f;
         }
-        st4(p.eout[0] + o, nx);
-        st4(p.eout[1] + o, ny);
-        st4(p.eout[2] + o, nz);
-        if (xl) {  // Ey, Ez on column X
+        if (rowY && wy1) {  // Ex, Ez on the y = Y wall
+          nx = make_float4(0.f, 0.f, 0.f, 0.f);
+          nz = nx;
+        }
+        if (st) {
+          st4(p.eout[0] + o, nx);
+          if (!rowY) st4(p.eout[1] + o, ny);
+          st4(p.eout[2] + o, nz);
+        }
+        if (xl && st) {  // Ey, Ez on column X
           const int b = rc + 4, oX = o + 4;
           float hxy_X = sm.hn[0][r - 1][XC];
           if (at_y0 && warp == 0) hxy_X = wy0 ? 0.0f : hxX;
           // The Hz / Hy ghosts beyond x = X: zero on a metallic wall, else the edge value.
           float g0 = D1(hxX - hxXp), g1 = D1(wx1 ? 0.0f - hz.w : 0.0f);   // Ey: dHx/dz, dHz/dx
           float h0 = D1(wx1 ? 0.0f - hy.w : 0.0f), h1v = D1(hxX - hxy_X);  // Ez: dHy/dx, dHx/dy
-          if (AZ) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
+          if (rowY) h1v = D1(wy1 ? 0.0f - hxy_X : 0.0f);                    // the y = Y ghost
+          if (AZ && !rowY) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
           if (AX) {
-            g1 = psi1_apply<Exact, 2>(p.et[3], sm.cc[9], qY3, k, j, X, res, g1, true);
+            if (!rowY) g1 = psi1_apply<Exact, 2>(p.et[3], sm.cc[9], qY3, k, j, X, res, g1, true);
             h0 = psi1_apply<Exact, 2>(p.et[4], sm.cc[10], qY4, k, j, X, res, h0, true);
           }
           if (AY) h1v = psi1_apply<Exact, 1>(p.et[5], sm.cc[11], qY5, k, j, X, res, h1v, true);
           const float4 t = sm.cls[cidX];
           const float ny_ = e_upd<Exact>(E0y[b], t.y, g0, g1);
           const float nz_ = e_upd<Exact>(E0z[b], t.z, h0, h1v);
-          p.eout[1][oX] = wx1 ? 0.0f : ny_;
-          p.eout[2][oX] = (wx1 || (at_y0 && warp == 0 && wy0)) ? 0.0f : nz_;
+          if (!rowY) p.eout[1][oX] = wx1 ? 0.0f : ny_;
+          p.eout[2][oX] = (wx1 || (at_y0 && warp == 0 && wy0) || (rowY && wy1)) ? 0.0f : nz_;
         }
         hxp = hx;
         hyp = hy;
@@ -886,11 +923,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       };
       using std::integral_constant;
       if constexpr (!Cpml) {
-        if (xface || yface) body(integral_constant<int, 8>{});
+        if (ylast) body(integral_constant<int, 32 | 8>{});
+        else if (xface || yface) body(integral_constant<int, 8>{});
         else body(integral_constant<int, 0>{});
       } else {
         shell_z = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
-        if (shell_y || shell_z) body(integral_constant<int, 16 | 8 | 7>{});  // y / z slabs (and x)
+        if (ylast || shell_y || shell_z) body(integral_constant<int, 16 | 8 | 7>{});  // last row, y / z slabs
         else if (shell_x) body(integral_constant<int, 8 | 1>{});           // x slab tiles (about half)
         else if (xface || yface) body(integral_constant<int, 8>{});
         else body(integral_constant<int, 0>{});
@@ -985,8 +1023,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         }
       };
 #pragma unroll 1
-      for (int q = 0; q < 4; ++q) h_cell(r, c0 + q, 7, emit);
-      if (xl) h_cell(r, XC, 1, emit);
+      for (int q = 0; q < 4; ++q) h_cell(r, c0 + q, 7, emit && own);
+      if (xl) h_cell(r, XC, 1, emit && own);
       if (emit) {
         if (warp == 0 && j0 > 0) {
 #pragma unroll 1
@@ -997,7 +1035,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         }
       }
       __syncthreads();
-      if (emit) {
+      if (emit && own) {
 #pragma unroll 1
         for (int q = 0; q < 4; ++q) e_cell(r, c0 + q, get(hxp, q), get(hyp, q));
         if (xl) e_cell(r, XC, hxXp, 0.0f);
