@@ -319,7 +319,7 @@ class DeviceProgram:
 
     def __init__(self, spec: ProgramSpec, device="cuda", schedule="fused", tile=(32, 8), z_chunk=16,
                  graphs=True, layout="auto", dft_batch: int = 16, dft_overlap: bool = True,
-                 arithmetic: str = "exact", step_kernel: str = "codebook", wait_limit_ns: int = 0,
+                 arithmetic: str = "exact", step_kernel: str = "classes", wait_limit_ns: int = 0,
                  test_stall: bool = False):
         self.lib = abi.load_library()
         self.device = _require_cuda(device)
