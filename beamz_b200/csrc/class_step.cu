@@ -70,7 +70,6 @@ struct ClassTile {
   static constexpr int EBOX = ((EH * BX + 31) / 32) * 32;  // floats; every box starts on 128 B
   static constexpr int HBOX = ((HH * BX + 31) / 32) * 32;
   static constexpr int IBOX = TY * TX;  // class ids (bytes), rows j0 .. j0+TY-1, x i0 .. i0+127
-  static constexpr int XC = 4 + TX;     // box column of x = i0 + 128 (column X of the last tile)
   static constexpr int XW = 16;         // staged x-psi window (slots)
   static constexpr int XPS = ((HH * XW + 31) / 32) * 32;
   struct Smem {
@@ -143,12 +142,6 @@ __device__ __forceinline__ float4 next4(float4 v, float n) { return make_float4(
 // (p, v.x, v.y, v.z): the x-1 neighbours.
 __device__ __forceinline__ float4 prev4(float p, float4 v) { return make_float4(p, v.x, v.y, v.z); }
 __device__ __forceinline__ float get(const float4& v, int q) { return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w)); }
-__device__ __forceinline__ void put(float4& v, int q, float s) {
-  if (q == 0) v.x = s;
-  else if (q == 1) v.y = s;
-  else if (q == 2) v.z = s;
-  else v.w = s;
-}
 
 // ---- arithmetic ------------------------------------------------------------
 // Exact: beamz's float32 order (kernels.py:458-626): every difference divided
@@ -419,7 +412,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     class_step_kernel(const __grid_constant__ ClassMaps maps, const __grid_constant__ Step3D p) {
   using T = ClassTile<NW>;
   using S = typename T::Smem;
-  constexpr int BX = T::BX, TX = T::TX, TY = T::TY, XC = T::XC;
+  constexpr int BX = T::BX, TX = T::TX, TY = T::TY;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   S& sm = *reinterpret_cast<S*>(smem_raw);
   const int lane = threadIdx.x, warp = threadIdx.y;
@@ -440,11 +433,9 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const float res = p.res, inv_res = p.inv_res;
   const unsigned long long wait_ns = p.wait_ns;
 
-  // When X is a multiple of 128 the last tile also owns column X (Hx, Ey, Ez
-  // there), done by lane 31, so no CTA is spent on one column.
-  const bool xcol = X % TX == 0 && i0 + TX == X;
-  const int xe = xcol ? 1 : 0;
-  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX + xe <= p.cpml_inner[2][1]);
+  // When X is a multiple of 128 the tiles end at x = X - 1 and column X (Hx,
+  // Ey, Ez there) is the column kernel's, launched before this one.
+  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX <= p.cpml_inner[2][1]);
   // Compact x work: in a tile that touches an x slab, the recurrences of a
   // row's x-slab cells are shared by the row's warp -- each lane takes items
   // lane and lane + 32 of the row's (term, slot) list, the first x term's
@@ -537,19 +528,19 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int c0 = 4 + 4 * lane;         // own first column in the boxes and hn
   const int i = i0 + 4 * lane;         // its lattice x
   const int rc = r * BX + c0;
-  const bool xl = xcol && lane == 31;
   const bool fast_ok0 = (j0 + TY <= Y || ylast) && i0 + TX <= X && cc_smem;
   const bool own = j >= jown;  // this warp's row is the tile's to store
   const bool xface = i0 == 0, yface = j0 == 0;
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
   const bool fast_ok = fast_ok0 && (!ax || xcompact);
   const bool shell_x = ax, shell_y = ay;  // the tile's absorber axes (z is per plane)
+
   // Tile-constant x state per lane, in shared memory so that it holds no
   // register outside the x work: the x-slab masks of the own cells for Hyx,
   // Hzx, Eyx, Ezx (xslab_of) and the lane's compact items, packed as valid |
   // second term << 1 | slot << 2 | (x - i0) << 8 (items lane and lane + 32 of
-  // the H terms' list, then of the E terms').  Column X is lane 31's own work,
-  // so the items stop short of it.
+  // the H terms' list, then of the E terms').  The items stop at the tile's
+  // last column (column X is the column kernel's).
   if (xcompact && warp == 0) {
     auto pack = [&](const CpmlTermDev& t3, const CpmlTermDev& t4, int q) {
       const XItems a3 = x_items(t3, i0, i0 + TX), a4 = x_items(t4, i0, i0 + TX);
@@ -573,7 +564,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 
   // H of the previous plane on the own cells (the z-backward differences of E).
   float4 hxp = make_float4(0.f, 0.f, 0.f, 0.f), hyp = hxp;
-  float hxXp = 0.0f;
 
   int e0 = kstart % 3, e1 = (kstart + 1) % 3, hs = kstart & 1;
   for (int k = kstart; k < k1; ++k) {
@@ -629,8 +619,6 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const bool halo_col = emit && warp == 2 && lane < TY && !at_x0;   // Hy, Hz on column i0-1
         const int jc = j0 + lane;                                         // halo_col's row
         // ---- every global load of the plane goes out first ----
-        // Class id of column X (lane 31 of the last tile).
-        const int cidX = xl && emit ? p.site_class[(k * (Y + 1) + j) * p.pitch8 + X] : 0;
         // psi of the H terms: own cells, halos, column X.
         float4 qh0, qh1, qh2, qh5;
         if (AY && !rowY) {
@@ -716,45 +704,19 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           st4(p.hout[1] + o, hy);
           if (!rowY) st4(p.hout[2] + o, hz);
         }
-        // Hx on column X (lane 31 of the last tile).
-        float hxX = 0.0f;
-        if (xl && !rowY) {
-          const int b = rc + 4;
-          float qX0 = 0.f, qX1 = 0.f;
-          if (AY) qX0 = psi1_fetch<1>(p.ht[0], k, j, X);
-          if (AZ) qX1 = psi1_fetch<0>(p.ht[1], k, j, X);
-          float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
-          if (AY) d0 = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qX0, k, j, X, res, d0, emit && st);
-          if (AZ) d1 = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qX1, k, j, X, res, d1, emit && st);
-          hxX = wx1 ? 0.0f : h1<Exact>(HOx[b], sm.hcoef[0], sm.hcoef[3], d0, d1);
-          sm.hn[0][r][XC] = hxX;
-          if (emit && st) p.hout[0][o + 4] = hxX;  // lane 31: i + 4 = X
-        }
         // ---- recomputed halo: row j0-1 (Hx by warp 0, Hz by warp 1) and
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
         if (halo_row_x) {
           const int b = c0;
           float4 qa, qb;
-          float qR0 = 0.f, qR1 = 0.f;
           if (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
           if (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
-          if (xl) {
-            if (AY) qR0 = psi1_fetch<1>(p.ht[0], k, jh, X);
-            if (AZ) qR1 = psi1_fetch<0>(p.ht[1], k, jh, X);
-          }
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
           if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
           if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
           float4 h = h4<Exact>(ld4(HOx + b), sm.hcoef[0], sm.hcoef[3], d0, d1);
           if (at_x0 && lane == 0 && wx0) h.x = 0.0f;
           st4(&sm.hn[0][0][b], h);
-          if (xl) {
-            const int bb = XC;
-            float e0v = D1(E0z[bb + BX] - E0z[bb]), e1v = D1(E1y[bb] - E0y[bb]);
-            if (AY) e0v = psi1_apply<Exact, 1>(p.ht[0], sm.cc[0], qR0, k, jh, X, res, e0v, false);
-            if (AZ) e1v = psi1_apply<Exact, 0>(p.ht[1], sm.cc[1], qR1, k, jh, X, res, e1v, false);
-            sm.hn[0][0][XC] = wx1 ? 0.0f : h1<Exact>(HOx[bb], sm.hcoef[0], sm.hcoef[3], e0v, e1v);
-          }
         } else if (halo_row_z) {
           const int b = c0;
           float4 qa, qb;
@@ -794,20 +756,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           sm.hn[1][rr][3] = hyv;
           sm.hn[2][rr][3] = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], f0, f1);
         }
-        float qY2 = 0.f, qY3 = 0.f, qY4 = 0.f, qY5 = 0.f;
-        if (emit) {
-          if (xl) {
-            if (AZ && !rowY) qY2 = psi1_fetch<0>(p.et[2], k, j, X);
-            if (AX && !rowY) qY3 = psi1_fetch<2>(p.et[3], k, j, X);
-            if (AX) qY4 = psi1_fetch<2>(p.et[4], k, j, X);
-            if (AY) qY5 = psi1_fetch<1>(p.et[5], k, j, X);
-          }
-        }
         __syncthreads();
         if (!emit) {
           hxp = hx;
           hyp = hy;
-          hxXp = hxX;
           return;
         }
         // ---- compact x work of the E terms (Eyx, Ezx) on this warp's row ----
@@ -897,29 +849,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if (!rowY) st4(p.eout[1] + o, ny);
           st4(p.eout[2] + o, nz);
         }
-        if (xl && st) {  // Ey, Ez on column X
-          const int b = rc + 4, oX = o + 4;
-          float hxy_X = sm.hn[0][r - 1][XC];
-          if (at_y0 && warp == 0) hxy_X = wy0 ? 0.0f : hxX;
-          // The Hz / Hy ghosts beyond x = X: zero on a metallic wall, else the edge value.
-          float g0 = D1(hxX - hxXp), g1 = D1(wx1 ? 0.0f - hz.w : 0.0f);   // Ey: dHx/dz, dHz/dx
-          float h0 = D1(wx1 ? 0.0f - hy.w : 0.0f), h1v = D1(hxX - hxy_X);  // Ez: dHy/dx, dHx/dy
-          if (rowY) h1v = D1(wy1 ? 0.0f - hxy_X : 0.0f);                    // the y = Y ghost
-          if (AZ && !rowY) g0 = psi1_apply<Exact, 0>(p.et[2], sm.cc[8], qY2, k, j, X, res, g0, true);
-          if (AX) {
-            if (!rowY) g1 = psi1_apply<Exact, 2>(p.et[3], sm.cc[9], qY3, k, j, X, res, g1, true);
-            h0 = psi1_apply<Exact, 2>(p.et[4], sm.cc[10], qY4, k, j, X, res, h0, true);
-          }
-          if (AY) h1v = psi1_apply<Exact, 1>(p.et[5], sm.cc[11], qY5, k, j, X, res, h1v, true);
-          const float4 t = sm.cls[cidX];
-          const float ny_ = e_upd<Exact>(E0y[b], t.y, g0, g1);
-          const float nz_ = e_upd<Exact>(E0z[b], t.z, h0, h1v);
-          if (!rowY) p.eout[1][oX] = wx1 ? 0.0f : ny_;
-          p.eout[2][oX] = (wx1 || (at_y0 && warp == 0 && wy0) || (rowY && wy1)) ? 0.0f : nz_;
-        }
         hxp = hx;
         hyp = hy;
-        hxXp = hxX;
       };
       using std::integral_constant;
       if constexpr (!Cpml) {
@@ -1024,12 +955,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       };
 #pragma unroll 1
       for (int q = 0; q < 4; ++q) h_cell(r, c0 + q, 7, emit && own);
-      if (xl) h_cell(r, XC, 1, emit && own);
       if (emit) {
         if (warp == 0 && j0 > 0) {
 #pragma unroll 1
           for (int q = 0; q < 4; ++q) h_cell(0, c0 + q, 1 | 4, false);
-          if (xl) h_cell(0, XC, 1, false);
         } else if (warp == 2 && lane < TY && i0 > 0) {
           h_cell(1 + lane, 3, 2 | 4, false);
         }
@@ -1038,15 +967,167 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       if (emit && own) {
 #pragma unroll 1
         for (int q = 0; q < 4; ++q) e_cell(r, c0 + q, get(hxp, q), get(hyp, q));
-        if (xl) e_cell(r, XC, hxXp, 0.0f);
       }
       hxp = ld4(&sm.hn[0][r][c0]);
       hyp = ld4(&sm.hn[1][r][c0]);
-      if (xl) hxXp = sm.hn[0][r][XC];
     }
     e0 = e1;
     e1 = e1 == 2 ? 0 : e1 + 1;
     hs ^= 1;
+  }
+}
+
+
+
+// ---- column x = X ------------------------------------------------------------
+// When X is a multiple of 128 the tiles end at x = X - 1 and this kernel, run
+// before the class step on the same stream, updates the lattice column x = X:
+// Hx there, then Ey and Ez, with the general path's per-cell rules (ghosts,
+// PEC, CPML, H sources).  It reads only the step's inputs, so it depends on no
+// other launch of the step: the H of x = X - 1 that Ey and Ez see through the
+// ghost beyond x = X counts only with a metallic x = X wall, and is then
+// recomputed here from the same inputs with the class step's arithmetic.  A
+// block covers 32 rows x 8 planes and recomputes the Hx of the row before and
+// of the plane before read-only; every load of a thread goes out before the
+// first use, so the column costs about one memory round trip.  (Done inside
+// the tiles, by one lane or one warp, the column put its psi latency on the
+// critical path of a quarter of the CTAs: 12-15 % of the 512 x 512 x 256 step.)
+constexpr int kColJ = 32, kColK = 8;
+
+// One CPML term at a cell of the column: psi <- b psi + a d, d' = d / kappa +
+// psi, with the coefficients as the class step stages them.
+template <bool Exact, int Axis>
+__device__ __forceinline__ float col_cpml(const CpmlTermDev& t, float res, float inv_res, float psi_old, int k, int j,
+                                          int x, float d, bool write) {
+  const int slot = slot_of(t, Axis == 0 ? k : (Axis == 1 ? j : x));
+  if (slot < 0) return d;
+  const float4 c = make_float4(Exact ? __ldg(t.a + slot) : __ldg(t.a + slot) * inv_res, __ldg(t.b + slot),
+                               __ldg(t.k + slot), 0.0f);
+  float n;
+  const float r = cpml_d<Exact>(c, res, psi_old, d, &n);
+  if (write) t.psi_out[psi_off<Axis>(t, slot, k, j, x)] = n;
+  return r;
+}
+
+// psi of a term at a cell, 0 outside its slab.
+template <int Axis>
+__device__ __forceinline__ float col_psi(const CpmlTermDev& t, int k, int j, int x) {
+  const int slot = slot_of(t, Axis == 0 ? k : (Axis == 1 ? j : x));
+  return slot >= 0 ? t.psi_in[psi_off<Axis>(t, slot, k, j, x)] : 0.0f;
+}
+
+template <bool Cpml, bool Exact>
+__global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __grid_constant__ Step3D p) {
+  __shared__ float hx[kColK + 1][kColJ + 1];  // new Hx at (k0 - 1 + a, j0 - 1 + b, X)
+  __shared__ float amp[kMaxFusedSources];
+  const int Z = p.Z, Y = p.Y, X = p.X;
+  const int j0 = blockIdx.x * kColJ, k0 = blockIdx.y * kColK;
+  const int tid = threadIdx.y * kColJ + threadIdx.x;
+  const int P = p.pitch, PL = (Y + 1) * p.pitch;  // element offsets < 2^31 (validated)
+  const float res = p.res, inv_res = p.inv_res;
+  const float dbs = p.div_bs, drs = p.div_rs;
+  const bool wz0 = wall(p.metallic, 0, false), wz1 = wall(p.metallic, 0, true);
+  const bool wy0 = wall(p.metallic, 1, false), wy1 = wall(p.metallic, 1, true);
+  const bool wx0 = wall(p.metallic, 2, false), wx1 = wall(p.metallic, 2, true);
+  auto D1 = [&](float v) { return dv<Exact>(v, dbs, drs); };
+  // This thread's E cell (k, j, X): its inputs are loaded first.
+  const int k = k0 + threadIdx.y, j = j0 + threadIdx.x;
+  const bool live = k <= Z && j <= Y;
+  const bool ey_ok = live && j < Y, ez_ok = live && k < Z;
+  const int o = live ? k * PL + j * P + X : 0;
+  const float ey0 = ey_ok ? p.ein[1][o] : 0.0f, ez0 = ez_ok ? p.ein[2][o] : 0.0f;
+  const float4 t = live ? p.class_coef[p.site_class[(static_cast<int64_t>(k) * (Y + 1) + j) * p.pitch8 + X]]
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+  float q_eyz = 0.f, q_eyx = 0.f, q_ezx = 0.f, q_ezy = 0.f;
+  if (Cpml) {
+    if (ey_ok) {
+      q_eyz = col_psi<0>(p.et[2], k, j, X);
+      q_eyx = col_psi<2>(p.et[3], k, j, X);
+    }
+    if (ez_ok) {
+      q_ezx = col_psi<2>(p.et[4], k, j, X);
+      q_ezy = col_psi<1>(p.et[5], k, j, X);
+    }
+  }
+  if (tid < p.n_hsrc) amp[tid] = source_amplitude(p.hsrc[tid], p.step_counter[0] + p.step_offset);
+  __syncthreads();
+  const float hdec = p.hm.decay[0][0], hsrc = p.hm.source[0][0] * (Exact ? 1.0f : inv_res);
+  // Hx (storage (Z, Y, X + 1)): dEz/dy - dEy/dz.
+  for (int q = tid; q < (kColK + 1) * (kColJ + 1); q += kColJ * kColK) {
+    const int a = q / (kColJ + 1), b = q % (kColJ + 1);
+    const int kk = k0 - 1 + a, jj = j0 - 1 + b;
+    float h = 0.0f;
+    if (kk >= 0 && kk < Z && jj >= 0 && jj < Y) {
+      const bool own = a > 0 && b > 0;
+      const int oh = kk * PL + jj * P + X;
+      float qy = 0.f, qz = 0.f;
+      if (Cpml) {
+        qy = col_psi<1>(p.ht[0], kk, jj, X);
+        qz = col_psi<0>(p.ht[1], kk, jj, X);
+      }
+      float d0 = D1(p.ein[2][oh + P] - p.ein[2][oh]);
+      float d1 = D1(p.ein[1][oh + PL] - p.ein[1][oh]);
+      if (Cpml) {
+        d0 = col_cpml<Exact, 1>(p.ht[0], res, inv_res, qy, kk, jj, X, d0, own);
+        d1 = col_cpml<Exact, 0>(p.ht[1], res, inv_res, qz, kk, jj, X, d1, own);
+      }
+      h = h1<Exact>(p.hin[0][oh], hdec, hsrc, d0, d1);
+      if (p.n_hsrc > 0) h = h_sources_at(p, amp, 3, kk, jj, X, h);
+      if (wx1) h = 0.0f;  // PEC: normal H on the x = X wall
+      if (own) p.hout[0][oh] = h;
+    }
+    hx[a][b] = h;
+  }
+  __syncthreads();
+  if (!live) return;
+  const int a = threadIdx.y + 1, b = threadIdx.x + 1;
+  // Hz, Hy at x = X - 1 (only a metallic x = X wall makes the ghost use them),
+  // as the class step computes them: read-only on psi.
+  float hz_w = 0.0f, hy_w = 0.0f;
+  if (wx1) {
+    const int ow = o - 1;
+    if (ey_ok) {  // Hz(k, j, X - 1): dEy/dx - dEx/dy
+      float d0 = D1(p.ein[1][ow + 1] - p.ein[1][ow]), d1 = D1(p.ein[0][ow + P] - p.ein[0][ow]);
+      if (Cpml) {
+        d0 = col_cpml<Exact, 2>(p.ht[4], res, inv_res, col_psi<2>(p.ht[4], k, j, X - 1), k, j, X - 1, d0, false);
+        d1 = col_cpml<Exact, 1>(p.ht[5], res, inv_res, col_psi<1>(p.ht[5], k, j, X - 1), k, j, X - 1, d1, false);
+      }
+      hz_w = h1<Exact>(p.hin[2][ow], p.hm.decay[2][0], p.hm.source[2][0] * (Exact ? 1.0f : inv_res), d0, d1);
+      if (p.n_hsrc > 0) hz_w = h_sources_at(p, amp, 5, k, j, X - 1, hz_w);
+      if ((k == 0 && wz0) || (k == Z && wz1)) hz_w = 0.0f;
+    }
+    if (ez_ok) {  // Hy(k, j, X - 1): dEx/dz - dEz/dx
+      float d0 = D1(p.ein[0][ow + PL] - p.ein[0][ow]), d1 = D1(p.ein[2][ow + 1] - p.ein[2][ow]);
+      if (Cpml) {
+        d0 = col_cpml<Exact, 0>(p.ht[2], res, inv_res, col_psi<0>(p.ht[2], k, j, X - 1), k, j, X - 1, d0, false);
+        d1 = col_cpml<Exact, 2>(p.ht[3], res, inv_res, col_psi<2>(p.ht[3], k, j, X - 1), k, j, X - 1, d1, false);
+      }
+      hy_w = h1<Exact>(p.hin[1][ow], p.hm.decay[1][0], p.hm.source[1][0] * (Exact ? 1.0f : inv_res), d0, d1);
+      if (p.n_hsrc > 0) hy_w = h_sources_at(p, amp, 4, k, j, X - 1, hy_w);
+      if ((j == 0 && wy0) || (j == Y && wy1)) hy_w = 0.0f;
+    }
+  }
+  if (ey_ok) {  // Ey: dHx/dz - dHz/dx, the Hz ghost beyond x = X
+    float d0 = D1(ghost_diff(hx[a][b], hx[a - 1][b], k, Z, wz0, wz1));
+    float d1 = D1(ghost_diff(0.0f, hz_w, X, X, wx0, wx1));
+    if (Cpml) {
+      d0 = col_cpml<Exact, 0>(p.et[2], res, inv_res, q_eyz, k, j, X, d0, true);
+      d1 = col_cpml<Exact, 2>(p.et[3], res, inv_res, q_eyx, k, j, X, d1, true);
+    }
+    float e = e_upd<Exact>(ey0, t.y, d0, d1);
+    if ((k == 0 && wz0) || (k == Z && wz1) || wx1) e = 0.0f;
+    p.eout[1][o] = e;
+  }
+  if (ez_ok) {  // Ez: dHy/dx - dHx/dy, the Hy ghost beyond x = X
+    float d0 = D1(ghost_diff(0.0f, hy_w, X, X, wx0, wx1));
+    float d1 = D1(ghost_diff(hx[a][b], hx[a][b - 1], j, Y, wy0, wy1));
+    if (Cpml) {
+      d0 = col_cpml<Exact, 2>(p.et[4], res, inv_res, q_ezx, k, j, X, d0, true);
+      d1 = col_cpml<Exact, 1>(p.et[5], res, inv_res, q_ezy, k, j, X, d1, true);
+    }
+    float e = e_upd<Exact>(ez0, t.z, d0, d1);
+    if ((j == 0 && wy0) || (j == Y && wy1) || wx1) e = 0.0f;
+    p.eout[2][o] = e;
   }
 }
 
@@ -1064,7 +1145,7 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   if (err != cudaSuccess) return err;
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
-  const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;  // a multiple of 128 leaves column X to lane 31
+  const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;  // a multiple of 128 leaves column X to the column kernel
   const int gy = (p.Y + 1 + T::TY - 1) / T::TY, gz = (kmax + zc - 1) / zc;
   Step3D q = p;
   q.z_chunk = zc;
@@ -1089,6 +1170,12 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   q.order[3] = zhi;
   const long long ctas = static_cast<long long>(gx) * gy * gz;
   if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  if (p.X % T::TX == 0) {  // column X first: it reads only the step's inputs
+    const dim3 cgrid((p.Y + 1 + kColJ - 1) / kColJ, (p.Z + 1 + kColK - 1) / kColK, 1);
+    class_column_kernel<Cpml, Exact><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
+    err = cudaPeekAtLastError();
+    if (err != cudaSuccess) return err;
+  }
   kern<<<dim3(static_cast<unsigned>(ctas), 1, 1), dim3(32, NW, 1), smem, s>>>(maps, q);
   return cudaPeekAtLastError();
 }

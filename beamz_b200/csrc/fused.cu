@@ -384,12 +384,10 @@ cudaError_t launch_fused_t(cudaStream_t s, const Step3D& p) {
   using S = FusedSmem<TX, TY>;
   const size_t smem = sizeof(S);
   auto kern = fused_step_kernel<TX, TY, Active, Cpml, Mat, Metric>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (err != cudaSuccess) return err;
-    configured = true;
-  }
+  // The dynamic shared-memory limit is a per-device function attribute: set it
+  // on every launch (cheap) rather than once per process.
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
   const dim3 grid((p.X + 1 + TX - 1) / TX, (p.Y + 1 + TY - 1) / TY, (kmax + zc - 1) / zc);

@@ -421,12 +421,10 @@ cudaError_t launch_lean_t(cudaStream_t s, const Step3D& p) {
   using L = Lean<NW, R, D>;
   const size_t smem = sizeof(typename L::Smem);
   auto kern = lean_step_kernel<NW, R, D, Cpml, Mat, Metric>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (err != cudaSuccess) return err;
-    configured = true;
-  }
+  // The dynamic shared-memory limit is a per-device function attribute: set it
+  // on every launch (cheap) rather than once per process.
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
   const dim3 grid((p.X + 1 + L::TX - 1) / L::TX, (p.Y + 1 + L::TY - 1) / L::TY, (kmax + zc - 1) / zc);

@@ -721,12 +721,10 @@ cudaError_t launch_tma_t(cudaStream_t s, const TmaMaps& maps, const Step3D& p) {
   using T = TmaTile<NW, R>;
   const size_t smem = sizeof(typename T::Smem);
   auto kern = tma_step_kernel<NW, R, Cpml>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (err != cudaSuccess) return err;
-    configured = true;
-  }
+  // The dynamic shared-memory limit is a per-device function attribute: set it
+  // on every launch (cheap) rather than once per process.
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
   // A multiple-of-32 X leaves column X to the last full tile (xcol).

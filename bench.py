@@ -495,8 +495,10 @@ def main():
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"tma_step_{args.scene}.json")
-    if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16:
+    # The ncu capture of the dominant kernel on this workload, when one is committed.
+    kname = {"classes": "class_step", "codebook": "tma_step"}.get(prog.step_kernel, "fused_step")
+    prof = os.path.join(ROOT, "profiles", f"{kname}_{args.scene}.json")
+    if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16 and args.cpml_faces == "all":
         with open(prof) as fh:
             traffic = json.load(fh).get("dram_bytes_per_launch")
 

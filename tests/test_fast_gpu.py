@@ -4,8 +4,8 @@ accuracy target (relative L2 <= 1e-5 for fields and CPML memories, <= 1e-4
 for the DFT arena) with the opt-in tolerance arithmetic (FDTD_FLAG_FAST_MATH:
 1/dx folded into the coefficients, fused multiply-adds) over short runs.
 Grids are wide enough in x (>= 128 lattice points) that the straight tile
-bodies run, with column X owned by the last tile (X a multiple of 128) and
-with a partial last tile (X not a multiple)."""
+bodies run, with column X updated by the column kernel after the tiles (X a
+multiple of 128) and with a partial last tile (X not a multiple)."""
 
 from __future__ import annotations
 
@@ -26,7 +26,7 @@ FIELD_TOL = 1e-5
 DFT_TOL = 1e-4
 
 CASES = [
-    dict(grid=(10, 20, 256), pml_cells=6),                                         # column X owned by lane 31
+    dict(grid=(10, 20, 256), pml_cells=6),                                         # column X: the column kernel
     dict(grid=(9, 17, 300), pml_cells=5, metallic=("front", "left", "top")),       # partial last tile, PEC
     dict(grid=(12, 24, 130), pml_cells=4, metallic=("right", "bottom", "back")),
     dict(grid=(11, 16, 256), cpml_edges=(), metallic=("front", "back", "bottom", "top", "left", "right")),
@@ -97,6 +97,26 @@ def test_class_step_from_zero_fields_with_sources(case):
     out = R.run_steps(R.initial_state(prog), prog, nsteps).numpy()
     oprog = to_oracle(spec)
     st = O.run(oracle_state(oprog), oprog, nsteps)
+    _bitwise(out, st)
+    _compare(out, st)
+
+
+@pytest.mark.parametrize("metallic", [(), ("right", "front", "top")])
+def test_column_x_with_an_h_source_on_it(metallic):
+    """The column kernel (x = X when X is a multiple of 128) applies H-timing
+    sources on Hx there, the x = X wall and the CPML terms of the column, bit
+    for bit, over chunks of several planes and rows."""
+    nsteps = 10
+    spec = scenario_3d(grid=(19, 41, 128), seed=11, pml_cells=4, nsteps=nsteps, metallic=metallic)
+    rng = np.random.default_rng(5)
+    nz, ny, nx = spec.grid_shape
+    spec.sources.append(P.SourcePlan("Hx", "h", (3, 5, nx - 1), rng.standard_normal((9, 33, 2)).astype(np.float32),
+                                     (rng.standard_normal(nsteps) * 1e-3).astype(np.float32)))
+    fields = random_initial_fields(spec, seed=6)
+    prog = R.compile_program(spec, step_kernel="classes")
+    out = R.run_steps(R.initial_state(prog, fields=fields), prog, nsteps).numpy()
+    oprog = to_oracle(spec)
+    st = O.run(oracle_state(oprog, fields), oprog, nsteps)
     _bitwise(out, st)
     _compare(out, st)
 
