@@ -16,7 +16,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 11
+FDTD_ABI_VERSION = 12
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
@@ -125,6 +125,7 @@ class FdtdDft(ctypes.Structure):
         ("im", FdtdBuffer),
         ("weight_sum", FdtdBuffer),
         ("samples", FdtdBuffer),
+        ("affine", FdtdBuffer),
     ]
 
 

@@ -157,13 +157,54 @@ constexpr int kDftMaxBatch = 16;
 // step CTAs, so sampling on a side stream overlaps the next step.
 constexpr int kDftSampleThreads = 128;
 
+// A (monitor, component) whose plan has the affine form (FdtdDft::affine) is
+// sampled without reading the plan: the block's 128 threads take tiles of
+// 32 points along b by 4 along a, so the rows that neighbouring points share
+// (the other slot of a two-plane interpolation) are read once through L1.
 __global__ void __launch_bounds__(kDftSampleThreads, 16) dft_sample_kernel(DftDev d, float* samples, int slot) {
   const int mc = blockIdx.y;
   const int m = mc / 6, c = mc % 6;
   const int np = min(max(d.counts[5 * m + 1], 0), d.max_points);
+  if (d.masks[m * 6 + c] == 0.0f) return;
+  float* out = samples + ((static_cast<int64_t>(slot) * d.monitor_count + m) * 6 + c) * d.max_points;
+  const int* af = d.affine != nullptr ? d.affine + mc * 24 : nullptr;
+  if (af != nullptr && af[0] == 1) {
+    const int na = af[1], nb = af[2], base = af[3], sa = af[4], sb = af[5], k = min(af[6], kGatherSlots);
+    if (static_cast<int64_t>(na) * nb > np) return;  // not this plan's form: nothing is sampled
+    int delta[kGatherSlots];
+    float w[kGatherSlots];
+#pragma unroll
+    for (int s = 0; s < kGatherSlots; ++s) {
+      delta[s] = af[8 + s];
+      w[s] = __int_as_float(af[16 + s]);
+    }
+    const float* field = d.fields[c];
+    const int64_t len = d.field_len[c];
+    const int tb = (nb + 31) / 32, tiles = tb * ((na + 3) / 4);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+      const int a = (t / tb) * 4 + ty, b = (t % tb) * 32 + tx;
+      if (a >= na || b >= nb) continue;
+      const int64_t i0 = base + static_cast<int64_t>(a) * sa + static_cast<int64_t>(b) * sb;
+      float f[kGatherSlots];
+#pragma unroll
+      for (int s = 0; s < kGatherSlots; ++s) {
+        const int64_t i = i0 + delta[s];
+        f[s] = (s < k && i >= 0 && i < len) ? field[i] : 0.0f;
+      }
+      float v = 0.0f;
+#pragma unroll
+      for (int s = 0; s < kGatherSlots; ++s) {
+        const int64_t i = i0 + delta[s];
+        if (s < k && i >= 0 && i < len) v = v + f[s] * w[s];
+      }
+      out[static_cast<int64_t>(a) * nb + b] = v;
+    }
+    return;
+  }
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np || d.masks[m * 6 + c] == 0.0f) return;
-  samples[((static_cast<int64_t>(slot) * d.monitor_count + m) * 6 + c) * d.max_points + p] = dft_gather(d, m, c, p);
+  if (p >= np) return;
+  out[p] = dft_gather(d, m, c, p);
 }
 
 __global__ void __launch_bounds__(kDftThreads) dft_flush_kernel(DftDev d, const float* samples, const int* counter,

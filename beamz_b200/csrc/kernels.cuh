@@ -184,6 +184,7 @@ struct DftDev {
   const float* step_time;
   int step_time_len;
   float dt;
+  const int* affine;  // [M, 6, 24] affine plans (FdtdDft::affine), or null
 };
 
 // Monitor-plane reduction (analysis.cu); see FdtdMonitorReduce.

@@ -242,6 +242,8 @@ int validate(const FdtdProgram& p) {
                                 &d.im, &d.weight_sum})
       if (b->data == nullptr && elements(*b) > 0) return kInvalid;
     if (d.batch < 0 || d.batch > 16) return kInvalid;
+    if (d.affine.data != nullptr && (d.affine.element_type != FDTD_S32 || elements(d.affine) != 24 * 6 * M))
+      return kInvalid;
     if (d.samples.data != nullptr &&
         (!is_f32(d.samples) || elements(d.samples) != static_cast<int64_t>(d.batch) * M * 6 * d.indices.dims[3]))
       return kInvalid;
@@ -490,6 +492,7 @@ DftDev make_dft(const FdtdProgram& p, const FdtdBuffer* bank_fields) {
   d.step_time = static_cast<const float*>(p.step_time.data);
   d.step_time_len = static_cast<int>(elements(p.step_time));
   d.dt = p.dt;
+  d.affine = static_cast<const int*>(m.affine.data);
   return d;
 }
 

@@ -204,6 +204,7 @@ class DftArena:
     value_count: int
     weight_count: int
     layout: list  # per monitor: (value_offset, freq_count, point_count, weight_offset)
+    affine: object = None  # [M, 6, 24] int32: affine forms of the plans (FdtdDft.affine)
 
 
 def voxel_histogram(ids, device):
@@ -289,9 +290,59 @@ def pack_dft_monitors(monitors, device, shapes, strides) -> DftArena | None:
         voff += 6 * nf * p
         woff += nf
     t = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
-    arena = DftArena(indices, weights, t(freqs), t(masks), t(counts), t(codes), t(windows), voff, woff, layout)
+    affine = np.zeros((M, 6, 24), np.int32)
+    for m, mon in enumerate(monitors):
+        for c in range(6):
+            if mon.component_mask[c] != 0 and mon.points > 0:
+                words = _affine_plan(indices[m, c, :, : mon.points], weights[m, c, :, : mon.points])
+                if words is not None:
+                    affine[m, c] = words
+    arena = DftArena(indices, weights, t(freqs), t(masks), t(counts), t(codes), t(windows), voff, woff, layout,
+                     t(affine))
     cur.synchronize()  # the plan is complete before any stream of the program reads it
     return arena
+
+
+def _affine_plan(idx, w):
+    """The 24-word affine form (FdtdDft.affine) of one packed [K, n] gather
+    plan on the device, or None when the plan does not have it exactly: the
+    nonzero-weight slots (at most 4, first) carry the same weight and the same
+    offset from slot 0 at every point, and slot 0's index is
+    base + (p // nb) * sa + (p % nb) * sb.  Plane monitors on uniform
+    coordinates have this form; sampling them then reads no plan."""
+    torch = _torch()
+    K, n = idx.shape
+    nonzero = (w != 0).sum(dim=1)
+    full, empty = nonzero == n, nonzero == 0
+    if not bool((full | empty).all()):
+        return None
+    k = int(full.sum())
+    if not 1 <= k <= 4 or not bool(full[:k].all()):
+        return None
+    wk, ik = w[:k], idx[:k].long()
+    if not bool((wk == wk[:, :1]).all()):
+        return None
+    delta = ik - ik[:1]
+    if not bool((delta == delta[:, :1]).all()):
+        return None
+    b0 = ik[0]
+    na, nb, sa, sb = 1, n, 0, 0
+    if n > 1:
+        sb = int(b0[1] - b0[0])
+        breaks = ((b0[1:] - b0[:-1]) != sb).nonzero()
+        nb = int(breaks[0, 0]) + 1 if breaks.numel() else n
+        if n % nb:
+            return None
+        na = n // nb
+        sa = int(b0[nb] - b0[0]) if na > 1 else 0
+        p = torch.arange(n, device=idx.device)
+        if not bool((b0 == b0[0] + (p // nb) * sa + (p % nb) * sb).all()):
+            return None
+    if max(abs(sa), abs(sb), abs(int(b0[0]))) >= 2**31:
+        return None
+    bits = wk[:, 0].contiguous().view(torch.int32).tolist()
+    return ([1, na, nb, int(b0[0]), sa, sb, k, 0] + [int(v) for v in delta[:, 0].tolist()] + [0] * (8 - k)
+            + [int(v) for v in bits] + [0] * (8 - k))
 
 
 def _pack_plan(lib, stream, indices, weights, dims, strides, device):
@@ -503,7 +554,7 @@ class DeviceProgram:
         if self.arena is not None:
             a = self.arena
             s.dft.monitor_count = len(spec.monitors)
-            for name in ("indices", "weights", "freqs", "masks", "counts", "codes", "windows"):
+            for name in ("indices", "weights", "freqs", "masks", "counts", "codes", "windows", "affine"):
                 setattr(s.dft, name, buf(getattr(a, name)))
         # Time-domain field recorders.
         if len(spec.recorders) > abi.FDTD_MAX_RECORDERS:

@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 11
+#define FDTD_ABI_VERSION 12
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -177,6 +177,16 @@ typedef struct FdtdDft {
    * so the arena is bit-identical to per-step accumulation, with the arena
    * read and written once per batch instead of once per step. */
   FdtdBuffer samples;
+  /* S32 [M, 6, 24], optional: per (monitor, component) the affine form of its
+   * gather plan, which the batched sampling then uses instead of indices /
+   * weights (no plan read per point).  Word 0 = 1 marks it: every point
+   * p = a * nb + b (a < na, b < nb) sums slot s < k at index
+   * base + a * sa + b * sb + delta[s] with weight w[s], in slot order, as the
+   * packed plan does (k <= 4).  Words: 0 flag, 1 na, 2 nb, 3 base, 4 sa, 5 sb, 6 k,
+   * 8..15 delta[8], 16..23 w[8] (float bits).  The runtime derives it from the
+   * packed plan only where the plan has exactly that form (plane monitors on
+   * uniform coordinates do). */
+  FdtdBuffer affine;
 } FdtdDft;
 
 /* A time-domain field recorder (beamz: FieldRecorder, compiled by

@@ -382,6 +382,32 @@ def test_dft_step_batching_is_bit_identical(dims):
             np.testing.assert_array_equal(out[key], outs[0][key], err_msg=key)
 
 
+@pytest.mark.parametrize("layout", ["pitched", "dense"])
+def test_affine_dft_sampling_equals_the_gather_plan(layout):
+    """Plane monitors on uniform coordinates get the affine form of their
+    plans, and sampling through it (no plan read per point) gives the arena of
+    the packed gather plan bit for bit."""
+    from beamz_b200 import workloads as W
+
+    spec = W.scene_3d_512(total_steps=40, shape=(28, 40, 128), pml_cells=4)
+    outs = []
+    for affine in (True, False):
+        prog = R.compile_program(spec, schedule="fused" if layout == "pitched" else "phases")
+        assert prog.dft_batch > 1
+        flags = prog.arena.affine[..., 0].cpu().numpy()
+        masks = prog.arena.masks.cpu().numpy()
+        np.testing.assert_array_equal(flags, (masks != 0).astype(np.int32))  # every sampled plan
+        if not affine:
+            prog.arena.affine.zero_()  # the gather plans instead
+        st = R.initial_state(prog)
+        R.run_steps(st, prog, 21)
+        R.run_steps(st, prog, 19)
+        outs.append(st.numpy())
+    for key in ("dft_re", "dft_im", "dft_w"):
+        np.testing.assert_array_equal(outs[0][key], outs[1][key], err_msg=key)
+    assert np.abs(outs[0]["dft_re"]).max() > 0
+
+
 @pytest.mark.parametrize("pol", ["tm", "te"])
 def test_2d_pre_e_sources_inside_the_fused_step(pol):
     """2D fused programs add pre-E sources to the staged E planes instead of

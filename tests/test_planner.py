@@ -177,3 +177,38 @@ def test_sources_clear_of_monitors():
         src = P.SourcePlan("Ey", "pre_e", start, np.ones(ext, np.float32), np.zeros(4, np.float32))
         got = P.sources_clear_of_monitors(dataclasses.replace(spec, sources=[src]))
         assert got == (not (cells & gathered)), (start, ext)
+
+
+def test_affine_form_of_plane_plans():
+    """The affine form (FdtdDft.affine) reproduces a plane monitor's gather
+    plan exactly -- every index and weight -- and is refused when the weights
+    vary from point to point."""
+    torch = pytest.importorskip("torch")
+    from beamz_b200 import runtime as R
+    from beamz_b200 import workloads as W
+
+    spec = W.scene_3d_512(total_steps=4, shape=(20, 36, 44), pml_cells=4)
+    seen = 0
+    for mon in spec.monitors:
+        for c in range(6):
+            if mon.component_mask[c] == 0:
+                continue
+            idx = np.asarray(mon.indices[c]).reshape(mon.points, -1)
+            w = np.asarray(mon.weights[c]).reshape(mon.points, -1)
+            words = R._affine_plan(torch.as_tensor(idx.T.copy()), torch.as_tensor(w.T.copy()))
+            assert words is not None
+            flag, na, nb, base, sa, sb, k = words[:7]
+            assert flag == 1 and na * nb == mon.points and 1 <= k <= 4
+            p = np.arange(mon.points)
+            b0 = base + (p // nb) * sa + (p % nb) * sb
+            for s in range(k):
+                np.testing.assert_array_equal(idx[:, s], b0 + words[8 + s])
+                wk = np.array([words[16 + s]], np.int32).view(np.float32)[0]
+                np.testing.assert_array_equal(w[:, s], np.full(mon.points, wk, np.float32))
+            assert not np.any(w[:, k:])
+            seen += 1
+            w2 = w.copy()
+            w2[5, 0] *= 2.0
+            assert R._affine_plan(torch.as_tensor(idx.T.copy()), torch.as_tensor(w2.T.copy())) is None
+    assert seen == 16  # four planes, four sampled components each
+
