@@ -567,7 +567,8 @@ def main():
                        "tile": list(tile), "z_chunk": args.z_chunk},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": {"classes": "class_step_kernel", "codebook": "tma_step_kernel"}.get(
+                         "kernel": {"classes": "class_step_kernel + class_column_kernel (one step)",
+                                    "codebook": "tma_step_kernel"}.get(
                              prog.step_kernel, "fused step"), "kernel_ms": round(kernel_ms, 4),
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": f"{peak_kind} hbm_gbs"},
             "peak_hbm_gb": round(peak_hbm / 1e9, 2),
