@@ -32,8 +32,10 @@
 // coefficients (dt/(mu0 dx) for H, dt/(eps0 eps dx) per class for E, a/dx for
 // the CPML) and explicit fused multiply-adds.
 //
-// Tile-planes that touch a z face, an H source or a partial x tile run a
-// general per-cell path with every validity, ghost and PEC rule; the rest run
+// The tiles end at x = X - 1 (a partial last tile masks its stores past X)
+// and the lattice column x = X is a small column kernel's, run before the
+// step.  Tile-planes that touch a z face or an H source run a general
+// per-cell path with every validity, ghost and PEC rule; the rest run
 // a straight body compiled for their case: the interior, the x = 0 / y = 0
 // faces, the x-slab tiles (about half of them on a 512-wide grid), the other
 // absorber tiles (axes as plane-uniform run-time flags), and the last tile
@@ -134,6 +136,16 @@ __device__ __forceinline__ TileIdx tile_of(int L, int gx, int gy, int gz, const 
 // ---- float4 helpers ----------------------------------------------------------
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+// The first `nv` of four cells (all four: one 16-byte store).
+__device__ __forceinline__ void st4m(float* p, float4 v, int nv) {
+  if (nv >= 4) {
+    st4(p, v);
+    return;
+  }
+  if (nv > 0) p[0] = v.x;
+  if (nv > 1) p[1] = v.y;
+  if (nv > 2) p[2] = v.z;
+}
 __device__ __forceinline__ float4 sub4(float4 a, float4 b) {
   return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
 }
@@ -214,16 +226,19 @@ __device__ __forceinline__ int psi_off(const CpmlTermDev& t, int slot, int k, in
 // A term whose slot is uniform over a lane's four cells (y terms on a row, z
 // terms on a plane): psi of the four cells is fetched ahead of its use (the
 // offset is recomputed when applying, to keep registers free).
+// `nv`: how many of the lane's four cells lie before x = X (a partial last
+// tile stores nothing, and loads no psi, past it).
 template <int Axis>
-__device__ __forceinline__ float4 psi4_fetch(const CpmlTermDev& t, int slot, int k, int j, int i) {
+__device__ __forceinline__ float4 psi4_fetch(const CpmlTermDev& t, int slot, int k, int j, int i, int nv) {
   if (slot < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
   const float* s = t.psi_in + psi_off<Axis>(t, slot, k, j, i);
-  return make_float4(s[0], s[1], s[2], s[3]);
+  if (nv >= 4) return make_float4(s[0], s[1], s[2], s[3]);
+  return make_float4(nv > 0 ? s[0] : 0.f, nv > 1 ? s[1] : 0.f, nv > 2 ? s[2] : 0.f, 0.f);
 }
 
 template <bool Exact, int Axis>
 __device__ __forceinline__ float4 psi4_apply(const CpmlTermDev& t, const float4* cc, int slot, float4 v, int k, int j,
-                                             int i, float res, float4 d, bool write) {
+                                             int i, float res, float4 d, bool write, int nv) {
   if (slot < 0) return d;
   const float4 c = cc[slot];
   float4 n;
@@ -234,10 +249,10 @@ __device__ __forceinline__ float4 psi4_apply(const CpmlTermDev& t, const float4*
   r.w = cpml_d<Exact>(c, res, v.w, d.w, &n.w);
   if (write) {
     float* o = t.psi_out + psi_off<Axis>(t, slot, k, j, i);
-    o[0] = n.x;
-    o[1] = n.y;
-    o[2] = n.z;
-    o[3] = n.w;
+    if (nv > 0) o[0] = n.x;
+    if (nv > 1) o[1] = n.y;
+    if (nv > 2) o[2] = n.z;
+    if (nv > 3) o[3] = n.w;
   }
   return r;
 }
@@ -418,7 +433,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int lane = threadIdx.x, warp = threadIdx.y;
   const int tid = warp * 32 + lane;
   const int Z = p.Z, Y = p.Y, X = p.X;
-  const int gx = X % TX == 0 ? X / TX : X / TX + 1, gy = (Y + TY) / TY, gz = (Z + p.z_chunk) / p.z_chunk;
+  const int gx = (X + TX - 1) / TX, gy = (Y + TY) / TY, gz = (Z + p.z_chunk) / p.z_chunk;
   const TileIdx tile = tile_of(blockIdx.x, gx, gy, gz, p.order);
   // The last tile row, when it would hold rows past Y, is shifted down to
   // end at row Y (j0 = Y + 1 - TY) so that it runs a straight body; its rows
@@ -433,9 +448,11 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const float res = p.res, inv_res = p.inv_res;
   const unsigned long long wait_ns = p.wait_ns;
 
-  // When X is a multiple of 128 the tiles end at x = X - 1 and column X (Hx,
-  // Ey, Ez there) is the column kernel's, launched before this one.
-  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i0 + TX <= p.cpml_inner[2][1]);
+  // The tiles end at x = X - 1 -- the last one partial when X is not a
+  // multiple of 128, its lanes past X storing nothing (nv below) -- and column
+  // X (Hx, Ey, Ez there) is the column kernel's, launched before this one.
+  const int i1 = min(i0 + TX, X);  // the tile's columns end here (a partial last tile before i0 + 128)
+  const bool ax = Cpml && !(i0 - 1 >= p.cpml_inner[2][0] && i1 <= p.cpml_inner[2][1]);
   // Compact x work: in a tile that touches an x slab, the recurrences of a
   // row's x-slab cells are shared by the row's warp -- each lane takes items
   // lane and lane + 32 of the row's (term, slot) list, the first x term's
@@ -453,7 +470,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   if (xstage) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      const XItems a = x_items(t < 2 ? p.ht[3 + t] : p.et[1 + t], i0, i0 + TX);
+      const XItems a = x_items(t < 2 ? p.ht[3 + t] : p.et[1 + t], i0, i1);
       if (a.lo_n + a.hi_n == 0) continue;
       const int first = a.lo_n > 0 ? a.lo_s : a.hi_s;
       const int last = a.hi_n > 0 ? a.hi_s + a.hi_n - 1 : a.lo_s + a.lo_n - 1;
@@ -528,7 +545,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const int c0 = 4 + 4 * lane;         // own first column in the boxes and hn
   const int i = i0 + 4 * lane;         // its lattice x
   const int rc = r * BX + c0;
-  const bool fast_ok0 = (j0 + TY <= Y || ylast) && i0 + TX <= X && cc_smem;
+  const bool fast_ok0 = (j0 + TY <= Y || ylast) && cc_smem;
+  const int nv = min(max(X - i, 0), 4);  // own cells before x = X (a partial last tile)
   const bool own = j >= jown;  // this warp's row is the tile's to store
   const bool xface = i0 == 0, yface = j0 == 0;
   const bool ay = Cpml && !(j0 - 1 >= p.cpml_inner[1][0] && j0 + TY <= p.cpml_inner[1][1]);
@@ -543,7 +561,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   // last column (column X is the column kernel's).
   if (xcompact && warp == 0) {
     auto pack = [&](const CpmlTermDev& t3, const CpmlTermDev& t4, int q) {
-      const XItems a3 = x_items(t3, i0, i0 + TX), a4 = x_items(t4, i0, i0 + TX);
+      const XItems a3 = x_items(t3, i0, i1), a4 = x_items(t4, i0, i1);
       const int n3 = a3.lo_n + a3.hi_n;
       const bool second = q >= n3;
       int slot = 0, x = 0;
@@ -607,6 +625,10 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         // jown, row Y in warp TY-1 (Hx, Hz and Ey do not exist there and the
         // y = Y ghost applies).
         constexpr bool LY = M & 32;
+        // The run-time and last-row bodies also take the partial last tile:
+        // stores and psi accesses stop at x = X (nv); the others handle all
+        // four cells of every lane with no test.
+        const int nvv = (RT || LY) ? nv : 4;
         const bool lyr = LY || (RT && ylast);
         const bool st = !lyr || own;       // this row is stored
         const bool rowY = lyr && j == Y;   // row Y: Hx, Hz, Ey absent
@@ -619,26 +641,26 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const bool halo_col = emit && warp == 2 && lane < TY && !at_x0;   // Hy, Hz on column i0-1
         const int jc = j0 + lane;                                         // halo_col's row
         // ---- every global load of the plane goes out first ----
-        // psi of the H terms: own cells, halos, column X.
+        // psi of the H terms: own cells and halos.
         float4 qh0, qh1, qh2, qh5;
         if (AY && !rowY) {
-          qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i);
-          qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i);
+          qh0 = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], j), k, j, i, nvv);
+          qh5 = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], j), k, j, i, nvv);
         }
         if (AZ) {
-          if (!rowY) qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i);
-          qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i);
+          if (!rowY) qh1 = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, j, i, nvv);
+          qh2 = psi4_fetch<0>(p.ht[2], slot_of(p.ht[2], k), k, j, i, nvv);
         }
         // psi of the E terms too: in flight through the whole H phase.
         float4 qe0, qe1, qe2, qe5;
         if (emit) {
           if (AY) {
-            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i);
-            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i);
+            qe0 = psi4_fetch<1>(p.et[0], slot_of(p.et[0], j), k, j, i, nvv);
+            qe5 = psi4_fetch<1>(p.et[5], slot_of(p.et[5], j), k, j, i, nvv);
           }
           if (AZ) {
-            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i);
-            if (!rowY) qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i);
+            qe1 = psi4_fetch<0>(p.et[1], slot_of(p.et[1], k), k, j, i, nvv);
+            if (!rowY) qe2 = psi4_fetch<0>(p.et[2], slot_of(p.et[2], k), k, j, i, nvv);
           }
         }
         // ---- compact x work of the H terms (Hyx, Hzx) on this warp's row ----
@@ -677,13 +699,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(ld4(E0x + rc + BX), ex));  // Hz: dEy/dx, dEx/dy
         }
         if (AY && !rowY) {
-          dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit && st);
-          dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit && st);
+          dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit && st, nvv);
+          dz1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], j), qh5, k, j, i, res, dz1, emit && st, nvv);
         }
         if (AZ) {
           if (!rowY)
-            dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit && st);
-          dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit && st);
+            dx1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qh1, k, j, i, res, dx1, emit && st, nvv);
+          dy0 = psi4_apply<Exact, 0>(p.ht[2], sm.cc[2], slot_of(p.ht[2], k), qh2, k, j, i, res, dy0, emit && st, nvv);
         }
         if (AX) {
           dy1 = xtake(dy1, sm.xst[0][lane], sm.xd[0][warp]);
@@ -700,20 +722,20 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         st4(&sm.hn[2][r][c0], hz);
         const int o = k * PL + j * P + i;
         if (emit && st) {
-          if (!rowY) st4(p.hout[0] + o, hx);
-          st4(p.hout[1] + o, hy);
-          if (!rowY) st4(p.hout[2] + o, hz);
+          if (!rowY) st4m(p.hout[0] + o, hx, nvv);
+          st4m(p.hout[1] + o, hy, nvv);
+          if (!rowY) st4m(p.hout[2] + o, hz, nvv);
         }
         // ---- recomputed halo: row j0-1 (Hx by warp 0, Hz by warp 1) and
         //      column i0-1 (Hy, Hz by warp 2), read-only on psi ----
         if (halo_row_x) {
           const int b = c0;
           float4 qa, qb;
-          if (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i);
-          if (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i);
+          if (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i, nvv);
+          if (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i, nvv);
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
-          if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false);
-          if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false);
+          if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false, nvv);
+          if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false, nvv);
           float4 h = h4<Exact>(ld4(HOx + b), sm.hcoef[0], sm.hcoef[3], d0, d1);
           if (at_x0 && lane == 0 && wx0) h.x = 0.0f;
           st4(&sm.hn[0][0][b], h);
@@ -729,13 +751,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               qa = psix_fetch(p.ht[4], xs4, k, jh);
             }
           }
-          if (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i);
+          if (AY) qb = psi4_fetch<1>(p.ht[5], slot_of(p.ht[5], jh), k, jh, i, nvv);
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
           if (lane == 31) e4 = E0y[b + 4];
           float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
           if (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
-          if (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false);
+          if (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false, nvv);
           st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), sm.hcoef[2], sm.hcoef[5], d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
@@ -810,13 +832,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           fz1 = D4(wy1 ? sub4(z4, hxy) : z4);
         }
         if (AY) {
-          fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, st);
-          fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, st);
+          fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, st, nvv);
+          fz1 = psi4_apply<Exact, 1>(p.et[5], sm.cc[11], slot_of(p.et[5], j), qe5, k, j, i, res, fz1, st, nvv);
         }
         if (AZ) {
-          fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, st);
+          fx1 = psi4_apply<Exact, 0>(p.et[1], sm.cc[7], slot_of(p.et[1], k), qe1, k, j, i, res, fx1, st, nvv);
           if (!rowY)
-            fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, st);
+            fy0 = psi4_apply<Exact, 0>(p.et[2], sm.cc[8], slot_of(p.et[2], k), qe2, k, j, i, res, fy0, st, nvv);
         }
         if (AX) {
           fy1 = xtake(fy1, sm.xst[2][lane], sm.xd[0][warp]);
@@ -845,21 +867,22 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           nz = nx;
         }
         if (st) {
-          st4(p.eout[0] + o, nx);
-          if (!rowY) st4(p.eout[1] + o, ny);
-          st4(p.eout[2] + o, nz);
+          st4m(p.eout[0] + o, nx, nvv);
+          if (!rowY) st4m(p.eout[1] + o, ny, nvv);
+          st4m(p.eout[2] + o, nz, nvv);
         }
         hxp = hx;
         hyp = hy;
       };
       using std::integral_constant;
       if constexpr (!Cpml) {
-        if (ylast) body(integral_constant<int, 32 | 8>{});
+        if (ylast || i0 + TX > X) body(integral_constant<int, 32 | 8>{});  // last row, partial last tile
         else if (xface || yface) body(integral_constant<int, 8>{});
         else body(integral_constant<int, 0>{});
       } else {
         shell_z = !(k >= p.cpml_inner[0][0] && k < p.cpml_inner[0][1]);
-        if (ylast || shell_y || shell_z) body(integral_constant<int, 16 | 8 | 7>{});  // last row, y / z slabs
+        if (ylast || shell_y || shell_z || i0 + TX > X)
+          body(integral_constant<int, 16 | 8 | 7>{});  // last row, y / z slabs, partial last tile
         else if (shell_x) body(integral_constant<int, 8 | 1>{});           // x slab tiles (about half)
         else if (xface || yface) body(integral_constant<int, 8>{});
         else body(integral_constant<int, 0>{});
@@ -871,6 +894,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       // bit 0 Hx, 1 Hy, 2 Hz; `own` stores it (and its psi).
       auto h_cell = [&](int rr, int cc, int which, bool own) {
         const int jj = j0 - 1 + rr, ii = i0 - 4 + cc, b = rr * BX + cc;
+        own = own && ii < X;  // column X: the column kernel
         const int o = k * PL + jj * P + ii;
         const bool zZ = k < Z, yY = jj >= 0 && jj < Y, yY1 = jj >= 0 && jj <= Y;
         const bool iX = ii >= 0 && ii < X, iX1 = ii >= 0 && ii <= X;
@@ -915,7 +939,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       // plane there (hxz, hyz).
       auto e_cell = [&](int rr, int cc, float hxz, float hyz) {
         const int jj = j0 - 1 + rr, ii = i0 - 4 + cc, b = rr * BX + cc;
-        if (jj > Y || ii > X) return;
+        if (jj > Y || ii >= X) return;  // column X: the column kernel
         const int o = k * PL + jj * P + ii;
         const float hx = sm.hn[0][rr][cc], hy = sm.hn[1][rr][cc], hz = sm.hn[2][rr][cc];
         const float hz_y = sm.hn[2][rr - 1][cc], hx_y = sm.hn[0][rr - 1][cc];
@@ -980,8 +1004,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
 
 
 // ---- column x = X ------------------------------------------------------------
-// When X is a multiple of 128 the tiles end at x = X - 1 and this kernel, run
-// before the class step on the same stream, updates the lattice column x = X:
+// The class step's tiles end at x = X - 1 and this kernel, run before it on
+// the same stream, updates the lattice column x = X:
 // Hx there, then Ey and Ez, with the general path's per-cell rules (ghosts,
 // PEC, CPML, H sources).  It reads only the step's inputs, so it depends on no
 // other launch of the step: the H of x = X - 1 that Ey and Ez see through the
@@ -1145,7 +1169,7 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   if (err != cudaSuccess) return err;
   const int kmax = p.Z + 1;
   const int zc = p.z_chunk > 0 ? p.z_chunk : kmax;
-  const int gx = p.X % T::TX == 0 ? p.X / T::TX : (p.X + T::TX) / T::TX;  // a multiple of 128 leaves column X to the column kernel
+  const int gx = (p.X + T::TX - 1) / T::TX;  // the tiles end at x = X - 1: column X is the column kernel's
   const int gy = (p.Y + 1 + T::TY - 1) / T::TY, gz = (kmax + zc - 1) / zc;
   Step3D q = p;
   q.z_chunk = zc;
@@ -1170,7 +1194,7 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   q.order[3] = zhi;
   const long long ctas = static_cast<long long>(gx) * gy * gz;
   if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-  if (p.X % T::TX == 0) {  // column X first: it reads only the step's inputs
+  {  // column X first: it reads only the step's inputs
     const dim3 cgrid((p.Y + 1 + kColJ - 1) / kColJ, (p.Z + 1 + kColK - 1) / kColK, 1);
     class_column_kernel<Cpml, Exact><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
     err = cudaPeekAtLastError();
