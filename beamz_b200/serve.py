@@ -52,6 +52,7 @@ class Result:
     admitted: float
     finished: float
     records: list | None = None  # per field recorder: runtime.recorded(...)
+    gpu_s: float | None = None  # device time of the request's steps (sequential path: CUDA events)
 
     @property
     def latency(self) -> float:
@@ -293,11 +294,16 @@ def run_sequential(requests: list[Request], device="cuda", return_fields: bool =
         admitted = clock() - t0
         program = runtime.compile_program(req.spec, device=dev, tile="auto", z_chunk="auto")
         state = runtime.initial_state(program)
+        stream = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         runtime.run_steps(state, program, req.nsteps)
+        e1.record(stream)
         out = _collect(state, program, return_fields)
         torch.cuda.synchronize(dev)
         results[req.rid] = Result(req.rid, req.nsteps, out["dft_re"], out["dft_im"], out["dft_w"], out["fields"],
-                                  req.arrival, admitted, clock() - t0, out["records"])
+                                  req.arrival, admitted, clock() - t0, out["records"],
+                                  gpu_s=e0.elapsed_time(e1) / 1e3)
         del state, program
     return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
 
@@ -313,9 +319,18 @@ class ServingStats:
 
 
 def summarize(results: list[Result]) -> ServingStats:
+    """Makespan, sims/s and latency percentiles; with per-request device
+    times (the sequential path) also the GPU-busy fraction of the makespan and
+    its inverse -- the most that filling the idle gaps between one request's
+    steps and the next can gain, unless requests too small to fill the GPU
+    also run side by side."""
     lat = np.array([r.latency for r in results])
     start = min(r.arrival for r in results)
     end = max(r.finished for r in results)
     span = max(end - start, 1e-9)
-    return ServingStats(len(results), span, len(results) / span, float(np.percentile(lat, 50)),
-                        float(np.percentile(lat, 99)))
+    stats = ServingStats(len(results), span, len(results) / span, float(np.percentile(lat, 50)),
+                         float(np.percentile(lat, 99)))
+    if all(r.gpu_s is not None for r in results):
+        busy = float(sum(r.gpu_s for r in results))
+        stats.extra = {"gpu_busy_s": busy, "gpu_busy_fraction": busy / span, "gap_filling_bound": span / max(busy, 1e-9)}
+    return stats

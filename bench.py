@@ -215,7 +215,8 @@ def serving_arm(args, rank, world):
                         "makespan_s": round(b.makespan_s, 2), "peak_resident": engine.peak_active,
                         "peak_gb": round(engine.peak_bytes / 1e9, 2)},
             "sequential": {"sims_per_s": round(q.sims_per_s, 3), "p50_s": round(q.p50_s, 3),
-                           "p99_s": round(q.p99_s, 3), "makespan_s": round(q.makespan_s, 2)},
+                           "p99_s": round(q.p99_s, 3), "makespan_s": round(q.makespan_s, 2),
+                           **{k: round(v, 3) for k, v in q.extra.items()}},
             "speedup": round(b.sims_per_s / q.sims_per_s, 3), "results_identical": same,
             "clocks": clocks.summary()}
     if rank == 0:
