@@ -16,12 +16,13 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_fdtd_b200.so")
 
-FDTD_ABI_VERSION = 12
+FDTD_ABI_VERSION = 13
 FDTD_F32, FDTD_S32, FDTD_BF16, FDTD_U8, FDTD_F64 = 0, 1, 2, 3, 4
 FDTD_FLAG_GRAPH_CACHE = 1 << 7
 FDTD_FLAG_DFT_OVERLAP = 1 << 16
 FDTD_FLAG_CLASSES = 1 << 17
 FDTD_FLAG_FAST_MATH = 1 << 19
+FDTD_FLAG_LOSSY = 1 << 20
 FDTD_FLAG_TEST_STALL = 1 << 18
 FDTD_SCHEDULE_PHASES, FDTD_SCHEDULE_FUSED = 0, 1
 FDTD_MATERIAL_SITE, FDTD_MATERIAL_VOXEL, FDTD_MATERIAL_CODEBOOK = 0, 1, 2
@@ -259,6 +260,8 @@ class FdtdProgram(ctypes.Structure):
         ("recorders", FdtdRecorder * FDTD_MAX_RECORDERS),
         ("site_class", FdtdBuffer),
         ("class_coef", FdtdBuffer),
+        ("h_class", FdtdBuffer),
+        ("h_class_coef", FdtdBuffer),
     ]
 
 

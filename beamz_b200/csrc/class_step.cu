@@ -63,7 +63,10 @@ namespace {
 constexpr int kSlots = 32;  // CPML coefficient slots staged per term
 constexpr unsigned kFull = 0xffffffffu;
 
-template <int NW>
+// Lossy: conductive material (FDTD_FLAG_LOSSY) -- per-class (decay, source)
+// pairs for E and H classes, the H classes staged with the halo; no x-psi
+// staging (its room holds the H classes).
+template <int NW, bool Lossy = false>
 struct ClassTile {
   static constexpr int TX = 128, TY = NW, NT = 32 * NW;
   static constexpr int BX = TX + 8;  // staged row: x from i0-4 to i0+131 (16-byte aligned start)
@@ -74,29 +77,43 @@ struct ClassTile {
   static constexpr int IBOX = TY * TX;  // class ids (bytes), rows j0 .. j0+TY-1, x i0 .. i0+127
   static constexpr int XW = 16;         // staged x-psi window (slots)
   static constexpr int XPS = ((HH * XW + 31) / 32) * 32;
+  // Lossy: H-class box, rows j0-1 .. j0+TY-1, x from i0-16 (a 16-byte
+  // coordinate for 1-byte elements) to i0+127: the own cells and the halo.
+  static constexpr int HW = TX + 16;
+  static constexpr int HIBYTES = HH * HW;
+  static constexpr int HIBOX = ((HIBYTES + 127) / 128) * 128;
   struct Smem {
     alignas(128) float e[3][3][EBOX];  // E ring: plane slot, component (TMA boxes start on 128 B)
     alignas(128) float h[2][3][HBOX];  // H (old) ring
     alignas(128) uint8_t ids[2][IBOX];
     alignas(16) float hn[3][HH][BX];   // H (new) of this plane: own rows + halo row, own columns + halo column
-    float4 cls[256];                   // per class: dt/(eps0 eps dx) of Ex, Ey, Ez
+    float4 cls[256];  // per class: dt/(eps0 eps dx) of Ex, Ey, Ez; Lossy: [128][4] (decay, source) float2
     float4 cc[12][kSlots];  // CPML (a, b, 1/kappa) (a/dx in the tolerance form): H terms 0-5, E terms 6-11
     float xd[2][TY][32];    // corrected x differences of a row's x-slab cells by slot (compact x work)
     // x-term psi (Hyx, Hzx, Eyx, Ezx) of the bundle's plane, staged with it:
     // rows j0-1 .. j0+TY-1, a 16-slot window of the tile's slab run.
-    alignas(128) float xps[2][4][XPS];
+    alignas(128) float xps[Lossy ? 1 : 2][4][Lossy ? 32 : XPS];
+    alignas(128) uint8_t hids[Lossy ? 2 : 1][Lossy ? HIBOX : 128];  // Lossy: H classes by plane parity
+    float2 hcls[Lossy ? 64 * 4 : 1];  // Lossy: [64][4] (decay, source) of Hx, Hy, Hz
     int xwin[4];            // each term's window start (slot)
     int xst[8][32];         // per lane: x-slab masks xs3, xs4, xe3, xe4 and compact items h0, h1, e0, e1
     float hcoef[6];         // uniform H decay (Hx, Hy, Hz) and source (over dx in the tolerance form)
     float amp[kMaxFusedSources];
     unsigned long long bar[2];
   };
+  // Every TMA destination starts on 128 bytes; two 8-warp CTAs fit an SM
+  // (228 KB less 1 KB reserved per CTA).
+  static_assert((EBOX * 4) % 128 == 0 && (HBOX * 4) % 128 == 0 && IBOX % 128 == 0 && (XPS * 4) % 128 == 0 &&
+                    HIBOX % 128 == 0,
+                "TMA ring slots keep 128-byte alignment");
+  static_assert(NW != 8 || sizeof(Smem) <= 233472 / 2 - 1024, "8-warp class step: two CTAs per SM");
 };
 
 struct ClassMaps {
   CUtensorMap e[3];
   CUtensorMap h[3];
   CUtensorMap ids;
+  CUtensorMap hids;  // Lossy: H classes
   CUtensorMap xpsi[4];  // x-term psi slabs (Hyx, Hzx, Eyx, Ezx), when Step3D::xstage
 };
 
@@ -190,6 +207,36 @@ template <bool Exact>
 __device__ __forceinline__ float e_upd(float e, float c, float d0, float d1) {
   if constexpr (Exact) return e + c * (d0 - d1);
   return fmaf(c, d0 - d1, e);
+}
+
+// Conductive material (FDTD_FLAG_LOSSY): per-class (decay, source) pairs,
+// tab[class * 4 + component].  E <- decay E + source (d0 - d1), beamz's
+// per-site form (the dense kernels' e_update); H as h1.
+template <bool Exact>
+__device__ __forceinline__ float e_loss(float e, float2 c, float d0, float d1) {
+  if constexpr (Exact) return c.x * e + c.y * (d0 - d1);
+  return fmaf(c.y, d0 - d1, c.x * e);
+}
+
+// Four cells whose classes are the bytes of `ids4`, component n.
+// E classes are at most 128, H classes at most 64 (the ids are masked so that
+// no byte can read past a table).
+constexpr unsigned kEClassMask = 127u, kHClassMask = 63u;
+
+template <bool Exact>
+__device__ __forceinline__ float4 e4_loss(float4 e, const float2* tab, uint32_t ids4, int n, float4 d0, float4 d1) {
+  return make_float4(e_loss<Exact>(e.x, tab[(ids4 & kEClassMask) * 4 + n], d0.x, d1.x),
+                     e_loss<Exact>(e.y, tab[((ids4 >> 8) & kEClassMask) * 4 + n], d0.y, d1.y),
+                     e_loss<Exact>(e.z, tab[((ids4 >> 16) & kEClassMask) * 4 + n], d0.z, d1.z),
+                     e_loss<Exact>(e.w, tab[((ids4 >> 24) & kEClassMask) * 4 + n], d0.w, d1.w));
+}
+
+template <bool Exact>
+__device__ __forceinline__ float4 h4_loss(float4 h, const float2* tab, uint32_t ids4, int n, float4 d0, float4 d1) {
+  const float2 c0 = tab[(ids4 & kHClassMask) * 4 + n], c1 = tab[((ids4 >> 8) & kHClassMask) * 4 + n];
+  const float2 c2 = tab[((ids4 >> 16) & kHClassMask) * 4 + n], c3 = tab[((ids4 >> 24) & kHClassMask) * 4 + n];
+  return make_float4(h1<Exact>(h.x, c0.x, c0.y, d0.x, d1.x), h1<Exact>(h.y, c1.x, c1.y, d0.y, d1.y),
+                     h1<Exact>(h.z, c2.x, c2.y, d0.z, d1.z), h1<Exact>(h.w, c3.x, c3.y, d0.w, d1.w));
 }
 
 // ---- CPML --------------------------------------------------------------------
@@ -422,10 +469,10 @@ __device__ __forceinline__ float ghost_diff(float center, float below, int v, in
 }
 
 // 8-warp CTAs: two per SM (shared memory), 128 registers; 4-warp CTAs: four.
-template <int NW, bool Cpml, bool Exact>
+template <int NW, bool Cpml, bool Exact, bool Lossy>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     class_step_kernel(const __grid_constant__ ClassMaps maps, const __grid_constant__ Step3D p) {
-  using T = ClassTile<NW>;
+  using T = ClassTile<NW, Lossy>;
   using S = typename T::Smem;
   constexpr int BX = T::BX, TX = T::TX, TY = T::TY;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -466,7 +513,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   // slots in this tile fits one 16-slot window starting on a multiple of 4
   // (16-byte TMA coordinate); otherwise the x work loads it directly.
   int xwin[4] = {0, 0, 0, 0};
-  bool xstage = xcompact && p.xstage;
+  bool xstage = xcompact && p.xstage && !Lossy;
   if (xstage) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -485,7 +532,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   auto issue = [&](int q, int slot, bool first) {
     const int ne = (first ? 1 : 0) + (q + 1 <= Z ? 1 : 0);
     const unsigned bytes =
-        ne * 3 * T::EH * BX * 4 + 3 * T::HH * BX * 4 + T::IBOX + (xstage ? 4 * T::XW * T::HH * 4 : 0);
+        ne * 3 * T::EH * BX * 4 + 3 * T::HH * BX * 4 + T::IBOX + (xstage ? 4 * T::XW * T::HH * 4 : 0) +
+        (Lossy ? T::HIBYTES : 0);
     unsigned long long* b = &sm.bar[slot];
     tma::bar_expect(b, bytes);
     if (p.test_stall) return;  // test-only: the barrier is armed, no copy is issued, nothing is in flight
@@ -495,6 +543,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
       for (int c = 0; c < 3; ++c) tma::load_3d(sm.e[(q + 1) % 3][c], &maps.e[c], i0 - 4, j0 - 1, q + 1, b);
     for (int c = 0; c < 3; ++c) tma::load_3d(sm.h[q % 2][c], &maps.h[c], i0 - 4, j0 - 1, q, b);
     tma::load_3d(sm.ids[q % 2], &maps.ids, i0, j0, q, b);
+    if constexpr (Lossy) tma::load_3d(sm.hids[q % 2], &maps.hids, i0 - 16, j0 - 1, q, b);
     if (xstage) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) tma::load_3d(sm.xps[q % 2][t], &maps.xpsi[t], xwin[t], j0 - 1, q, b);
@@ -510,6 +559,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     issue(kstart, 0, true);
   }
   for (int e = tid; e < 256; e += T::NT) sm.cls[e] = p.class_coef[e];
+  if constexpr (Lossy)
+    for (int e = tid; e < 64 * 4; e += T::NT) sm.hcls[e] = p.h_class_coef[e];
   bool cc_smem = true;
   if (Cpml) {
 #pragma unroll
@@ -609,6 +660,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     const float* HOy = sm.h[hs][1];
     const float* HOz = sm.h[hs][2];
     const uint8_t* IDS = sm.ids[hs];
+    const uint8_t* HIDS = sm.hids[Lossy ? hs : 0];  // Lossy: H classes, box column = x - i0 + 16
     const bool src = p.n_hsrc > 0 && sources_touch(p, k, j0 - 1, j0 + TY, i0 - 1, i0 + TX);
 
     if (fast_ok && !src && k >= 1 && k < Z) {
@@ -711,9 +763,17 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           dy1 = xtake(dy1, sm.xst[0][lane], sm.xd[0][warp]);
           dz0 = xtake(dz0, sm.xst[1][lane], sm.xd[1][warp]);
         }
-        float4 hx = h4<Exact>(ld4(HOx + rc), sm.hcoef[0], sm.hcoef[3], dx0, dx1);
-        float4 hy = h4<Exact>(ld4(HOy + rc), sm.hcoef[1], sm.hcoef[4], dy0, dy1);
-        const float4 hz = h4<Exact>(ld4(HOz + rc), sm.hcoef[2], sm.hcoef[5], dz0, dz1);
+        float4 hx, hy, hz;
+        if constexpr (Lossy) {
+          const uint32_t hw4 = *reinterpret_cast<const uint32_t*>(HIDS + r * T::HW + 16 + 4 * lane);
+          hx = h4_loss<Exact>(ld4(HOx + rc), sm.hcls, hw4, 0, dx0, dx1);
+          hy = h4_loss<Exact>(ld4(HOy + rc), sm.hcls, hw4, 1, dy0, dy1);
+          hz = h4_loss<Exact>(ld4(HOz + rc), sm.hcls, hw4, 2, dz0, dz1);
+        } else {
+          hx = h4<Exact>(ld4(HOx + rc), sm.hcoef[0], sm.hcoef[3], dx0, dx1);
+          hy = h4<Exact>(ld4(HOy + rc), sm.hcoef[1], sm.hcoef[4], dy0, dy1);
+          hz = h4<Exact>(ld4(HOz + rc), sm.hcoef[2], sm.hcoef[5], dz0, dz1);
+        }
         if (at_x0 && lane == 0 && wx0) hx.x = 0.0f;  // PEC: normal H on the x = 0 wall
         if (at_y0 && warp == 0 && wy0) hy = make_float4(0.f, 0.f, 0.f, 0.f);
         if (rowY && wy1) hy = make_float4(0.f, 0.f, 0.f, 0.f);  // PEC: normal H on the y = Y wall
@@ -736,7 +796,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
           if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false, nvv);
           if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false, nvv);
-          float4 h = h4<Exact>(ld4(HOx + b), sm.hcoef[0], sm.hcoef[3], d0, d1);
+          float4 h;
+          if constexpr (Lossy)
+            h = h4_loss<Exact>(ld4(HOx + b), sm.hcls, *reinterpret_cast<const uint32_t*>(HIDS + 16 + 4 * lane), 0,
+                               d0, d1);
+          else
+            h = h4<Exact>(ld4(HOx + b), sm.hcoef[0], sm.hcoef[3], d0, d1);
           if (at_x0 && lane == 0 && wx0) h.x = 0.0f;
           st4(&sm.hn[0][0][b], h);
         } else if (halo_row_z) {
@@ -758,7 +823,11 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
           if (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
           if (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false, nvv);
-          st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), sm.hcoef[2], sm.hcoef[5], d0, d1));
+          if constexpr (Lossy)
+            st4(&sm.hn[2][0][b], h4_loss<Exact>(ld4(HOz + b), sm.hcls,
+                                                *reinterpret_cast<const uint32_t*>(HIDS + 16 + 4 * lane), 2, d0, d1));
+          else
+            st4(&sm.hn[2][0][b], h4<Exact>(ld4(HOz + b), sm.hcoef[2], sm.hcoef[5], d0, d1));
         } else if (halo_col) {
           const int rr = 1 + lane, b = rr * BX + 3;
           const bool hz_ok = !(lyr && jc == Y);  // Hz has no row Y
@@ -770,13 +839,16 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
           if (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
           if (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
-          float hyv = h1<Exact>(HOy[b], sm.hcoef[1], sm.hcoef[4], d0, d1);
+          const int hc = Lossy ? (HIDS[rr * T::HW + 15] & kHClassMask) : 0;  // the halo column's H class
+          const float2 cy = Lossy ? sm.hcls[hc * 4 + 1] : make_float2(sm.hcoef[1], sm.hcoef[4]);
+          const float2 cz = Lossy ? sm.hcls[hc * 4 + 2] : make_float2(sm.hcoef[2], sm.hcoef[5]);
+          float hyv = h1<Exact>(HOy[b], cy.x, cy.y, d0, d1);
           if (at_y0 && jc == 0 && wy0) hyv = 0.0f;
           float f0 = D1(E0y[b + 1] - E0y[b]), f1 = D1(E0x[b + BX] - E0x[b]);  // Hz: dEy/dx, dEx/dy
           if (AX && hz_ok) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
           if (AY && hz_ok) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
           sm.hn[1][rr][3] = hyv;
-          sm.hn[2][rr][3] = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], f0, f1);
+          sm.hn[2][rr][3] = h1<Exact>(HOz[b], cz.x, cz.y, f0, f1);
         }
         __syncthreads();
         if (!emit) {
@@ -846,14 +918,22 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         }
         const float4 ex = ld4(E0x + rc), ey = ld4(E0y + rc), ez = ld4(E0z + rc);  // E(k) of the own cells
         const uint32_t w4 = *reinterpret_cast<const uint32_t*>(IDS + warp * TX + 4 * lane);
-        const float4 t0 = sm.cls[w4 & 0xffu], t1 = sm.cls[(w4 >> 8) & 0xffu];
-        const float4 t2 = sm.cls[(w4 >> 16) & 0xffu], t3 = sm.cls[w4 >> 24];
-        float4 nx = make_float4(e_upd<Exact>(ex.x, t0.x, fx0.x, fx1.x), e_upd<Exact>(ex.y, t1.x, fx0.y, fx1.y),
-                                e_upd<Exact>(ex.z, t2.x, fx0.z, fx1.z), e_upd<Exact>(ex.w, t3.x, fx0.w, fx1.w));
-        float4 ny = make_float4(e_upd<Exact>(ey.x, t0.y, fy0.x, fy1.x), e_upd<Exact>(ey.y, t1.y, fy0.y, fy1.y),
-                                e_upd<Exact>(ey.z, t2.y, fy0.z, fy1.z), e_upd<Exact>(ey.w, t3.y, fy0.w, fy1.w));
-        float4 nz = make_float4(e_upd<Exact>(ez.x, t0.z, fz0.x, fz1.x), e_upd<Exact>(ez.y, t1.z, fz0.y, fz1.y),
-                                e_upd<Exact>(ez.z, t2.z, fz0.z, fz1.z), e_upd<Exact>(ez.w, t3.z, fz0.w, fz1.w));
+        float4 nx, ny, nz;
+        if constexpr (Lossy) {
+          const float2* ec = reinterpret_cast<const float2*>(sm.cls);
+          nx = e4_loss<Exact>(ex, ec, w4, 0, fx0, fx1);
+          ny = e4_loss<Exact>(ey, ec, w4, 1, fy0, fy1);
+          nz = e4_loss<Exact>(ez, ec, w4, 2, fz0, fz1);
+        } else {
+          const float4 t0 = sm.cls[w4 & 0xffu], t1 = sm.cls[(w4 >> 8) & 0xffu];
+          const float4 t2 = sm.cls[(w4 >> 16) & 0xffu], t3 = sm.cls[w4 >> 24];
+          nx = make_float4(e_upd<Exact>(ex.x, t0.x, fx0.x, fx1.x), e_upd<Exact>(ex.y, t1.x, fx0.y, fx1.y),
+                           e_upd<Exact>(ex.z, t2.x, fx0.z, fx1.z), e_upd<Exact>(ex.w, t3.x, fx0.w, fx1.w));
+          ny = make_float4(e_upd<Exact>(ey.x, t0.y, fy0.x, fy1.x), e_upd<Exact>(ey.y, t1.y, fy0.y, fy1.y),
+                           e_upd<Exact>(ey.z, t2.y, fy0.z, fy1.z), e_upd<Exact>(ey.w, t3.y, fy0.w, fy1.w));
+          nz = make_float4(e_upd<Exact>(ez.x, t0.z, fz0.x, fz1.x), e_upd<Exact>(ez.y, t1.z, fz0.y, fz1.y),
+                           e_upd<Exact>(ez.z, t2.z, fz0.z, fz1.z), e_upd<Exact>(ez.w, t3.z, fz0.w, fz1.w));
+        }
         if (at_y0 && warp == 0 && wy0) {  // PEC: Ex, Ez on the y = 0 wall
           nx = make_float4(0.f, 0.f, 0.f, 0.f);
           nz = nx;
@@ -896,6 +976,12 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const int jj = j0 - 1 + rr, ii = i0 - 4 + cc, b = rr * BX + cc;
         own = own && ii < X;  // column X: the column kernel
         const int o = k * PL + jj * P + ii;
+        // H coefficients: uniform, or (Lossy) the point's H class (box column
+        // of x = ii: cc + 12).
+        auto hco = [&](int n) {
+          if constexpr (Lossy) return sm.hcls[(HIDS[rr * T::HW + cc + 12] & kHClassMask) * 4 + n];
+          return make_float2(sm.hcoef[n], sm.hcoef[3 + n]);
+        };
         const bool zZ = k < Z, yY = jj >= 0 && jj < Y, yY1 = jj >= 0 && jj <= Y;
         const bool iX = ii >= 0 && ii < X, iX1 = ii >= 0 && ii <= X;
         if ((which & 1) && zZ && yY && iX1) {  // Hx: dEz/dy - dEy/dz
@@ -904,7 +990,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 1>(p.ht[0], sm.cc[0], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 0>(p.ht[1], sm.cc[1], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOx[b], sm.hcoef[0], sm.hcoef[3], d0, d1);
+          const float2 c = hco(0);
+          float h = h1<Exact>(HOx[b], c.x, c.y, d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 3, k, jj, ii, h);
           if ((ii == 0 && wx0) || (ii == X && wx1)) h = 0.0f;
           sm.hn[0][rr][cc] = h;
@@ -916,7 +1003,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 0>(p.ht[2], sm.cc[2], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 2>(p.ht[3], sm.cc[3], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOy[b], sm.hcoef[1], sm.hcoef[4], d0, d1);
+          const float2 c = hco(1);
+          float h = h1<Exact>(HOy[b], c.x, c.y, d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 4, k, jj, ii, h);
           if ((jj == 0 && wy0) || (jj == Y && wy1)) h = 0.0f;
           sm.hn[1][rr][cc] = h;
@@ -928,7 +1016,8 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 2>(p.ht[4], sm.cc[4], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 1>(p.ht[5], sm.cc[5], cc_smem, res, k, jj, ii, d1, own);
           }
-          float h = h1<Exact>(HOz[b], sm.hcoef[2], sm.hcoef[5], d0, d1);
+          const float2 c = hco(2);
+          float h = h1<Exact>(HOz[b], c.x, c.y, d0, d1);
           if (src) h = h_sources_at(p, sm.amp, 5, k, jj, ii, h);
           if ((k == 0 && wz0) || (k == Z && wz1)) h = 0.0f;
           sm.hn[2][rr][cc] = h;
@@ -945,14 +1034,21 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const float hz_y = sm.hn[2][rr - 1][cc], hx_y = sm.hn[0][rr - 1][cc];
         const float hz_x = sm.hn[2][rr][cc - 1], hy_x = sm.hn[1][rr][cc - 1];
         const bool in_box = cc >= 4 && cc < 4 + TX && rr >= 1 && rr <= TY;
-        const float4 t = sm.cls[in_box ? IDS[(rr - 1) * TX + cc - 4] : p.site_class[(k * (Y + 1) + jj) * p.pitch8 + ii]];
+        const int cid = in_box ? IDS[(rr - 1) * TX + cc - 4] : p.site_class[(k * (Y + 1) + jj) * p.pitch8 + ii];
+        const float4 t = sm.cls[Lossy ? 0 : cid];
+        // E <- E + t.c (d0 - d1), or (Lossy) decay E + source (d0 - d1).
+        auto eup = [&](float e, int n, float d0, float d1) {
+          if constexpr (Lossy)
+            return e_loss<Exact>(e, reinterpret_cast<const float2*>(sm.cls)[(cid & kEClassMask) * 4 + n], d0, d1);
+          return e_upd<Exact>(e, n == 0 ? t.x : (n == 1 ? t.y : t.z), d0, d1);
+        };
         if (ii < X) {  // Ex: dHz/dy - dHy/dz
           float d0 = D1(ghost_diff(hz, hz_y, jj, Y, wy0, wy1)), d1 = D1(ghost_diff(hy, hyz, k, Z, wz0, wz1));
           if (cpml) {
             d0 = cpml1<Exact, 1>(p.et[0], sm.cc[6], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 0>(p.et[1], sm.cc[7], cc_smem, res, k, jj, ii, d1, true);
           }
-          float e = e_upd<Exact>(E0x[b], t.x, d0, d1);
+          float e = eup(E0x[b], 0, d0, d1);
           if ((k == 0 && wz0) || (k == Z && wz1) || (jj == 0 && wy0) || (jj == Y && wy1)) e = 0.0f;
           p.eout[0][o] = e;
         }
@@ -962,7 +1058,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 0>(p.et[2], sm.cc[8], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 2>(p.et[3], sm.cc[9], cc_smem, res, k, jj, ii, d1, true);
           }
-          float e = e_upd<Exact>(E0y[b], t.y, d0, d1);
+          float e = eup(E0y[b], 1, d0, d1);
           if ((k == 0 && wz0) || (k == Z && wz1) || (ii == 0 && wx0) || (ii == X && wx1)) e = 0.0f;
           p.eout[1][o] = e;
         }
@@ -972,7 +1068,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             d0 = cpml1<Exact, 2>(p.et[4], sm.cc[10], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 1>(p.et[5], sm.cc[11], cc_smem, res, k, jj, ii, d1, true);
           }
-          float e = e_upd<Exact>(E0z[b], t.z, d0, d1);
+          float e = eup(E0z[b], 2, d0, d1);
           if ((jj == 0 && wy0) || (jj == Y && wy1) || (ii == 0 && wx0) || (ii == X && wx1)) e = 0.0f;
           p.eout[2][o] = e;
         }
@@ -1040,7 +1136,7 @@ __device__ __forceinline__ float col_psi(const CpmlTermDev& t, int k, int j, int
   return slot >= 0 ? t.psi_in[psi_off<Axis>(t, slot, k, j, x)] : 0.0f;
 }
 
-template <bool Cpml, bool Exact>
+template <bool Cpml, bool Exact, bool Lossy>
 __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __grid_constant__ Step3D p) {
   __shared__ float hx[kColK + 1][kColJ + 1];  // new Hx at (k0 - 1 + a, j0 - 1 + b, X)
   __shared__ float amp[kMaxFusedSources];
@@ -1060,8 +1156,13 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
   const bool ey_ok = live && j < Y, ez_ok = live && k < Z;
   const int o = live ? k * PL + j * P + X : 0;
   const float ey0 = ey_ok ? p.ein[1][o] : 0.0f, ez0 = ez_ok ? p.ein[2][o] : 0.0f;
-  const float4 t = live ? p.class_coef[p.site_class[(static_cast<int64_t>(k) * (Y + 1) + j) * p.pitch8 + X]]
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+  const int cid = live ? p.site_class[(static_cast<int64_t>(k) * (Y + 1) + j) * p.pitch8 + X] : 0;
+  const float4 t = Lossy ? make_float4(0.f, 0.f, 0.f, 0.f) : p.class_coef[cid];
+  const float2* ec = reinterpret_cast<const float2*>(p.class_coef);  // Lossy: [128][4] (decay, source)
+  // Lossy: the (decay, source) of H component n at lattice point (kk, jj, x).
+  auto hco = [&](int kk, int jj, int x, int n) {
+    return p.h_class_coef[(p.h_class[(static_cast<int64_t>(kk) * (Y + 1) + jj) * p.pitch8 + x] & kHClassMask) * 4 + n];
+  };
   float q_eyz = 0.f, q_eyx = 0.f, q_ezx = 0.f, q_ezy = 0.f;
   if (Cpml) {
     if (ey_ok) {
@@ -1095,7 +1196,8 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
         d0 = col_cpml<Exact, 1>(p.ht[0], res, inv_res, qy, kk, jj, X, d0, own);
         d1 = col_cpml<Exact, 0>(p.ht[1], res, inv_res, qz, kk, jj, X, d1, own);
       }
-      h = h1<Exact>(p.hin[0][oh], hdec, hsrc, d0, d1);
+      const float2 c = Lossy ? hco(kk, jj, X, 0) : make_float2(hdec, hsrc);
+      h = h1<Exact>(p.hin[0][oh], c.x, c.y, d0, d1);
       if (p.n_hsrc > 0) h = h_sources_at(p, amp, 3, kk, jj, X, h);
       if (wx1) h = 0.0f;  // PEC: normal H on the x = X wall
       if (own) p.hout[0][oh] = h;
@@ -1116,7 +1218,9 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
         d0 = col_cpml<Exact, 2>(p.ht[4], res, inv_res, col_psi<2>(p.ht[4], k, j, X - 1), k, j, X - 1, d0, false);
         d1 = col_cpml<Exact, 1>(p.ht[5], res, inv_res, col_psi<1>(p.ht[5], k, j, X - 1), k, j, X - 1, d1, false);
       }
-      hz_w = h1<Exact>(p.hin[2][ow], p.hm.decay[2][0], p.hm.source[2][0] * (Exact ? 1.0f : inv_res), d0, d1);
+      const float2 c = Lossy ? hco(k, j, X - 1, 2)
+                             : make_float2(p.hm.decay[2][0], p.hm.source[2][0] * (Exact ? 1.0f : inv_res));
+      hz_w = h1<Exact>(p.hin[2][ow], c.x, c.y, d0, d1);
       if (p.n_hsrc > 0) hz_w = h_sources_at(p, amp, 5, k, j, X - 1, hz_w);
       if ((k == 0 && wz0) || (k == Z && wz1)) hz_w = 0.0f;
     }
@@ -1126,7 +1230,9 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
         d0 = col_cpml<Exact, 0>(p.ht[2], res, inv_res, col_psi<0>(p.ht[2], k, j, X - 1), k, j, X - 1, d0, false);
         d1 = col_cpml<Exact, 2>(p.ht[3], res, inv_res, col_psi<2>(p.ht[3], k, j, X - 1), k, j, X - 1, d1, false);
       }
-      hy_w = h1<Exact>(p.hin[1][ow], p.hm.decay[1][0], p.hm.source[1][0] * (Exact ? 1.0f : inv_res), d0, d1);
+      const float2 c = Lossy ? hco(k, j, X - 1, 1)
+                             : make_float2(p.hm.decay[1][0], p.hm.source[1][0] * (Exact ? 1.0f : inv_res));
+      hy_w = h1<Exact>(p.hin[1][ow], c.x, c.y, d0, d1);
       if (p.n_hsrc > 0) hy_w = h_sources_at(p, amp, 4, k, j, X - 1, hy_w);
       if ((j == 0 && wy0) || (j == Y && wy1)) hy_w = 0.0f;
     }
@@ -1138,7 +1244,7 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
       d0 = col_cpml<Exact, 0>(p.et[2], res, inv_res, q_eyz, k, j, X, d0, true);
       d1 = col_cpml<Exact, 2>(p.et[3], res, inv_res, q_eyx, k, j, X, d1, true);
     }
-    float e = e_upd<Exact>(ey0, t.y, d0, d1);
+    float e = Lossy ? e_loss<Exact>(ey0, ec[(cid & kEClassMask) * 4 + 1], d0, d1) : e_upd<Exact>(ey0, t.y, d0, d1);
     if ((k == 0 && wz0) || (k == Z && wz1) || wx1) e = 0.0f;
     p.eout[1][o] = e;
   }
@@ -1149,17 +1255,17 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
       d0 = col_cpml<Exact, 2>(p.et[4], res, inv_res, q_ezx, k, j, X, d0, true);
       d1 = col_cpml<Exact, 1>(p.et[5], res, inv_res, q_ezy, k, j, X, d1, true);
     }
-    float e = e_upd<Exact>(ez0, t.z, d0, d1);
+    float e = Lossy ? e_loss<Exact>(ez0, ec[(cid & kEClassMask) * 4 + 2], d0, d1) : e_upd<Exact>(ez0, t.z, d0, d1);
     if ((j == 0 && wy0) || (j == Y && wy1) || wx1) e = 0.0f;
     p.eout[2][o] = e;
   }
 }
 
-template <int NW, bool Cpml, bool Exact>
+template <int NW, bool Cpml, bool Exact, bool Lossy = false>
 cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
-  using T = ClassTile<NW>;
+  using T = ClassTile<NW, Lossy>;
   const size_t smem = sizeof(typename T::Smem);
-  auto kern = class_step_kernel<NW, Cpml, Exact>;
+  auto kern = class_step_kernel<NW, Cpml, Exact, Lossy>;
   int device = 0;
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess) return err;
@@ -1196,7 +1302,7 @@ cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   {  // column X first: it reads only the step's inputs
     const dim3 cgrid((p.Y + 1 + kColJ - 1) / kColJ, (p.Z + 1 + kColK - 1) / kColK, 1);
-    class_column_kernel<Cpml, Exact><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
+    class_column_kernel<Cpml, Exact, Lossy><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
     err = cudaPeekAtLastError();
     if (err != cudaSuccess) return err;
   }
@@ -1221,6 +1327,11 @@ cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
   if (!tma::encode(&maps.ids, CU_TENSOR_MAP_DATA_TYPE_UINT8, p.site_class, p.X + 1, p.Y + 1, p.Z + 1, P8,
                    P8 * (p.Y + 1), T::TX, T::TY))
     return cudaErrorInvalidValue;
+  // Conductive material: the H classes, rows j0-1 .. and x from i0-16 (a
+  // 16-byte coordinate for 1-byte elements), 144 bytes wide.
+  if (p.lossy && !tma::encode(&maps.hids, CU_TENSOR_MAP_DATA_TYPE_UINT8, p.h_class, p.X + 1, p.Y + 1, p.Z + 1, P8,
+                              P8 * (p.Y + 1), ClassTile<NW, true>::HW, T::HH))
+    return cudaErrorInvalidValue;
   // x-term psi slabs (Hyx, Hzx, Eyx, Ezx): (plane, row, slot) with rows of
   // low + high slots.  Staged only when every row is a multiple of 16 bytes
   // and every slab 16-byte aligned (TMA's stride and base rules).
@@ -1240,6 +1351,8 @@ cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
     }
     q.xstage = ok ? 1 : 0;
   }
+  if (q.lossy)  // exact arithmetic only (validated)
+    return q.cpml ? launch_class_t<NW, true, true, true>(s, maps, q) : launch_class_t<NW, false, true, true>(s, maps, q);
   if (q.fast_math) return q.cpml ? launch_class_t<NW, true, false>(s, maps, q) : launch_class_t<NW, false, false>(s, maps, q);
   return q.cpml ? launch_class_t<NW, true, true>(s, maps, q) : launch_class_t<NW, false, true>(s, maps, q);
 }

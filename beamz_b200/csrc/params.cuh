@@ -72,6 +72,11 @@ struct Step3D {
   // absorber cells; their CTAs are dispatched before the others.
   int order[4];
   int xstage;  // class step: the x-term psi slabs have tensor maps (staged with each plane's bundle)
+  // FDTD_FLAG_LOSSY class step: class_coef holds (decay, source) pairs per E
+  // class and component ([128][4] float2), h_class / h_class_coef the H ones.
+  int lossy;
+  const uint8_t* h_class;
+  const float2* h_class_coef;
   // Derivative metrics per axis (z, y, x), or null (isotropic: divide by res).
   const float* metric_h[3];  // [n_axis]: forward differences feeding H
   const float* metric_e[3];  // [n_axis + 1]: backward differences feeding E

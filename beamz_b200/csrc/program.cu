@@ -171,6 +171,18 @@ int validate(const FdtdProgram& p) {
       return kInvalid;
   }
   if ((p.flags & FDTD_FLAG_FAST_MATH) && !(p.flags & FDTD_FLAG_CLASSES)) return kInvalid;
+  if (p.flags & FDTD_FLAG_LOSSY) {
+    // Conductive classes: exact arithmetic, H classes on the E classes' rows.
+    if (!(p.flags & FDTD_FLAG_CLASSES) || (p.flags & FDTD_FLAG_FAST_MATH)) return kInvalid;
+    const FdtdBuffer &cls = p.site_class, &hc = p.h_class;
+    if (hc.element_type != FDTD_U8 || hc.rank != 3 || hc.data == nullptr ||
+        (reinterpret_cast<uintptr_t>(hc.data) & 15) != 0)
+      return kInvalid;
+    for (int a = 0; a < 3; ++a)
+      if (hc.dims[a] != cls.dims[a]) return kInvalid;
+    if (!is_f32(p.h_class_coef) || elements(p.h_class_coef) != 64 * 4 * 2 || p.h_class_coef.data == nullptr)
+      return kInvalid;
+  }
   if ((p.flags & FDTD_FLAG_TEST_STALL) && !pitched) return kInvalid;
   if (p.wait_limit_ns < 0) return kInvalid;
   if (p.cpml) {
@@ -406,6 +418,9 @@ Step3D make_step(const FdtdProgram& p, const Layout& L, int bank, bool fused, in
     s.site_class = static_cast<const uint8_t*>(p.site_class.data);
     s.pitch8 = static_cast<int>(p.site_class.dims[2]);
     s.class_coef = static_cast<const float4*>(p.class_coef.data);
+    s.lossy = (p.flags & FDTD_FLAG_LOSSY) ? 1 : 0;
+    s.h_class = static_cast<const uint8_t*>(p.h_class.data);
+    s.h_class_coef = static_cast<const float2*>(p.h_class_coef.data);
   }
   for (int a = 0; a < 3; ++a) {
     s.metric_h[a] = static_cast<const float*>(p.metric_h[a].data);

@@ -156,13 +156,10 @@ class ClassOverflow(ValueError):
     """More than 256 distinct (Ex, Ey, Ez) coefficient triples: no uint8 class ids."""
 
 
-def device_site_classes(words, coef, res: float, nx: int, z_block: int = 64, over_dx: bool = False):
-    """uint8 material classes of the codebook words (each distinct (Ex, Ey, Ez)
-    id triple one class, numbered in increasing word order) on rows of a
-    16-byte multiple, and the (256, 4) float32 table of each class's Ex, Ey,
-    Ez coefficients: the codebook's own values, or with ``over_dx`` divided by
-    the cell size (rounded once from float64) for the tolerance arithmetic.
-    Raises :class:`ClassOverflow` above 256 classes."""
+def _word_classes(words, nx: int, limit: int, what: str, z_block: int = 64):
+    """uint8 classes of codebook words: each distinct word (a triple of
+    per-component ids) one class, numbered in increasing word order, on rows of
+    a 16-byte multiple; returns the classes and the words of the classes."""
     torch = _torch()
     dev = words.device
     nz1, ny1, _ = (int(v) for v in words.shape)
@@ -173,21 +170,84 @@ def device_site_classes(words, coef, res: float, nx: int, z_block: int = 64, ove
         present += torch.bincount(w, minlength=1 << 24).to(torch.int32)[: 1 << 24].clamp_(max=1)
         present.clamp_(max=1)
     keys = torch.nonzero(present, as_tuple=False).reshape(-1)
-    if keys.numel() > 256:
-        raise ClassOverflow(f"{keys.numel()} distinct E coefficient triples (> 256)")
+    if keys.numel() > limit:
+        raise ClassOverflow(f"{keys.numel()} distinct {what} coefficient triples (> {limit})")
     lut = torch.zeros(1 << 24, dtype=torch.uint8, device=dev)
     lut[keys] = torch.arange(keys.numel(), device=dev, dtype=torch.int32).to(torch.uint8)
     classes = torch.zeros((nz1, ny1, pitch8), dtype=torch.uint8, device=dev)
     for k0 in range(0, nz1, z_block):
         w = words[k0:k0 + z_block, :, : nx + 1].long()
         classes[k0:k0 + z_block, :, : nx + 1] = lut[w]
-    k = keys.cpu().numpy().astype(np.int64)
+    return classes, keys.cpu().numpy().astype(np.int64)
+
+
+def device_site_classes(words, coef, res: float, nx: int, z_block: int = 64, over_dx: bool = False):
+    """uint8 material classes of the codebook words (each distinct (Ex, Ey, Ez)
+    id triple one class, numbered in increasing word order) on rows of a
+    16-byte multiple, and the (256, 4) float32 table of each class's Ex, Ey,
+    Ez coefficients: the codebook's own values, or with ``over_dx`` divided by
+    the cell size (rounded once from float64) for the tolerance arithmetic.
+    Raises :class:`ClassOverflow` above 256 classes."""
+    torch = _torch()
+    dev = words.device
+    classes, k = _word_classes(words, nx, 256, "E", z_block)
     c64 = np.asarray(coef.cpu().numpy() if hasattr(coef, "cpu") else coef, np.float64)
     table = np.zeros((256, 4), np.float32)
     for n in range(3):
         v = c64[n, (k >> (8 * n)) & 0xFF]
         table[: k.size, n] = (v / np.float64(np.float32(res)) if over_dx else v).astype(np.float32)
     return classes, torch.as_tensor(table, device=dev)
+
+
+def _pair_words(pairs: dict, comps, shapes: dict, lattice, device):
+    """Codebook words of per-site (decay, source) pairs: per component the
+    distinct pairs (at most 256, numbered in increasing bit order) and each
+    site's index, in bytes 0-2 of an int32 word per lattice point (0 where the
+    component has no site); returns the words and the (3, 256) decay and source
+    tables.  Raises :class:`ClassOverflow` above 256 pairs."""
+    torch = _torch()
+    words = torch.zeros(lattice, dtype=torch.int32, device=device)
+    dec_t = np.zeros((3, 256), np.float32)
+    src_t = np.zeros((3, 256), np.float32)
+    for n, c in enumerate(comps):
+        dec, src = pairs[c]
+        d = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(dec, np.float32), shapes[c])), device=device)
+        v = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(src, np.float32), shapes[c])), device=device)
+        key = (d.view(torch.int32).long() << 32) | (v.view(torch.int32).long() & 0xFFFFFFFF)
+        del d, v
+        table, ids = torch.unique(key, return_inverse=True)
+        del key
+        if table.numel() > 256:
+            raise ClassOverflow(f"{c}: {table.numel()} distinct (decay, source) pairs (> 256)")
+        dz, dy, dx = (int(x) for x in shapes[c])
+        words[:dz, :dy, :dx] |= ids.to(torch.int32) << (8 * n)
+        t = table.cpu().numpy()
+        dec_t[n, : t.size] = (t >> 32).astype(np.int32).view(np.float32)
+        src_t[n, : t.size] = (t & 0xFFFFFFFF).astype(np.uint32).view(np.float32)
+    return words, dec_t, src_t
+
+
+def device_lossy_classes(e_pairs: dict, h_pairs: dict, shapes: dict, lattice, nx: int, device):
+    """Conductive material on the class step (FDTD_FLAG_LOSSY): uint8 E and H
+    classes per lattice point -- each distinct (Ex, Ey, Ez), resp. (Hx, Hy,
+    Hz), triple of (decay, source) pairs one class -- and their [classes, 4, 2]
+    float32 tables, at most 128 E and 64 H classes (shared-memory tables of the
+    step).  The pairs are beamz's per-site coefficients as they are (E <-
+    decay E + source curl, H <- decay H - source curl).  Raises
+    :class:`ClassOverflow` above those counts."""
+    torch = _torch()
+    out = []
+    for pairs, comps, limit, what in ((e_pairs, ("Ex", "Ey", "Ez"), 128, "E"), (h_pairs, ("Hx", "Hy", "Hz"), 64, "H")):
+        words, dec_t, src_t = _pair_words(pairs, comps, shapes, lattice, device)
+        classes, k = _word_classes(words, nx, limit, what)
+        del words
+        table = np.zeros((limit, 4, 2), np.float32)
+        for n in range(3):
+            ids = (k >> (8 * n)) & 0xFF
+            table[: k.size, n, 0] = dec_t[n, ids]
+            table[: k.size, n, 1] = src_t[n, ids]
+        out += [classes, torch.as_tensor(table, device=device)]
+    return tuple(out)
 
 
 @dataclass
@@ -386,9 +446,12 @@ class DeviceProgram:
         site_sources = lossless_site_sources(spec)
         pitched_ok = (spec.ndim == 3 and (spec.voxel_ids is not None or site_sources is not None)
                       and schedule == "fused" and h_uniform and spec.metrics is None)
-        if layout == "pitched" and not pitched_ok:
-            raise ValueError("the pitched layout needs a 3D voxel program, the fused schedule, uniform H and an "
-                             "isotropic grid")
+        lossy_ok = (spec.ndim == 3 and spec.voxel_ids is None and site_sources is None and spec.e_site is not None
+                    and all(c in spec.e_site for c in ("Ex", "Ey", "Ez")) and schedule == "fused"
+                    and spec.metrics is None and step_kernel == "classes" and arithmetic == "exact")
+        if layout == "pitched" and not (pitched_ok or lossy_ok):
+            raise ValueError("the pitched layout needs a 3D voxel or per-site program, the fused schedule, an "
+                             "isotropic grid and (with conductive material) the class step in exact arithmetic")
         f32 = np.float32
         dt_over_eps = f32(spec.dt) / f32(EPS_0)
         self.site_ids = self.site_coef = self.site_eps_table = None
@@ -411,8 +474,36 @@ class DeviceProgram:
                 if layout == "pitched":
                     raise
                 layout = "dense"
-        elif layout == "auto":
+        elif layout == "auto" and not lossy_ok:
             layout = "dense"
+        # Conductive (per-site decay) 3D programs: the class step with E and H
+        # classes of (decay, source) pairs (FDTD_FLAG_LOSSY), when at most 128
+        # E and 64 H classes occur; else the dense per-site step.
+        self.lossy = False
+        self.h_class = self.h_class_coef = None
+        if lossy_ok and layout in ("auto", "pitched"):
+            nz, ny, nx = (int(v) for v in spec.grid_shape)
+            self.pitch = -(-(nx + 1) // 4) * 4
+            self.bank_shape = (nz + 1, ny + 1, self.pitch)
+            try:
+                e_pairs = {c: spec.e_site[c] for c in ("Ex", "Ey", "Ez")}
+                self.site_class, self.class_coef, self.h_class, self.h_class_coef = device_lossy_classes(
+                    e_pairs, spec.h_coefficients(), self.shapes, self.bank_shape, nx, dev)
+                # Energy diagnostics read the E-site permittivity through codebook words.
+                if spec.e_site_eps is not None and all(c in spec.e_site_eps for c in ("Ex", "Ey", "Ez")):
+                    eps = {c: (spec.e_site_eps[c], spec.e_site_eps[c]) for c in ("Ex", "Ey", "Ez")}
+                    self.site_ids, eps_t, _ = _pair_words(eps, ("Ex", "Ey", "Ez"), self.shapes, self.bank_shape, dev)
+                    self.site_eps_table = torch.as_tensor(eps_t, device=dev)
+                else:
+                    self.site_ids = torch.zeros(self.bank_shape, dtype=torch.int32, device=dev)
+                self.site_coef = torch.zeros((3, 256), dtype=torch.float32, device=dev)
+                self.lossy = True
+                layout = "pitched"
+            except ClassOverflow:
+                if layout == "pitched":
+                    raise
+                self.site_class = self.class_coef = self.h_class = self.h_class_coef = None
+                layout = "dense"
         self.layout = layout
         # The pitched 3D step: the class step (uint8 material classes, 128-wide
         # tiles) unless the scene has more than 256 distinct E coefficient
@@ -422,8 +513,9 @@ class DeviceProgram:
             raise ValueError("arithmetic is 'fast' or 'exact'")
         if step_kernel not in ("classes", "codebook"):
             raise ValueError("step_kernel is 'classes' or 'codebook'")
-        self.site_class = self.class_coef = None
-        if layout == "pitched" and step_kernel == "classes":
+        if not self.lossy:
+            self.site_class = self.class_coef = None
+        if layout == "pitched" and step_kernel == "classes" and not self.lossy:
             try:
                 self.site_class, self.class_coef = device_site_classes(
                     self.site_ids, self.site_coef, float(spec.resolution), int(spec.grid_shape[2]),
@@ -443,6 +535,8 @@ class DeviceProgram:
             s.flags |= abi.FDTD_FLAG_CLASSES
             if arithmetic == "fast":
                 s.flags |= abi.FDTD_FLAG_FAST_MATH
+            if self.lossy:
+                s.flags |= abi.FDTD_FLAG_LOSSY
         s.wait_limit_ns = int(wait_limit_ns)
         if test_stall:  # test only: the pitched step's first wait runs out (nothing in flight)
             s.flags |= abi.FDTD_FLAG_TEST_STALL
@@ -489,6 +583,9 @@ class DeviceProgram:
             if self.site_class is not None:
                 s.site_class = buf(self.site_class)
                 s.class_coef = buf(self.class_coef)
+            if self.lossy:
+                s.h_class = buf(self.h_class)
+                s.h_class_coef = buf(self.h_class_coef)
         elif spec.voxel_ids is not None:
             s.material_kind = abi.FDTD_MATERIAL_VOXEL
             ids = np.ascontiguousarray(spec.voxel_ids, dtype=np.uint8)
@@ -512,6 +609,8 @@ class DeviceProgram:
             if c not in self.active:
                 continue
             i = COMPONENT_INDEX[c] - 3
+            if self.lossy:  # the H classes carry them; the pitched layout takes scalars here
+                dec, src = np.float32(1.0), np.float32(0.0)
             s.h_decay[i] = buf(_f32(dec, dev))
             s.h_source_site[i] = buf(_f32(src, dev))
         # CPML coefficient slabs.
@@ -890,6 +989,8 @@ def field_diagnostics(state: DeviceState, program: DeviceProgram) -> FieldDiagno
     partials, out = state._diag_scratch
     d = abi.FdtdDiagnostics()
     if program.layout == "pitched":
+        if program.site_eps_table is None:
+            raise ValueError("energy diagnostics of a conductive program need the spec's e_site_eps")
         d.site_eps_table = abi.buffer_of(program.site_eps_table)
     else:
         for i, c in enumerate(("Ex", "Ey", "Ez")):

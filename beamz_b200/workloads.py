@@ -82,6 +82,22 @@ def scene_3d_512(total_steps=1000, seed=0, shape=(256, 512, 512), pml_cells=12, 
                          sources=srcs, monitors=mons, total_steps=total_steps)
 
 
+def conductive(spec: P.ProgramSpec, sigma_by_id=(0.0, 4e4)) -> P.ProgramSpec:
+    """The same scene with conductive material: voxel id v gets conductivity
+    ``sigma_by_id[v]`` (S/m; default lossy Si, lossless oxide), lowered to
+    beamz's per-site E and H (decay, source) coefficients
+    (:func:`plan.lossy_site_coefficients_3d`, compile.py:563-640)."""
+    import dataclasses
+
+    ids = np.asarray(spec.voxel_ids)
+    table = np.ones(256, np.float32)
+    table[: len(spec.eps_table)] = spec.eps_table
+    sig = np.zeros(256, np.float32)
+    sig[: len(sigma_by_id)] = sigma_by_id
+    e_site, h_site, e_eps = P.lossy_site_coefficients_3d(table[ids], sig[ids], spec.dt)
+    return dataclasses.replace(spec, voxel_ids=None, eps_table=None, e_site=e_site, h_site=h_site, e_site_eps=e_eps)
+
+
 def scene_capacity(total_steps=500, seed=0, shape=(1024, 1024, 1536), pml_cells=12, monitors=False):
     nz, ny, nx = shape
     rng = np.random.default_rng(seed)
@@ -207,11 +223,20 @@ SCENES = {"3d_512": scene_3d_512, "capacity": scene_capacity, "2d_400": scene_2d
 
 def algorithmic_bytes(spec: P.ProgramSpec) -> int:
     """DRAM bytes one step must move at minimum: every field element read and
-    written once (4 B each way), every voxel id read once, every CPML psi
-    element read and written once.  DFT and coefficient traffic is excluded."""
+    written once (4 B each way), one material byte per cell (a voxel id, or an
+    E class and, with per-site H, an H class), every CPML psi element read and
+    written once.  DFT and coefficient traffic is excluded."""
     active = P.active_components(spec.ndim, spec.polarization)
     shapes = {c: P.component_shape(c, spec.grid_shape, spec.polarization) for c in active}
     field = sum(int(np.prod(s)) for s in shapes.values())
     psi = sum(int(np.prod(t.psi_shape(shapes[t.component]))) for t in list(spec.h_terms) + list(spec.e_terms))
-    voxels = int(np.prod(spec.grid_shape)) if spec.voxel_ids is not None else 0
-    return 8 * field + voxels + 8 * psi
+    cells = int(np.prod(spec.grid_shape))
+    if spec.voxel_ids is not None:
+        material = cells  # one voxel id per cell
+    elif spec.e_site is not None and spec.ndim == 3:
+        # Per-site material: one E class per cell, and one H class where H is per site too.
+        h_site = any(np.ndim(d) or np.ndim(s) for d, s in spec.h_coefficients().values())
+        material = cells * (2 if h_site else 1)
+    else:
+        material = 0
+    return 8 * field + material + 8 * psi

@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--z-chunk", type=int, default=16)
     ap.add_argument("--cpml-faces", choices=["all", "x", "y", "z", "none"], default="all",
                     help="3d_512 only: the faces that carry the absorber (the absorber's cost per axis)")
+    ap.add_argument("--material", choices=["dielectric", "conductive"], default="dielectric",
+                    help="3d_512 only: conductive Si boxes (sigma 4e4 S/m: per-site E and H decay)")
     ap.add_argument("--step-kernel", choices=["classes", "codebook"], default=None,
                     help="pitched 3D step (default: the runtime's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -147,7 +149,8 @@ def cpu_sample(spec_fn, total_steps, budget_s, threads=0):
 
 def config_block(args, spec) -> dict:
     """The workload description both arms print (the driver compares them)."""
-    scene = {"3d_512": "3d_512x512x256_cpml12_sibox_dipole_dft4x5", "capacity": "capacity_1536x1024x1024_cpml12",
+    scene = {"3d_512": "3d_512x512x256_cpml12_sibox_dipole_dft4x5" + ("_conductive" if getattr(args, "material", "") == "conductive" else ""),
+             "capacity": "capacity_1536x1024x1024_cpml12",
              "2d_400": "2d_400x400_tm_cpml20_strip_dft3"}[args.scene]
     return {"workload": scene, "grid_zyx": [int(v) for v in spec.grid_shape], "cells": int(spec.cells),
             "parallelism": f"replicas x{max(1, int(os.environ.get('WORLD_SIZE', '1')))}",
@@ -430,6 +433,8 @@ def main():
         shape_kw["cpml_edges"] = {"x": ("left", "right"), "y": ("bottom", "top"), "z": ("front", "back"),
                                   "none": ()}[args.cpml_faces]
     spec = scene_fn(total_steps=total, **shape_kw)
+    if args.material == "conductive":
+        spec = W.conductive(spec)
     sk = {"step_kernel": args.step_kernel} if args.step_kernel else {}
     prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
     state = R.initial_state(prog)
@@ -476,6 +481,8 @@ def main():
     # ---- dominant kernel alone: the fused step without sources or monitors ---
     if args.scene == "3d_512":
         kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw)
+        if args.material == "conductive":
+            kspec = W.conductive(kspec)
         kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
         kstate = R.initial_state(kprog)
     else:  # other scenes time their own step (a second copy of the 1.6 G-cell scene would not fit)
@@ -499,7 +506,8 @@ def main():
     # The ncu capture of the dominant kernel on this workload, when one is committed.
     kname = {"classes": "class_step", "codebook": "tma_step"}.get(prog.step_kernel, "fused_step")
     prof = os.path.join(ROOT, "profiles", f"{kname}_{args.scene}.json")
-    if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16 and args.cpml_faces == "all":
+    if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16 and args.cpml_faces == "all" \
+            and args.material == "dielectric":
         with open(prof) as fh:
             traffic = json.load(fh).get("dram_bytes_per_launch")
 

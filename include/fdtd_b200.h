@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 /* Bumped whenever a struct below changes layout (beamz: abi_layout.json "abi_version"). */
-#define FDTD_ABI_VERSION 12
+#define FDTD_ABI_VERSION 13
 
 /* Element types (beamz: cuda/src/launch.h:6-10, plus U8 for voxel ids and F64
  * for reduction results). */
@@ -56,6 +56,13 @@ enum {
  * to the float32 noise floor of the run itself (that of float32 against
  * float64), so parity with the float32 path is a tolerance, not equality. */
 #define FDTD_FLAG_FAST_MATH (1 << 19)
+/* With FDTD_FLAG_CLASSES: conductive (lossy) material on the class step.
+ * class_coef then holds F32 [128, 4, 2] -- per E class and component (Ex, Ey,
+ * Ez, unused) the (decay, source) pair of E <- decay E + source curl -- and
+ * h_class / h_class_coef give each lattice point an H class (at most 64) with
+ * F32 [64, 4, 2] (decay, source) pairs of H <- decay H - source curl
+ * (beamz: compile.py:563-640 per-site coefficients).  Exact arithmetic only. */
+#define FDTD_FLAG_LOSSY (1 << 20)
 /* Test only: the pitched step arms its first copy barrier without issuing the
  * copies, so its bounded wait runs out after wait_limit_ns with nothing in
  * flight, and the kernel returns after setting `status` -- the expiry path,
@@ -290,6 +297,10 @@ typedef struct FdtdProgram {
    * coefficient triple of the codebook. */
   FdtdBuffer site_class;
   FdtdBuffer class_coef;
+  /* FDTD_FLAG_LOSSY: U8 [Z+1, Y+1, pitch8] H class of every lattice point and
+   * its F32 [64, 4, 2] (decay, source) table (see FDTD_FLAG_LOSSY). */
+  FdtdBuffer h_class;
+  FdtdBuffer h_class_coef;
 } FdtdProgram;
 
 /* ABI version of the loaded library (beamz: cuda/src/extension.cc __abi_version__). */

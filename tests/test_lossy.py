@@ -37,7 +37,7 @@ def test_lossy_coefficients_match_the_reference():
     np.testing.assert_array_equal(e64["Ex"][0], GOLD["decay_Ex"])
 
 
-def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12, sigma_of=None):
+def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12, sigma_of=None, metallic=()):
     """A conductive 3D scene (boxes of eps and of sigma, CPML on every face,
     a pre-E dipole, an H source and a DFT plane) as a ProgramSpec, and the
     oracle program with both lossy forms available.  ``sigma_of(sigma)``
@@ -67,7 +67,8 @@ def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12, sigma_of=None
     mon = P.plane_monitor(grid, res, "x", 0.6 * grid[2] * res, (np.arange(pml_cells, grid[0] - pml_cells) + 0.5) * res,
                           (np.arange(pml_cells, grid[1] - pml_cells) + 0.5) * res, np.array([0.9, 1.1]) * f0)
     spec = P.ProgramSpec(tuple(grid), dt, res, e_site=e_site, h_site=h_site, e_site_eps=e_eps, h_terms=h_terms,
-                         e_terms=e_terms, sources=srcs, monitors=[mon], total_steps=nsteps)
+                         e_terms=e_terms, sources=srcs, monitors=[mon], total_steps=nsteps,
+                         metallic_edges=frozenset(metallic))
     shapes = O.component_shapes(grid)
     terms = lambda ts: [O.CpmlTerm(t.component, t.axis, t.sign, t.low, t.high, t.a, t.b, t.inv_kappa,  # noqa: E731
                                    shapes[t.component][t.axis]) for t in ts]
@@ -80,7 +81,7 @@ def lossy_scene(grid=(10, 12, 20), seed=0, pml_cells=3, nsteps=12, sigma_of=None
                              m.window_code, m.normalization_code, m.length_unit) for m in spec.monitors]
     monitors[0].value_offset, monitors[0].weight_offset = 0, 0
     oprog = O.OracleProgram(tuple(grid), dt, res, terms(h_terms), terms(e_terms), material=material,
-                            sources=sources, monitors=monitors)
+                            sources=sources, monitors=monitors, metallic_edges=frozenset(metallic))
     return spec, oprog, e_site, h_site, (eps, sigma)
 
 
