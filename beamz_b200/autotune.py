@@ -1,15 +1,20 @@
 """Per-grid-shape choice of the 3D step's tile shape and z chunk.
 
-The fused 3D step (csrc/fused_tma.cu) has two launch knobs: the CTA's y rows
-(`tile_y`: 4, 8 or 16 rows of 32 lattice points) and the number of z planes
-one CTA marches (`z_chunk`).  Large grids want long chunks (fewer re-read
-boundary planes); small grids want short ones, so that more CTAs are resident
-and each CTA's plane chain is shorter.  `choose` returns the measured best for
-a shape class, measuring the candidates once on the device when asked to
-(`tune=True`) and remembering the result in a JSON table; without a table
-entry it falls back to rules fitted to B200 measurements.
+The class step (csrc/class_step.cu, the pitched 3D hot path) has two launch
+knobs: the CTA's rows (`tile_y`: 8 or 4 rows of 128 lattice points, 8 or 4
+warps) and the number of z planes one CTA marches (`z_chunk`).  Large grids
+want long chunks (fewer re-read boundary planes); small grids want short
+ones, so that more CTAs are resident and each CTA's plane chain is shorter.
+`choose` returns the measured best for a shape class, measuring the
+candidates once on the device when asked to (`tune=True`) and remembering the
+result in a JSON table; without a table entry it falls back to rules fitted
+to B200 measurements.
 
-Temporal blocking is not implemented (depth 1): one launch advances one step.
+The temporal-block depth is 1 (one launch advances one step): a second step
+inside the z-march would need the first step's E and H on a one- to two-cell
+x / y ring around each tile (25-50 % more work on 8-row tiles) and a second
+set of plane rings in shared memory, which the step's two CTAs per SM already
+fill.
 """
 
 from __future__ import annotations
@@ -20,7 +25,7 @@ import threading
 
 import numpy as np
 
-TILE_Y = (4, 8, 16)
+TILE_Y = (8, 4)
 Z_CHUNKS = (4, 8, 16, 32)
 _LOCK = threading.Lock()
 _MEMO: dict = {}
@@ -73,7 +78,7 @@ def measure(spec, device="cuda", steps: int = 24, candidates=None) -> dict:
     candidates = candidates or [(ty, zc) for ty in TILE_Y for zc in Z_CHUNKS]
     out = {}
     for ty, zc in candidates:
-        prog = runtime.compile_program(spec, device=dev, tile=(32, ty), z_chunk=zc, graphs=True)
+        prog = runtime.compile_program(spec, device=dev, tile=(128, ty), z_chunk=zc, graphs=True)
         if prog.layout != "pitched":
             return {}
         prog._times_for(3 * steps + 4)
