@@ -45,10 +45,16 @@ def shape_class(spec) -> str:
 
 
 def heuristic(spec) -> tuple[int, int]:
-    """Rules from B200 sweeps: 8-row tiles throughout; 16-plane chunks once the
-    grid holds enough CTAs for many waves, 8-plane chunks below that."""
+    """Rules from B200 sweeps of the class step (us per step, best first):
+    8-row tiles throughout; 16-plane chunks once the grid holds enough CTAs
+    for many waves (512x512x256: 903 vs 946 with 8), 8-plane chunks below
+    that (192^3: 247 vs 283 with 4), 4-plane chunks for grids of a few
+    million cells, whose CTAs would otherwise not fill the GPU (128^3: 75 vs
+    92 with 8)."""
     cells = int(np.prod(spec.grid_shape))
-    return (8, 16) if cells >= 32 * 1024 * 1024 else (8, 8)
+    if cells >= 32 * 1024 * 1024:
+        return (8, 16)
+    return (8, 8) if cells >= 4 * 1024 * 1024 else (8, 4)
 
 
 def _load(path: str) -> dict:
