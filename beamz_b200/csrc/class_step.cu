@@ -469,7 +469,9 @@ __device__ __forceinline__ float ghost_diff(float center, float below, int v, in
 }
 
 // 8-warp CTAs: two per SM (shared memory), 128 registers; 4-warp CTAs: four.
-template <int NW, bool Cpml, bool Exact, bool Lossy>
+// Partial: X is not a multiple of 128 (the last tile is partial); only then
+// do the run-time bodies carry the per-lane store masks.
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     class_step_kernel(const __grid_constant__ ClassMaps maps, const __grid_constant__ Step3D p) {
   using T = ClassTile<NW, Lossy>;
@@ -680,7 +682,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         // The run-time and last-row bodies also take the partial last tile:
         // stores and psi accesses stop at x = X (nv); the others handle all
         // four cells of every lane with no test.
-        const int nvv = (RT || LY) ? nv : 4;
+        const int nvv = Partial && (RT || LY) ? nv : 4;
         const bool lyr = LY || (RT && ylast);
         const bool st = !lyr || own;       // this row is stored
         const bool rowY = lyr && j == Y;   // row Y: Hx, Hz, Ey absent
@@ -1261,11 +1263,20 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
   }
 }
 
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
+cudaError_t launch_class_p(cudaStream_t s, const ClassMaps& maps, const Step3D& p);
+
 template <int NW, bool Cpml, bool Exact, bool Lossy = false>
 cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
+  if (p.X % ClassTile<NW, Lossy>::TX != 0) return launch_class_p<NW, Cpml, Exact, Lossy, true>(s, maps, p);
+  return launch_class_p<NW, Cpml, Exact, Lossy, false>(s, maps, p);
+}
+
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
+cudaError_t launch_class_p(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
   using T = ClassTile<NW, Lossy>;
   const size_t smem = sizeof(typename T::Smem);
-  auto kern = class_step_kernel<NW, Cpml, Exact, Lossy>;
+  auto kern = class_step_kernel<NW, Cpml, Exact, Lossy, Partial>;
   int device = 0;
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess) return err;
