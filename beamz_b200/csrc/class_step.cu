@@ -471,7 +471,7 @@ __device__ __forceinline__ float ghost_diff(float center, float below, int v, in
 // 8-warp CTAs: two per SM (shared memory), 128 registers; 4-warp CTAs: four.
 // Partial: X is not a multiple of 128 (the last tile is partial); only then
 // do the run-time bodies carry the per-lane store masks.
-template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial, bool Metric>
 __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
     class_step_kernel(const __grid_constant__ ClassMaps maps, const __grid_constant__ Step3D p) {
   using T = ClassTile<NW, Lossy>;
@@ -592,6 +592,56 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
   const float dbs = p.div_bs, drs = p.div_rs;  // div_rn's scaled cell size and reciprocal
   auto D1 = [&](float v) { return dv<Exact>(v, dbs, drs); };
   auto D4 = [&](float4 v) { return dv4<Exact>(v, dbs, drs); };
+  // Derivatives along an axis at a coordinate: with Metric (axis-uniform and
+  // rectilinear grids, 3D: every axis carries one) the difference times the
+  // inverse distance there (beamz/simulation/kernels.py:164-176, 293-323),
+  // forward differences (feeding H) on metric_h at 0..n-1, backward ones
+  // (feeding E) on metric_e at 0..n; halo coordinates that are never stored
+  // are clamped into the arrays.  Otherwise D1 / D4.  MH4 / ME4 take four
+  // cells on one coordinate (z or y), MH4x / ME4x the four x cells from c.
+  auto MH = [&](float v, int axis, int c) -> float {
+    if constexpr (Metric) return v * p.metric_h[axis][clampi(c, axis_cells(p, axis) - 1)];
+    else return D1(v);
+  };
+  auto ME = [&](float v, int axis, int c) -> float {
+    if constexpr (Metric) return v * p.metric_e[axis][clampi(c, axis_cells(p, axis))];
+    else return D1(v);
+  };
+  auto MH4 = [&](float4 v, int axis, int c) -> float4 {
+    if constexpr (Metric) {
+      const float m = p.metric_h[axis][clampi(c, axis_cells(p, axis) - 1)];
+      return make_float4(v.x * m, v.y * m, v.z * m, v.w * m);
+    } else {
+      return D4(v);
+    }
+  };
+  auto ME4 = [&](float4 v, int axis, int c) -> float4 {
+    if constexpr (Metric) {
+      const float m = p.metric_e[axis][clampi(c, axis_cells(p, axis))];
+      return make_float4(v.x * m, v.y * m, v.z * m, v.w * m);
+    } else {
+      return D4(v);
+    }
+  };
+  auto MH4x = [&](float4 v, int c) -> float4 {
+    if constexpr (Metric) {
+      const float* m = p.metric_h[2];
+      const int hi = X - 1;
+      return make_float4(v.x * m[clampi(c, hi)], v.y * m[clampi(c + 1, hi)], v.z * m[clampi(c + 2, hi)],
+                         v.w * m[clampi(c + 3, hi)]);
+    } else {
+      return D4(v);
+    }
+  };
+  auto ME4x = [&](float4 v, int c) -> float4 {
+    if constexpr (Metric) {
+      const float* m = p.metric_e[2];
+      return make_float4(v.x * m[clampi(c, X)], v.y * m[clampi(c + 1, X)], v.z * m[clampi(c + 2, X)],
+                         v.w * m[clampi(c + 3, X)]);
+    } else {
+      return D4(v);
+    }
+  };
 
   const int r = 1 + warp;              // own row in the staged boxes and hn
   const int j = j0 + warp;             // its lattice row
@@ -732,7 +782,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const int t = second ? 1 : 0;
               const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
-              const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, D1(Erow[b + 1] - Erow[b]), &nv);
+              const float dp = cpml_d<Exact>(sm.cc[second ? 4 : 3][slot], res, psi, MH(Erow[b + 1] - Erow[b], 2, i0 + xo), &nv);
               if (emit && st) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
@@ -748,9 +798,9 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
             ez4 = E0z[rc + 4];
             ey4 = E0y[rc + 4];
           }
-          dx0 = D4(sub4(ld4(E0z + rc + BX), ez)), dx1 = D4(sub4(ld4(E1y + rc), ey));   // Hx: dEz/dy, dEy/dz
-          dy0 = D4(sub4(ld4(E1x + rc), ex)), dy1 = D4(sub4(next4(ez, ez4), ez));       // Hy: dEx/dz, dEz/dx
-          dz0 = D4(sub4(next4(ey, ey4), ey)), dz1 = D4(sub4(ld4(E0x + rc + BX), ex));  // Hz: dEy/dx, dEx/dy
+          dx0 = MH4(sub4(ld4(E0z + rc + BX), ez), 1, j), dx1 = MH4(sub4(ld4(E1y + rc), ey), 0, k);  // Hx: dEz/dy, dEy/dz
+          dy0 = MH4(sub4(ld4(E1x + rc), ex), 0, k), dy1 = MH4x(sub4(next4(ez, ez4), ez), i);       // Hy: dEx/dz, dEz/dx
+          dz0 = MH4x(sub4(next4(ey, ey4), ey), i), dz1 = MH4(sub4(ld4(E0x + rc + BX), ex), 1, j);  // Hz: dEy/dx, dEx/dy
         }
         if (AY && !rowY) {
           dx0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], j), qh0, k, j, i, res, dx0, emit && st, nvv);
@@ -795,7 +845,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           float4 qa, qb;
           if (AY) qa = psi4_fetch<1>(p.ht[0], slot_of(p.ht[0], jh), k, jh, i, nvv);
           if (AZ) qb = psi4_fetch<0>(p.ht[1], slot_of(p.ht[1], k), k, jh, i, nvv);
-          float4 d0 = D4(sub4(ld4(E0z + b + BX), ld4(E0z + b))), d1 = D4(sub4(ld4(E1y + b), ld4(E0y + b)));
+          float4 d0 = MH4(sub4(ld4(E0z + b + BX), ld4(E0z + b)), 1, jh), d1 = MH4(sub4(ld4(E1y + b), ld4(E0y + b)), 0, k);
           if (AY) d0 = psi4_apply<Exact, 1>(p.ht[0], sm.cc[0], slot_of(p.ht[0], jh), qa, k, jh, i, res, d0, false, nvv);
           if (AZ) d1 = psi4_apply<Exact, 0>(p.ht[1], sm.cc[1], slot_of(p.ht[1], k), qb, k, jh, i, res, d1, false, nvv);
           float4 h;
@@ -822,7 +872,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           const float4 eyh = ld4(E0y + b);
           float e4 = __shfl_down_sync(kFull, eyh.x, 1);
           if (lane == 31) e4 = E0y[b + 4];
-          float4 d0 = D4(sub4(next4(eyh, e4), eyh)), d1 = D4(sub4(ld4(E0x + b + BX), ld4(E0x + b)));
+          float4 d0 = MH4x(sub4(next4(eyh, e4), eyh), i), d1 = MH4(sub4(ld4(E0x + b + BX), ld4(E0x + b)), 1, jh);
           if (AX) d0 = psix_apply<Exact>(p.ht[4], sm.cc[4], xs4, qa, k, jh, res, d0, false);
           if (AY) d1 = psi4_apply<Exact, 1>(p.ht[5], sm.cc[5], slot_of(p.ht[5], jh), qb, k, jh, i, res, d1, false, nvv);
           if constexpr (Lossy)
@@ -838,7 +888,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if (AX) qc1 = psi1_fetch<2>(p.ht[3], k, jc, ih);
           if (AX && hz_ok) qc2 = psi1_fetch<2>(p.ht[4], k, jc, ih);
           if (AY && hz_ok) qc3 = psi1_fetch<1>(p.ht[5], k, jc, ih);
-          float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);  // Hy: dEx/dz, dEz/dx
+          float d0 = MH(E1x[b] - E0x[b], 0, k), d1 = MH(E0z[b + 1] - E0z[b], 2, ih);  // Hy: dEx/dz, dEz/dx
           if (AZ) d0 = psi1_apply<Exact, 0>(p.ht[2], sm.cc[2], qc0, k, jc, ih, res, d0, false);
           if (AX) d1 = psi1_apply<Exact, 2>(p.ht[3], sm.cc[3], qc1, k, jc, ih, res, d1, false);
           const int hc = Lossy ? (HIDS[rr * T::HW + 15] & kHClassMask) : 0;  // the halo column's H class
@@ -846,7 +896,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           const float2 cz = Lossy ? sm.hcls[hc * 4 + 2] : make_float2(sm.hcoef[2], sm.hcoef[5]);
           float hyv = h1<Exact>(HOy[b], cy.x, cy.y, d0, d1);
           if (at_y0 && jc == 0 && wy0) hyv = 0.0f;
-          float f0 = D1(E0y[b + 1] - E0y[b]), f1 = D1(E0x[b + BX] - E0x[b]);  // Hz: dEy/dx, dEx/dy
+          float f0 = MH(E0y[b + 1] - E0y[b], 2, ih), f1 = MH(E0x[b + BX] - E0x[b], 1, jc);  // Hz: dEy/dx, dEx/dy
           if (AX && hz_ok) f0 = psi1_apply<Exact, 2>(p.ht[4], sm.cc[4], qc2, k, jc, ih, res, f0, false);
           if (AY && hz_ok) f1 = psi1_apply<Exact, 1>(p.ht[5], sm.cc[5], qc3, k, jc, ih, res, f1, false);
           sm.hn[1][rr][3] = hyv;
@@ -875,7 +925,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
               const int t = second ? 3 : 2;
               const float psi = xstage ? sm.xps[hs][t][r * T::XW + slot - sm.xwin[t]] : d.psi_in[off];
               float nv;
-              const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, D1(dv), &nv);
+              const float dp = cpml_d<Exact>(sm.cc[second ? 10 : 9][slot], res, psi, ME(dv, 2, i0 + xo), &nv);
               if (st) d.psi_out[off] = nv;
               sm.xd[second ? 1 : 0][warp][slot] = dp;
             }
@@ -897,13 +947,13 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           hzy = wy0 ? make_float4(0.f, 0.f, 0.f, 0.f) : hz;
           hxy = wy0 ? make_float4(0.f, 0.f, 0.f, 0.f) : hx;
         }
-        float4 fx0 = D4(sub4(hz, hzy)), fx1 = D4(sub4(hy, hyp));              // Ex: dHz/dy, dHy/dz
-        float4 fy0 = D4(sub4(hx, hxp)), fy1 = D4(sub4(hz, prev4(hzl, hz)));   // Ey: dHx/dz, dHz/dx
-        float4 fz0 = D4(sub4(hy, prev4(hyl, hy))), fz1 = D4(sub4(hx, hxy));   // Ez: dHy/dx, dHx/dy
+        float4 fx0 = ME4(sub4(hz, hzy), 1, j), fx1 = ME4(sub4(hy, hyp), 0, k);        // Ex: dHz/dy, dHy/dz
+        float4 fy0 = ME4(sub4(hx, hxp), 0, k), fy1 = ME4x(sub4(hz, prev4(hzl, hz)), i);  // Ey: dHx/dz, dHz/dx
+        float4 fz0 = ME4x(sub4(hy, prev4(hyl, hy)), i), fz1 = ME4(sub4(hx, hxy), 1, j);  // Ez: dHy/dx, dHx/dy
         if (rowY) {  // ghost beyond y = Y: zero on a metallic wall, else the edge value
           const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-          fx0 = D4(wy1 ? sub4(z4, hzy) : z4);
-          fz1 = D4(wy1 ? sub4(z4, hxy) : z4);
+          fx0 = ME4(wy1 ? sub4(z4, hzy) : z4, 1, j);
+          fz1 = ME4(wy1 ? sub4(z4, hxy) : z4, 1, j);
         }
         if (AY) {
           fx0 = psi4_apply<Exact, 1>(p.et[0], sm.cc[6], slot_of(p.et[0], j), qe0, k, j, i, res, fx0, st, nvv);
@@ -987,7 +1037,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
         const bool zZ = k < Z, yY = jj >= 0 && jj < Y, yY1 = jj >= 0 && jj <= Y;
         const bool iX = ii >= 0 && ii < X, iX1 = ii >= 0 && ii <= X;
         if ((which & 1) && zZ && yY && iX1) {  // Hx: dEz/dy - dEy/dz
-          float d0 = D1(E0z[b + BX] - E0z[b]), d1 = D1(E1y[b] - E0y[b]);
+          float d0 = MH(E0z[b + BX] - E0z[b], 1, jj), d1 = MH(E1y[b] - E0y[b], 0, k);
           if (cpml) {
             d0 = cpml1<Exact, 1>(p.ht[0], sm.cc[0], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 0>(p.ht[1], sm.cc[1], cc_smem, res, k, jj, ii, d1, own);
@@ -1000,7 +1050,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if (own) p.hout[0][o] = h;
         }
         if ((which & 2) && zZ && yY1 && iX) {  // Hy: dEx/dz - dEz/dx
-          float d0 = D1(E1x[b] - E0x[b]), d1 = D1(E0z[b + 1] - E0z[b]);
+          float d0 = MH(E1x[b] - E0x[b], 0, k), d1 = MH(E0z[b + 1] - E0z[b], 2, ii);
           if (cpml) {
             d0 = cpml1<Exact, 0>(p.ht[2], sm.cc[2], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 2>(p.ht[3], sm.cc[3], cc_smem, res, k, jj, ii, d1, own);
@@ -1013,7 +1063,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           if (own) p.hout[1][o] = h;
         }
         if ((which & 4) && yY && iX) {  // Hz: dEy/dx - dEx/dy
-          float d0 = D1(E0y[b + 1] - E0y[b]), d1 = D1(E0x[b + BX] - E0x[b]);
+          float d0 = MH(E0y[b + 1] - E0y[b], 2, ii), d1 = MH(E0x[b + BX] - E0x[b], 1, jj);
           if (cpml) {
             d0 = cpml1<Exact, 2>(p.ht[4], sm.cc[4], cc_smem, res, k, jj, ii, d0, own);
             d1 = cpml1<Exact, 1>(p.ht[5], sm.cc[5], cc_smem, res, k, jj, ii, d1, own);
@@ -1045,7 +1095,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           return e_upd<Exact>(e, n == 0 ? t.x : (n == 1 ? t.y : t.z), d0, d1);
         };
         if (ii < X) {  // Ex: dHz/dy - dHy/dz
-          float d0 = D1(ghost_diff(hz, hz_y, jj, Y, wy0, wy1)), d1 = D1(ghost_diff(hy, hyz, k, Z, wz0, wz1));
+          float d0 = ME(ghost_diff(hz, hz_y, jj, Y, wy0, wy1), 1, jj), d1 = ME(ghost_diff(hy, hyz, k, Z, wz0, wz1), 0, k);
           if (cpml) {
             d0 = cpml1<Exact, 1>(p.et[0], sm.cc[6], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 0>(p.et[1], sm.cc[7], cc_smem, res, k, jj, ii, d1, true);
@@ -1055,7 +1105,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           p.eout[0][o] = e;
         }
         if (jj < Y) {  // Ey: dHx/dz - dHz/dx
-          float d0 = D1(ghost_diff(hx, hxz, k, Z, wz0, wz1)), d1 = D1(ghost_diff(hz, hz_x, ii, X, wx0, wx1));
+          float d0 = ME(ghost_diff(hx, hxz, k, Z, wz0, wz1), 0, k), d1 = ME(ghost_diff(hz, hz_x, ii, X, wx0, wx1), 2, ii);
           if (cpml) {
             d0 = cpml1<Exact, 0>(p.et[2], sm.cc[8], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 2>(p.et[3], sm.cc[9], cc_smem, res, k, jj, ii, d1, true);
@@ -1065,7 +1115,7 @@ __global__ void __launch_bounds__(32 * NW, NW == 8 ? 2 : 4)
           p.eout[1][o] = e;
         }
         if (k < Z) {  // Ez: dHy/dx - dHx/dy
-          float d0 = D1(ghost_diff(hy, hy_x, ii, X, wx0, wx1)), d1 = D1(ghost_diff(hx, hx_y, jj, Y, wy0, wy1));
+          float d0 = ME(ghost_diff(hy, hy_x, ii, X, wx0, wx1), 2, ii), d1 = ME(ghost_diff(hx, hx_y, jj, Y, wy0, wy1), 1, jj);
           if (cpml) {
             d0 = cpml1<Exact, 2>(p.et[4], sm.cc[10], cc_smem, res, k, jj, ii, d0, true);
             d1 = cpml1<Exact, 1>(p.et[5], sm.cc[11], cc_smem, res, k, jj, ii, d1, true);
@@ -1138,7 +1188,7 @@ __device__ __forceinline__ float col_psi(const CpmlTermDev& t, int k, int j, int
   return slot >= 0 ? t.psi_in[psi_off<Axis>(t, slot, k, j, x)] : 0.0f;
 }
 
-template <bool Cpml, bool Exact, bool Lossy>
+template <bool Cpml, bool Exact, bool Lossy, bool Metric>
 __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __grid_constant__ Step3D p) {
   __shared__ float hx[kColK + 1][kColJ + 1];  // new Hx at (k0 - 1 + a, j0 - 1 + b, X)
   __shared__ float amp[kMaxFusedSources];
@@ -1152,6 +1202,16 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
   const bool wy0 = wall(p.metallic, 1, false), wy1 = wall(p.metallic, 1, true);
   const bool wx0 = wall(p.metallic, 2, false), wx1 = wall(p.metallic, 2, true);
   auto D1 = [&](float v) { return dv<Exact>(v, dbs, drs); };
+  // Forward (H) and backward (E) derivatives along an axis at a coordinate:
+  // the difference times the metric's inverse distance there, or D1.
+  auto MH = [&](float v, int axis, int c) -> float {
+    if constexpr (Metric) return v * p.metric_h[axis][clampi(c, axis_cells(p, axis) - 1)];
+    else return D1(v);
+  };
+  auto ME = [&](float v, int axis, int c) -> float {
+    if constexpr (Metric) return v * p.metric_e[axis][clampi(c, axis_cells(p, axis))];
+    else return D1(v);
+  };
   // This thread's E cell (k, j, X): its inputs are loaded first.
   const int k = k0 + threadIdx.y, j = j0 + threadIdx.x;
   const bool live = k <= Z && j <= Y;
@@ -1192,8 +1252,8 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
         qy = col_psi<1>(p.ht[0], kk, jj, X);
         qz = col_psi<0>(p.ht[1], kk, jj, X);
       }
-      float d0 = D1(p.ein[2][oh + P] - p.ein[2][oh]);
-      float d1 = D1(p.ein[1][oh + PL] - p.ein[1][oh]);
+      float d0 = MH(p.ein[2][oh + P] - p.ein[2][oh], 1, jj);
+      float d1 = MH(p.ein[1][oh + PL] - p.ein[1][oh], 0, kk);
       if (Cpml) {
         d0 = col_cpml<Exact, 1>(p.ht[0], res, inv_res, qy, kk, jj, X, d0, own);
         d1 = col_cpml<Exact, 0>(p.ht[1], res, inv_res, qz, kk, jj, X, d1, own);
@@ -1215,7 +1275,7 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
   if (wx1) {
     const int ow = o - 1;
     if (ey_ok) {  // Hz(k, j, X - 1): dEy/dx - dEx/dy
-      float d0 = D1(p.ein[1][ow + 1] - p.ein[1][ow]), d1 = D1(p.ein[0][ow + P] - p.ein[0][ow]);
+      float d0 = MH(p.ein[1][ow + 1] - p.ein[1][ow], 2, X - 1), d1 = MH(p.ein[0][ow + P] - p.ein[0][ow], 1, j);
       if (Cpml) {
         d0 = col_cpml<Exact, 2>(p.ht[4], res, inv_res, col_psi<2>(p.ht[4], k, j, X - 1), k, j, X - 1, d0, false);
         d1 = col_cpml<Exact, 1>(p.ht[5], res, inv_res, col_psi<1>(p.ht[5], k, j, X - 1), k, j, X - 1, d1, false);
@@ -1227,7 +1287,7 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
       if ((k == 0 && wz0) || (k == Z && wz1)) hz_w = 0.0f;
     }
     if (ez_ok) {  // Hy(k, j, X - 1): dEx/dz - dEz/dx
-      float d0 = D1(p.ein[0][ow + PL] - p.ein[0][ow]), d1 = D1(p.ein[2][ow + 1] - p.ein[2][ow]);
+      float d0 = MH(p.ein[0][ow + PL] - p.ein[0][ow], 0, k), d1 = MH(p.ein[2][ow + 1] - p.ein[2][ow], 2, X - 1);
       if (Cpml) {
         d0 = col_cpml<Exact, 0>(p.ht[2], res, inv_res, col_psi<0>(p.ht[2], k, j, X - 1), k, j, X - 1, d0, false);
         d1 = col_cpml<Exact, 2>(p.ht[3], res, inv_res, col_psi<2>(p.ht[3], k, j, X - 1), k, j, X - 1, d1, false);
@@ -1240,8 +1300,8 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
     }
   }
   if (ey_ok) {  // Ey: dHx/dz - dHz/dx, the Hz ghost beyond x = X
-    float d0 = D1(ghost_diff(hx[a][b], hx[a - 1][b], k, Z, wz0, wz1));
-    float d1 = D1(ghost_diff(0.0f, hz_w, X, X, wx0, wx1));
+    float d0 = ME(ghost_diff(hx[a][b], hx[a - 1][b], k, Z, wz0, wz1), 0, k);
+    float d1 = ME(ghost_diff(0.0f, hz_w, X, X, wx0, wx1), 2, X);
     if (Cpml) {
       d0 = col_cpml<Exact, 0>(p.et[2], res, inv_res, q_eyz, k, j, X, d0, true);
       d1 = col_cpml<Exact, 2>(p.et[3], res, inv_res, q_eyx, k, j, X, d1, true);
@@ -1251,8 +1311,8 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
     p.eout[1][o] = e;
   }
   if (ez_ok) {  // Ez: dHy/dx - dHx/dy, the Hy ghost beyond x = X
-    float d0 = D1(ghost_diff(0.0f, hy_w, X, X, wx0, wx1));
-    float d1 = D1(ghost_diff(hx[a][b], hx[a][b - 1], j, Y, wy0, wy1));
+    float d0 = ME(ghost_diff(0.0f, hy_w, X, X, wx0, wx1), 2, X);
+    float d1 = ME(ghost_diff(hx[a][b], hx[a][b - 1], j, Y, wy0, wy1), 1, j);
     if (Cpml) {
       d0 = col_cpml<Exact, 2>(p.et[4], res, inv_res, q_ezx, k, j, X, d0, true);
       d1 = col_cpml<Exact, 1>(p.et[5], res, inv_res, q_ezy, k, j, X, d1, true);
@@ -1263,20 +1323,20 @@ __global__ void __launch_bounds__(kColJ * kColK) class_column_kernel(const __gri
   }
 }
 
-template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial, bool Metric>
 cudaError_t launch_class_p(cudaStream_t s, const ClassMaps& maps, const Step3D& p);
 
-template <int NW, bool Cpml, bool Exact, bool Lossy = false>
+template <int NW, bool Cpml, bool Exact, bool Lossy = false, bool Metric = false>
 cudaError_t launch_class_t(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
-  if (p.X % ClassTile<NW, Lossy>::TX != 0) return launch_class_p<NW, Cpml, Exact, Lossy, true>(s, maps, p);
-  return launch_class_p<NW, Cpml, Exact, Lossy, false>(s, maps, p);
+  if (p.X % ClassTile<NW, Lossy>::TX != 0) return launch_class_p<NW, Cpml, Exact, Lossy, true, Metric>(s, maps, p);
+  return launch_class_p<NW, Cpml, Exact, Lossy, false, Metric>(s, maps, p);
 }
 
-template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial>
+template <int NW, bool Cpml, bool Exact, bool Lossy, bool Partial, bool Metric>
 cudaError_t launch_class_p(cudaStream_t s, const ClassMaps& maps, const Step3D& p) {
   using T = ClassTile<NW, Lossy>;
   const size_t smem = sizeof(typename T::Smem);
-  auto kern = class_step_kernel<NW, Cpml, Exact, Lossy, Partial>;
+  auto kern = class_step_kernel<NW, Cpml, Exact, Lossy, Partial, Metric>;
   int device = 0;
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess) return err;
@@ -1313,7 +1373,7 @@ cudaError_t launch_class_p(cudaStream_t s, const ClassMaps& maps, const Step3D& 
   if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   {  // column X first: it reads only the step's inputs
     const dim3 cgrid((p.Y + 1 + kColJ - 1) / kColJ, (p.Z + 1 + kColK - 1) / kColK, 1);
-    class_column_kernel<Cpml, Exact, Lossy><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
+    class_column_kernel<Cpml, Exact, Lossy, Metric><<<cgrid, dim3(kColJ, kColK, 1), 0, s>>>(q);
     err = cudaPeekAtLastError();
     if (err != cudaSuccess) return err;
   }
@@ -1362,6 +1422,13 @@ cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
     }
     q.xstage = ok ? 1 : 0;
   }
+  if constexpr (NW == 8) {
+    // Derivative metrics (axis-uniform / rectilinear grids): exact arithmetic
+    // on lossless classes only (validated), 128 x 8 tiles.
+    if (has_metric(q))
+      return q.cpml ? launch_class_t<8, true, true, false, true>(s, maps, q)
+                    : launch_class_t<8, false, true, false, true>(s, maps, q);
+  }
   if (q.lossy)  // exact arithmetic only (validated)
     return q.cpml ? launch_class_t<NW, true, true, true>(s, maps, q) : launch_class_t<NW, false, true, true>(s, maps, q);
   if (q.fast_math) return q.cpml ? launch_class_t<NW, true, false>(s, maps, q) : launch_class_t<NW, false, false>(s, maps, q);
@@ -1370,9 +1437,10 @@ cudaError_t launch_class_shape(cudaStream_t s, const Step3D& p) {
 
 }  // namespace
 
-// tile_y: 8 (8 warps, 128 x 8 tiles) or 4 (4 warps, 128 x 4 tiles).
+// tile_y: 8 (8 warps, 128 x 8 tiles) or 4 (4 warps, 128 x 4 tiles; programs
+// with derivative metrics always take 8).
 cudaError_t launch_class_step(cudaStream_t s, const Step3D& p, int tile_y) {
-  return tile_y == 4 ? launch_class_shape<4>(s, p) : launch_class_shape<8>(s, p);
+  return tile_y == 4 && !has_metric(p) ? launch_class_shape<4>(s, p) : launch_class_shape<8>(s, p);
 }
 
 }  // namespace fdtd

@@ -132,7 +132,10 @@ int validate(const FdtdProgram& p) {
     }
   }
   if (has_metric(p)) {
-    if (pitched) return kInvalid;
+    // On the pitched layout, only the class step carries metrics, in exact
+    // arithmetic on lossless classes.
+    if (pitched && (!(p.flags & FDTD_FLAG_CLASSES) || (p.flags & (FDTD_FLAG_FAST_MATH | FDTD_FLAG_LOSSY))))
+      return kInvalid;
     for (int a = 0; a < 3; ++a) {
       const int n = a == 0 ? L.Z : (a == 1 ? L.Y : L.X);
       const FdtdBuffer &mh = p.metric_h[a], &me = p.metric_e[a];

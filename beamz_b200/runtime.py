@@ -444,14 +444,19 @@ class DeviceProgram:
         dev = self.device
         h_uniform = all(np.ndim(d) == 0 and np.ndim(s_) == 0 for d, s_ in spec.h_coefficients().values())
         site_sources = lossless_site_sources(spec)
+        # Derivative metrics (axis-uniform / rectilinear grids) ride on the
+        # class step in exact arithmetic; the codebook step has none.
+        layout_arg = layout
+        metric_ok = spec.metrics is None or (step_kernel == "classes" and arithmetic == "exact")
         pitched_ok = (spec.ndim == 3 and (spec.voxel_ids is not None or site_sources is not None)
-                      and schedule == "fused" and h_uniform and spec.metrics is None)
+                      and schedule == "fused" and h_uniform and metric_ok)
         lossy_ok = (spec.ndim == 3 and spec.voxel_ids is None and site_sources is None and spec.e_site is not None
                     and all(c in spec.e_site for c in ("Ex", "Ey", "Ez")) and schedule == "fused"
                     and spec.metrics is None and step_kernel == "classes" and arithmetic == "exact")
         if layout == "pitched" and not (pitched_ok or lossy_ok):
-            raise ValueError("the pitched layout needs a 3D voxel or per-site program, the fused schedule, an "
-                             "isotropic grid and (with conductive material) the class step in exact arithmetic")
+            raise ValueError("the pitched layout needs a 3D voxel or per-site program and the fused schedule; "
+                             "conductive material or a non-isotropic grid also need the class step in exact "
+                             "arithmetic")
         f32 = np.float32
         dt_over_eps = f32(spec.dt) / f32(EPS_0)
         self.site_ids = self.site_coef = self.site_eps_table = None
@@ -521,7 +526,13 @@ class DeviceProgram:
                     self.site_ids, self.site_coef, float(spec.resolution), int(spec.grid_shape[2]),
                     over_dx=arithmetic == "fast")
             except ClassOverflow:
-                step_kernel = "codebook"
+                if spec.metrics is not None:  # the codebook step carries no metrics: the dense step
+                    if layout_arg == "pitched":
+                        raise
+                    layout = self.layout = "dense"
+                    self.site_ids = self.site_coef = self.site_eps_table = None
+                else:
+                    step_kernel = "codebook"
         if layout != "pitched":
             step_kernel = "dense"
         if step_kernel != "classes":

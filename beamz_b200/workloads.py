@@ -98,6 +98,23 @@ def conductive(spec: P.ProgramSpec, sigma_by_id=(0.0, 4e4)) -> P.ProgramSpec:
     return dataclasses.replace(spec, voxel_ids=None, eps_table=None, e_site=e_site, h_site=h_site, e_site_eps=e_eps)
 
 
+def graded(spec: P.ProgramSpec, kind: str = "rectilinear", seed: int = 0, spread=(1.0, 1.25)) -> P.ProgramSpec:
+    """The same scene on an axis-uniform or rectilinear grid: seeded cell
+    widths within ``spread`` x the cell size on every axis (never below it, so
+    the scene's time step stays stable), lowered to beamz's per-axis inverse
+    distances (:func:`plan.derivative_metrics`, kernels.py:164-176)."""
+    import dataclasses
+
+    rng = np.random.default_rng(seed)
+    widths = {}
+    for a, n in zip(("z", "y", "x"), spec.grid_shape):
+        if kind == "axis_uniform":
+            widths[a] = np.full(int(n), spec.resolution * rng.uniform(*spread))
+        else:
+            widths[a] = spec.resolution * rng.uniform(*spread, int(n))
+    return dataclasses.replace(spec, metrics=P.derivative_metrics(widths, kind))
+
+
 def scene_capacity(total_steps=500, seed=0, shape=(1024, 1024, 1536), pml_cells=12, monitors=False):
     nz, ny, nx = shape
     rng = np.random.default_rng(seed)

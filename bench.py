@@ -49,6 +49,8 @@ def parse():
                     help="3d_512 only: the faces that carry the absorber (the absorber's cost per axis)")
     ap.add_argument("--material", choices=["dielectric", "conductive"], default="dielectric",
                     help="3d_512 only: conductive Si boxes (sigma 4e4 S/m: per-site E and H decay)")
+    ap.add_argument("--grid", choices=["uniform", "axis_uniform", "rectilinear"], default="uniform",
+                    help="3d_512 only: seeded cell widths of 1-1.25 x 20 nm per axis (derivative metrics)")
     ap.add_argument("--step-kernel", choices=["classes", "codebook"], default=None,
                     help="pitched 3D step (default: the runtime's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,7 +64,10 @@ def parse():
     ap.add_argument("--accuracy", choices=["reduced", "full"], default="reduced",
                     help="accuracy key: a reduced copy of the scene against the FP32 and FP64 oracles (default), "
                          "or the full 512x512x256 scene over all 1000 steps against the C restatement (minutes)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.grid != "uniform" and args.scene != "3d_512":
+        ap.error("--grid applies to the 3d_512 scene")
+    return args
 
 
 def peaks():
@@ -149,7 +154,9 @@ def cpu_sample(spec_fn, total_steps, budget_s, threads=0):
 
 def config_block(args, spec) -> dict:
     """The workload description both arms print (the driver compares them)."""
-    scene = {"3d_512": "3d_512x512x256_cpml12_sibox_dipole_dft4x5" + ("_conductive" if getattr(args, "material", "") == "conductive" else ""),
+    suffix = ("_conductive" if getattr(args, "material", "") == "conductive" else "") + (
+        "_" + args.grid if getattr(args, "grid", "uniform") != "uniform" else "")
+    scene = {"3d_512": "3d_512x512x256_cpml12_sibox_dipole_dft4x5" + suffix,
              "capacity": "capacity_1536x1024x1024_cpml12",
              "2d_400": "2d_400x400_tm_cpml20_strip_dft3"}[args.scene]
     return {"workload": scene, "grid_zyx": [int(v) for v in spec.grid_shape], "cells": int(spec.cells),
@@ -435,6 +442,8 @@ def main():
     spec = scene_fn(total_steps=total, **shape_kw)
     if args.material == "conductive":
         spec = W.conductive(spec)
+    if args.grid != "uniform":
+        spec = W.graded(spec, args.grid)
     sk = {"step_kernel": args.step_kernel} if args.step_kernel else {}
     prog = R.compile_program(spec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
     state = R.initial_state(prog)
@@ -483,6 +492,8 @@ def main():
         kspec = scene_fn(total_steps=3 * args.kernel_steps + 3, monitors=False, sources=False, **shape_kw)
         if args.material == "conductive":
             kspec = W.conductive(kspec)
+        if args.grid != "uniform":
+            kspec = W.graded(kspec, args.grid)
         kprog = R.compile_program(kspec, device=dev, schedule="fused", tile=tile, z_chunk=args.z_chunk, **sk)
         kstate = R.initial_state(kprog)
     else:  # other scenes time their own step (a second copy of the 1.6 G-cell scene would not fit)
@@ -507,7 +518,7 @@ def main():
     kname = {"classes": "class_step", "codebook": "tma_step"}.get(prog.step_kernel, "fused_step")
     prof = os.path.join(ROOT, "profiles", f"{kname}_{args.scene}.json")
     if os.path.exists(prof) and not args.shape and tile == (32, 8) and args.z_chunk == 16 and args.cpml_faces == "all" \
-            and args.material == "dielectric":
+            and args.material == "dielectric" and args.grid == "uniform":
         with open(prof) as fh:
             traffic = json.load(fh).get("dram_bytes_per_launch")
 

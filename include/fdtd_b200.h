@@ -282,7 +282,9 @@ typedef struct FdtdProgram {
    * the inverse distances that multiply the forward differences of the H
    * update at each H coordinate; metric_e[a] is F32 [n_a + 1], those of the
    * backward differences of the E update at each E coordinate (an axis-uniform
-   * grid repeats one value).  FDTD_LAYOUT_DENSE only; no adjoint. */
+   * grid repeats one value).  FDTD_LAYOUT_DENSE, or FDTD_LAYOUT_PITCHED with
+   * FDTD_FLAG_CLASSES and neither FDTD_FLAG_FAST_MATH nor FDTD_FLAG_LOSSY (the
+   * class step, 128 x 8 tiles whatever tile_y asks); no adjoint. */
   FdtdBuffer metric_h[3];
   FdtdBuffer metric_e[3];
   /* Field recorders, run after each step's DFT sample (see FdtdRecorder). */

@@ -1,7 +1,7 @@
-"""Axis-uniform and rectilinear grids on the device: the dense step kernels
-(both schedules, 3D voxel and conductive per-site material, 2D TM/TE) bit for
-bit against the oracle's metric form (pinned to beamz's metric updates in
-tests/test_metric.py)."""
+"""Axis-uniform and rectilinear grids on the device: the class step (3D voxel
+programs, fused schedule) and the dense step kernels (phases, conductive
+per-site material, 2D TM/TE) bit for bit against the oracle's metric form
+(pinned to beamz's metric updates in tests/test_metric.py)."""
 
 from __future__ import annotations
 
@@ -36,7 +36,7 @@ def test_metric_3d_step_matches_the_oracle_bit_for_bit(schedule, kind):
     spec = with_metrics(base, kind, seed=1)
     fields = random_initial_fields(spec, seed=4)
     prog = R.compile_program(spec, schedule=schedule)
-    assert prog.layout == "dense"
+    assert prog.layout == ("pitched" if schedule == "fused" else "dense")
     out = R.run_steps(R.initial_state(prog, fields=fields), prog, 10).numpy()
     st = O.run(oracle_state(to_oracle(spec), fields), to_oracle(spec), 10)
     _assert_bitwise(out, st, P.COMPONENTS)
@@ -73,8 +73,39 @@ def test_metric_2d_step_matches_the_oracle_bit_for_bit(pol, schedule):
     _assert_bitwise(out, st, P.active_components(2, pol))
 
 
-def test_metric_programs_take_the_dense_layout():
+METRIC_CASES = [
+    dict(grid=(10, 13, 128), metallic=("back", "top"), kind="rectilinear"),       # one full tile
+    dict(grid=(9, 20, 150), metallic=("right", "bottom"), kind="rectilinear"),    # a partial last tile, PEC on x = X
+    dict(grid=(28, 30, 140), metallic=("left", "front"), kind="axis_uniform", pml_cells=12),  # staged x psi
+]
+
+
+@pytest.mark.parametrize("tile_y", [8, 4])
+@pytest.mark.parametrize("case", range(len(METRIC_CASES)))
+def test_metric_class_step_matches_the_oracle_bit_for_bit(case, tile_y):
+    """The class step with per-axis inverse distances: fields and CPML
+    memories bit for bit over two chunked calls, the DFT arena within 1e-4."""
+    kw = dict(METRIC_CASES[case])
+    kind = kw.pop("kind")
+    spec = with_metrics(scenario_3d(seed=case + 3, nsteps=14, **kw), kind, seed=case + 1)
+    fields = random_initial_fields(spec, seed=case + 7)
+    prog = R.compile_program(spec, tile=(128, tile_y))
+    assert prog.layout == "pitched" and prog.step_kernel == "classes"
+    st = R.initial_state(prog, fields=fields)
+    R.run_steps(st, prog, 9)
+    out = R.run_steps(st, prog, 5).numpy()
+    ost = O.run(oracle_state(to_oracle(spec), fields), to_oracle(spec), 14)
+    _assert_bitwise(out, ost, P.COMPONENTS)
+
+
+def test_metric_programs_layouts():
+    """Metric programs take the class step; the tolerance arithmetic and the
+    codebook step carry no metrics, so those go to the dense step (and refuse
+    the pitched layout when it is asked for)."""
     spec = with_metrics(scenario_3d(grid=(8, 9, 10), seed=1, nsteps=2))
-    assert R.compile_program(spec).layout == "dense"
-    with pytest.raises(ValueError, match="isotropic"):
-        R.compile_program(spec, layout="pitched")
+    prog = R.compile_program(spec)
+    assert prog.layout == "pitched" and prog.step_kernel == "classes"
+    assert R.compile_program(spec, arithmetic="fast").layout == "dense"
+    assert R.compile_program(spec, step_kernel="codebook").layout == "dense"
+    with pytest.raises(ValueError, match="non-isotropic"):
+        R.compile_program(spec, layout="pitched", step_kernel="codebook")
