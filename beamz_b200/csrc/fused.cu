@@ -55,13 +55,25 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Planes that hold any active component of the given range (E: 0-2, H:
+// 3-5): the 2D TM embedding (Z = 1) keeps Ez, Hx and Hy on plane 0 only, so
+// its plane 1 holds nothing to stage or update.
+template <int Active>
+__device__ __forceinline__ int active_planes(const Step3D& p, int first, int last) {
+  int n = 0;
+#pragma unroll
+  for (int c = first; c <= last; ++c)
+    if ((Active >> c) & 1) n = max(n, component_dims(c, p.Z, p.Y, p.X).z);
+  return n;
+}
+
 // Issue the copies of E plane q (all three components) into its ring slot.
 template <int TX, int TY, int Active>
 __device__ __forceinline__ void issue_e_plane(FusedSmem<TX, TY>& sm, const Step3D& p, int q, int j0, int i0,
                                               int tid) {
   using S = FusedSmem<TX, TY>;
   constexpr int NT = TX * TY;
-  if (q > p.Z) return;  // beyond the last E plane: slot is never read
+  if (q >= active_planes<Active>(p, 0, 2)) return;  // beyond the last E plane: slot is never read
   const int slot = q % S::ES;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -82,7 +94,7 @@ __device__ __forceinline__ void issue_h_plane(FusedSmem<TX, TY>& sm, const Step3
                                               int tid) {
   using S = FusedSmem<TX, TY>;
   constexpr int NT = TX * TY;
-  if (q > p.Z) return;
+  if (q >= active_planes<Active>(p, 3, 5)) return;
   const int slot = q % S::HS;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -205,7 +217,7 @@ __global__ void __launch_bounds__(TX* TY) fused_step_kernel(Step3D p) {
   const int tid = threadIdx.y * TX + threadIdx.x;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int Z = p.Z, Y = p.Y, X = p.X;
-  const int kmax = Z + 1;  // planes holding any component
+  const int kmax = max(active_planes<Active>(p, 0, 2), active_planes<Active>(p, 3, 5));  // planes with an active component
   const int k0 = blockIdx.z * p.z_chunk;
   const int k1 = min(k0 + p.z_chunk, kmax);
   const int kstart = k0 > 0 ? k0 - 1 : 0;
