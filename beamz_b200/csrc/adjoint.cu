@@ -37,18 +37,24 @@ namespace {
 
 // Term tables (3D order: H 0 Hx-y, 1 Hx-z, 2 Hy-z, 3 Hy-x, 4 Hz-x, 5 Hz-y;
 // E likewise for Ex, Ey, Ez; even terms enter with +, odd with -).
-__constant__ int kAdjHSrc[6] = {2, 1, 0, 2, 1, 0};   // E component each H term differentiates
-__constant__ int kAdjHAxis[6] = {1, 0, 0, 2, 2, 1};
-__constant__ int kAdjESrc[6] = {5, 4, 3, 5, 4, 3};   // H component each E term differentiates
-__constant__ int kAdjEAxis[6] = {1, 0, 0, 2, 2, 1};
+// The kernels take their component as a template argument, so that these
+// lookups (and the term loops of the gathers) resolve at compile time.
+__host__ __device__ constexpr int adj_h_src(int t) { return 2 - t % 3; }  // E component an H term differentiates
+__host__ __device__ constexpr int adj_e_src(int t) { return 5 - t % 3; }  // H component an E term differentiates
+// Axis of term t's derivative, for H and E terms alike: 1, 0, 0, 2, 2, 1.
+__host__ __device__ constexpr int adj_axis(int t) { return (t == 0 || t == 5) ? 1 : ((t == 1 || t == 2) ? 0 : 2); }
 
 constexpr int kAdjThreads = 256;
 
+// Element offsets of a component fit 32 bits (every entry point validates
+// arrays below 2^31 elements), so the split is two 32-bit divisions rather
+// than 64-bit ones, which the GPU emulates in dozens of instructions.
 __device__ __forceinline__ void unflat(int64_t idx, const Dims& d, int& k, int& j, int& i) {
-  i = static_cast<int>(idx % d.x);
-  const int64_t r = idx / d.x;
-  j = static_cast<int>(r % d.y);
-  k = static_cast<int>(r / d.y);
+  const unsigned id = static_cast<unsigned>(idx), dx = static_cast<unsigned>(d.x), dy = static_cast<unsigned>(d.y);
+  const unsigned r = id / dx;
+  i = static_cast<int>(id - r * dx);
+  k = static_cast<int>(r / dy);
+  j = static_cast<int>(r - static_cast<unsigned>(k) * dy);
 }
 
 __device__ __forceinline__ int coord_of(int axis, int k, int j, int i) { return axis == 0 ? k : (axis == 1 ? j : i); }
@@ -73,7 +79,8 @@ __device__ __forceinline__ float coef_at(const float* p, int full, int64_t idx) 
 
 // 4a. E transpose, per E site of component c: mask, identity part, the two
 // terms' lam_d into scratch, and the design-box gradient.
-__global__ void __launch_bounds__(kAdjThreads) adj_e_kernel(Step3D p, AdjDev a, int c) {
+template <int c>
+__global__ void __launch_bounds__(kAdjThreads) adj_e_kernel(Step3D p, AdjDev a) {
   const Dims d = component_dims(c, p.Z, p.Y, p.X);
   const int64_t n = static_cast<int64_t>(d.z) * d.y * d.x;
   for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n;
@@ -84,11 +91,12 @@ __global__ void __launch_bounds__(kAdjThreads) adj_e_kernel(Step3D p, AdjDev a, 
     if (e_constrained(p.metallic, c, d, k, j, i)) mu = 0.0f;
     a.lam[c][idx] = coef_at(p.em.decay[c], p.em.decay_full[c], idx) * mu;
     const float src = coef_at(p.em.source[c], p.em.source_full[c], idx);
+#pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int t = 2 * c + s;
       if (a.scratch_e[t] == nullptr) continue;
       float ld = (s == 0 ? src : -src) * mu;
-      if (p.cpml) ld = cpml_transpose(p.et[t], kAdjEAxis[t], k, j, i, ld);
+      if (p.cpml) ld = cpml_transpose(p.et[t], adj_axis(t), k, j, i, ld);
       a.scratch_e[t][idx] = ld;
     }
     if (a.grad[c] != nullptr && k >= a.box_lo[0] && k < a.box_hi[0] && j >= a.box_lo[1] && j < a.box_hi[1] &&
@@ -102,7 +110,8 @@ __global__ void __launch_bounds__(kAdjThreads) adj_e_kernel(Step3D p, AdjDev a, 
 }
 
 // 4b. B^T gather, per H site of component h.
-__global__ void __launch_bounds__(kAdjThreads) adj_hgather_kernel(Step3D p, AdjDev a, int h) {
+template <int h>
+__global__ void __launch_bounds__(kAdjThreads) adj_hgather_kernel(Step3D p, AdjDev a) {
   const Dims d = component_dims(h, p.Z, p.Y, p.X);
   const int64_t n = static_cast<int64_t>(d.z) * d.y * d.x;
   const float inv_res = 1.0f / p.res;
@@ -111,9 +120,10 @@ __global__ void __launch_bounds__(kAdjThreads) adj_hgather_kernel(Step3D p, AdjD
     int k, j, i;
     unflat(idx, d, k, j, i);
     float acc = 0.0f;
+#pragma unroll
     for (int t = 0; t < 6; ++t) {
-      if (kAdjESrc[t] != h || a.scratch_e[t] == nullptr) continue;
-      const int e = t / 2, axis = kAdjEAxis[t];
+      if (adj_e_src(t) != h || a.scratch_e[t] == nullptr) continue;
+      const int e = t / 2, axis = adj_axis(t);
       const Dims de = component_dims(e, p.Z, p.Y, p.X);
       const int N = axis == 0 ? d.z : (axis == 1 ? d.y : d.x);  // H samples; E has N + 1
       const int m = coord_of(axis, k, j, i);
@@ -129,7 +139,8 @@ __global__ void __launch_bounds__(kAdjThreads) adj_hgather_kernel(Step3D p, AdjD
 }
 
 // 3a. H transpose, per H site of component h.
-__global__ void __launch_bounds__(kAdjThreads) adj_h_kernel(Step3D p, AdjDev a, int h) {
+template <int h>
+__global__ void __launch_bounds__(kAdjThreads) adj_h_kernel(Step3D p, AdjDev a) {
   const Dims d = component_dims(h, p.Z, p.Y, p.X);
   const int64_t n = static_cast<int64_t>(d.z) * d.y * d.x;
   const int hc = h - 3;
@@ -141,18 +152,20 @@ __global__ void __launch_bounds__(kAdjThreads) adj_h_kernel(Step3D p, AdjDev a, 
     if (h_constrained(p.metallic, h, d, k, j, i)) mu = 0.0f;
     a.lam[h][idx] = coef_at(p.hm.decay[hc], p.hm.decay_full[hc], idx) * mu;
     const float src = coef_at(p.hm.source[hc], p.hm.source_full[hc], idx);
+#pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int t = 2 * hc + s;
       if (a.scratch_h[t] == nullptr) continue;
       float ld = (s == 0 ? -src : src) * mu;
-      if (p.cpml) ld = cpml_transpose(p.ht[t], kAdjHAxis[t], k, j, i, ld);
+      if (p.cpml) ld = cpml_transpose(p.ht[t], adj_axis(t), k, j, i, ld);
       a.scratch_h[t][idx] = ld;
     }
   }
 }
 
 // 3b. D^T gather, per E site of component e.
-__global__ void __launch_bounds__(kAdjThreads) adj_egather_kernel(Step3D p, AdjDev a, int e) {
+template <int e>
+__global__ void __launch_bounds__(kAdjThreads) adj_egather_kernel(Step3D p, AdjDev a) {
   const Dims d = component_dims(e, p.Z, p.Y, p.X);
   const int64_t n = static_cast<int64_t>(d.z) * d.y * d.x;
   const float inv_res = 1.0f / p.res;
@@ -161,9 +174,10 @@ __global__ void __launch_bounds__(kAdjThreads) adj_egather_kernel(Step3D p, AdjD
     int k, j, i;
     unflat(idx, d, k, j, i);
     float acc = 0.0f;
+#pragma unroll
     for (int t = 0; t < 6; ++t) {
-      if (kAdjHSrc[t] != e || a.scratch_h[t] == nullptr) continue;
-      const int hcomp = 3 + t / 2, axis = kAdjHAxis[t];
+      if (adj_h_src(t) != e || a.scratch_h[t] == nullptr) continue;
+      const int hcomp = 3 + t / 2, axis = adj_axis(t);
       const Dims dh = component_dims(hcomp, p.Z, p.Y, p.X);
       const int N = axis == 0 ? dh.z : (axis == 1 ? dh.y : dh.x);
       const int m = coord_of(axis, k, j, i);
@@ -284,26 +298,24 @@ cudaError_t launch_adjoint_step(cudaStream_t s, const Step3D& p, const DftDev* d
     const dim3 grid((dft->max_points + kAdjThreads - 1) / kAdjThreads, dft->monitor_count * 6, 1);
     adj_dft_kernel<<<grid, kAdjThreads, 0, s>>>(*dft, a, step);
   }
-  for (int c = 0; c < 3; ++c) {
-    if (!((active >> c) & 1)) continue;
+  // One launch per active component and pass, in the component order of the
+  // transpose (E sites, B^T gathers, H sites, D^T gathers).
+  auto grid = [&](int c) {
     const Dims d = component_dims(c, p.Z, p.Y, p.X);
-    adj_e_kernel<<<blocks_for(static_cast<int64_t>(d.z) * d.y * d.x), kAdjThreads, 0, s>>>(p, a, c);
-  }
-  for (int h = 3; h < 6; ++h) {
-    if (!((active >> h) & 1)) continue;
-    const Dims d = component_dims(h, p.Z, p.Y, p.X);
-    adj_hgather_kernel<<<blocks_for(static_cast<int64_t>(d.z) * d.y * d.x), kAdjThreads, 0, s>>>(p, a, h);
-  }
-  for (int h = 3; h < 6; ++h) {
-    if (!((active >> h) & 1)) continue;
-    const Dims d = component_dims(h, p.Z, p.Y, p.X);
-    adj_h_kernel<<<blocks_for(static_cast<int64_t>(d.z) * d.y * d.x), kAdjThreads, 0, s>>>(p, a, h);
-  }
-  for (int e = 0; e < 3; ++e) {
-    if (!((active >> e) & 1)) continue;
-    const Dims d = component_dims(e, p.Z, p.Y, p.X);
-    adj_egather_kernel<<<blocks_for(static_cast<int64_t>(d.z) * d.y * d.x), kAdjThreads, 0, s>>>(p, a, e);
-  }
+    return blocks_for(static_cast<int64_t>(d.z) * d.y * d.x);
+  };
+  if (active & 1) adj_e_kernel<0><<<grid(0), kAdjThreads, 0, s>>>(p, a);
+  if (active & 2) adj_e_kernel<1><<<grid(1), kAdjThreads, 0, s>>>(p, a);
+  if (active & 4) adj_e_kernel<2><<<grid(2), kAdjThreads, 0, s>>>(p, a);
+  if (active & 8) adj_hgather_kernel<3><<<grid(3), kAdjThreads, 0, s>>>(p, a);
+  if (active & 16) adj_hgather_kernel<4><<<grid(4), kAdjThreads, 0, s>>>(p, a);
+  if (active & 32) adj_hgather_kernel<5><<<grid(5), kAdjThreads, 0, s>>>(p, a);
+  if (active & 8) adj_h_kernel<3><<<grid(3), kAdjThreads, 0, s>>>(p, a);
+  if (active & 16) adj_h_kernel<4><<<grid(4), kAdjThreads, 0, s>>>(p, a);
+  if (active & 32) adj_h_kernel<5><<<grid(5), kAdjThreads, 0, s>>>(p, a);
+  if (active & 1) adj_egather_kernel<0><<<grid(0), kAdjThreads, 0, s>>>(p, a);
+  if (active & 2) adj_egather_kernel<1><<<grid(1), kAdjThreads, 0, s>>>(p, a);
+  if (active & 4) adj_egather_kernel<2><<<grid(2), kAdjThreads, 0, s>>>(p, a);
   return cudaPeekAtLastError();
 }
 
