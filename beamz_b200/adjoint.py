@@ -1,16 +1,19 @@
 """Adjoint (time-reversed) FDTD and permittivity gradients.
 
-:class:`AdjointProblem` runs one simulation forward with checkpoints every
-``checkpoint_every`` steps and back-propagates gradients of any function of
-its DFT arena to the per-site E update coefficients c = dt / (eps0 eps_site)
-inside a design box:
+:class:`AdjointProblem` runs one simulation forward and back-propagates
+gradients of any function of its DFT arena to the per-site E update
+coefficients c = dt / (eps0 eps_site) inside a design box:
 
-* forward: the plain fused step (``run_steps``), saving (fields, CPML
-  memories) at every checkpoint;
-* backward, segment by segment from the last: restore the checkpoint,
-  recompute the segment's steps while ``fdtd_adjoint_curl`` stores the curl of
-  each active E component over the box after every step, then apply
-  ``fdtd_adjoint_step`` for the segment's steps in reverse.  Each adjoint step
+* forward: the plain fused step (``run_steps``).  A field recorder in the
+  forward program keeps H over the box (and a one-cell margin) after every
+  step when that fits ``curl_store_bytes``; otherwise the forward saves
+  (fields, CPML memories) every ``checkpoint_every`` steps;
+* backward, from the last step: the curl of each active E component over the
+  box comes from the recorded H (256 steps at a time), or, with checkpoints,
+  segment by segment from the last: restore the checkpoint and recompute the
+  segment's steps while ``fdtd_adjoint_curl`` stores the curl after every
+  step (the same differences and divisions, so the same bits).  Then
+  ``fdtd_adjoint_step`` runs for the steps in reverse.  Each adjoint step
   injects the DFT adjoint source of that step's sample, transposes the E and
   H updates exactly (CPML memories, ghost planes and metallic walls included)
   and accumulates dJ/dc += mu * curl over the box.
@@ -49,7 +52,8 @@ def _torch():
 class AdjointProblem:
     """One differentiable simulation (dense layout, per-site E material)."""
 
-    def __init__(self, spec: ProgramSpec, nsteps: int, box, checkpoint_every: int = 100, device="cuda"):
+    def __init__(self, spec: ProgramSpec, nsteps: int, box, checkpoint_every: int = 100, device="cuda",
+                 curl_store_bytes: int = 4 << 30):
         from . import runtime
 
         torch = _torch()
@@ -62,11 +66,6 @@ class AdjointProblem:
         self.nsteps = int(nsteps)
         self.every = max(1, int(checkpoint_every))
         self.lib = abi.load_library()
-        self.forward_program = runtime.compile_program(spec, device=device, schedule="fused", layout="dense")
-        self.adjoint_program = runtime.compile_program(spec, device=device, schedule="phases", layout="dense")
-        self.forward_program._times_for(self.nsteps + 1)
-        self.adjoint_program._times_for(self.nsteps + 1)
-        self.device = self.forward_program.device
         self.active = active_components(spec.ndim, spec.polarization)
         self.e_active = [c for c in ("Ex", "Ey", "Ez") if c in self.active]
         # The box in the 3D lattice frame (2D TM is the z = 1 slab).
@@ -75,8 +74,80 @@ class AdjointProblem:
             lo, hi = (0, *lo), (1, *hi)
         self.box_lo, self.box_hi = lo, hi
         self.box_shape = tuple(h - l for l, h in zip(lo, hi))
+        # The gradient needs the forward curl over the box after every step.
+        # When H over the box (and a one-cell margin) for every step fits in
+        # `curl_store_bytes`, a field recorder inside the forward program
+        # keeps it and the backward pass runs no forward steps; otherwise the
+        # backward recomputes each checkpoint segment (``checkpoint_every``).
+        self.curl_record = self._curl_recorder(spec, curl_store_bytes)
+        fspec = spec if self.curl_record is None else dataclasses.replace(
+            spec, recorders=[*spec.recorders, self.curl_record[0]])
+        self.forward_program = runtime.compile_program(fspec, device=device, schedule="fused", layout="dense")
+        self.adjoint_program = runtime.compile_program(spec, device=device, schedule="phases", layout="dense")
+        self.forward_program._times_for(self.nsteps + 1)
+        self.adjoint_program._times_for(self.nsteps + 1)
+        self.device = self.forward_program.device
         self.checkpoints = []
         self.dft = None
+
+    def _curl_recorder(self, spec: ProgramSpec, limit: int):
+        """(RecorderPlan, margin, extended shape) recording every active H
+        component on the box grown by one cell towards lower coordinates (z
+        only in 3D), or None when it does not fit `limit` bytes (with the curls
+        computed from it), a recorder slot, or the components' extents."""
+        from .plan import RecorderPlan
+
+        if len(spec.recorders) >= abi.FDTD_MAX_RECORDERS or self.nsteps < 1:
+            return None
+        h_active = [c for c in ("Hx", "Hy", "Hz") if c in self.active]
+        margin = (1 if spec.ndim == 3 else 0, 1, 1)
+        ext_lo = tuple(l - m for l, m in zip(self.box_lo, margin))
+        ext = tuple(h - l for l, h in zip(ext_lo, self.box_hi))
+        values = int(np.prod(ext))
+        need = 4 * self.nsteps * (values * len(h_active) + int(np.prod(self.box_shape)) * len(self.e_active))
+        if need > limit or min(ext_lo) < 0:
+            return None
+        kk, jj, ii = np.meshgrid(*(np.arange(l, h) for l, h in zip(ext_lo, self.box_hi)), indexing="ij")
+        idx, w = [], []
+        for c in h_active:
+            shape = component_shape(c, spec.grid_shape, spec.polarization)
+            shape = (1, *shape) if spec.ndim == 2 else tuple(shape)
+            if any(h > n for h, n in zip(self.box_hi, shape)):
+                return None
+            flat = (kk * shape[1] + jj) * shape[2] + ii
+            idx.append(flat.reshape(-1, 1).astype(np.int32))
+            w.append(np.ones((values, 1), np.float32))
+        plan = RecorderPlan(tuple(h_active), 1, self.nsteps, idx, w, shapes=(ext,) * len(h_active))
+        return plan, margin, ext
+
+    def _curls(self, state, s0: int, s1: int):
+        """The forward curl of every active E component over the box after
+        steps s0 .. s1-1, from the recorded H: fdtd_adjoint_curl's
+        differences and divisions in its order (a device-tensor divisor, so
+        every quotient is a correctly rounded division)."""
+        torch = _torch()
+        plan, margin, ext = self.curl_record
+        bufs = state.records[len(state.records) - 1]["values"]
+        h = {c: bufs[q][s0:s1].reshape((s1 - s0, *ext)) for q, c in enumerate(plan.components)}
+        res = torch.tensor(np.float32(self.spec.resolution), device=self.device)
+        bz, by, bx = self.box_shape
+        mz = margin[0]
+        C, Y, X = slice(mz, mz + bz), slice(1, 1 + by), slice(1, 1 + bx)
+        Cm, Ym, Xm = slice(mz - 1, mz - 1 + bz) if mz else None, slice(0, by), slice(0, bx)
+        out = [None] * 3
+        if "Ex" in self.e_active:
+            cu = (h["Hz"][:, C, Y, X] - h["Hz"][:, C, Ym, X]) / res
+            if "Hy" in h:
+                cu = cu - (h["Hy"][:, C, Y, X] - h["Hy"][:, Cm, Y, X]) / res
+            out[0] = cu
+        if "Ey" in self.e_active:
+            cu = -(h["Hz"][:, C, Y, X] - h["Hz"][:, C, Y, Xm]) / res
+            if "Hx" in h:
+                cu = cu + (h["Hx"][:, C, Y, X] - h["Hx"][:, Cm, Y, X]) / res
+            out[1] = cu
+        if "Ez" in self.e_active:
+            out[2] = (h["Hy"][:, C, Y, X] - h["Hy"][:, C, Y, Xm]) / res - (h["Hx"][:, C, Y, X] - h["Hx"][:, C, Ym, X]) / res
+        return [None if c is None else c.contiguous() for c in out]
 
     # -- coefficients ---------------------------------------------------------
     def set_coefficients(self, coefs: dict) -> None:
@@ -110,7 +181,8 @@ class AdjointProblem:
         self.checkpoints = []
         done = 0
         while done < self.nsteps:
-            self.checkpoints.append(self._snapshot(state))
+            if self.curl_record is None:  # the backward pass recomputes from these
+                self.checkpoints.append(self._snapshot(state))
             n = min(self.every, self.nsteps - done)
             rt.run_steps(state, self.forward_program, n)
             done += n
@@ -148,7 +220,7 @@ class AdjointProblem:
         torch = _torch()
         rt = self.runtime
         dev = self.device
-        if not self.checkpoints:
+        if self.dft is None:
             raise RuntimeError("run forward() first")
         shapes = self.adjoint_program.shapes
         lam = rt.initial_state(self.adjoint_program)  # adjoint fields and memories, zero
@@ -169,6 +241,18 @@ class AdjointProblem:
         for c in self.e_active:
             grads[COMPONENT_INDEX[c]] = torch.zeros(self.box_shape, dtype=torch.float32, device=dev)
         stream = rt._stream(prog)
+        if self.curl_record is not None:  # curls from the forward's recorded H, 256 steps at a time
+            for s1 in range(self.nsteps, 0, -256):
+                s0 = max(0, s1 - 256)
+                curl_all = self._curls(self._state, s0, s1)
+                for n in reversed(range(s0, s1)):
+                    curls = [None if c is None else c[n - s0] for c in curl_all]
+                    a = self._step_struct(n, scratch_e, scratch_h, g_re, g_im, curls, grads)
+                    s = prog.fill(lam, 0)
+                    abi.check(self.lib.fdtd_adjoint_step(stream, ctypes.byref(s), ctypes.byref(a)),
+                              "fdtd_adjoint_step")
+                del curl_all
+            return self._finish(lam, grads)
         fprog = self.forward_program
         rstate = rt.initial_state(fprog)
         nseg = len(self.checkpoints)
@@ -190,6 +274,13 @@ class AdjointProblem:
                 abi.check(self.lib.fdtd_adjoint_step(stream, ctypes.byref(s), ctypes.byref(a)), "fdtd_adjoint_step")
             del curls
         rstate.check()
+        return self._finish(lam, grads)
+
+    def _finish(self, lam, grads):
+        torch = _torch()
+        shapes = self.adjoint_program.shapes
+        dev = self.device
+        lam.check()
         self.lambda_state = lam
         out = {}
         lo, hi = self.box_lo, self.box_hi
