@@ -284,9 +284,17 @@ __global__ void __launch_bounds__(kAdjThreads) adj_curl_kernel(Step3D p, AdjDev 
   }
 }
 
+// Grid-stride launches of 16 blocks per SM: each thread then takes a few
+// dozen elements of a large component rather than one, so block scheduling
+// does not dominate these short per-element passes.
 unsigned blocks_for(int64_t n) {
+  int dev = 0, sms = 0;  // the current device's SM count (a cheap attribute query)
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      sms <= 0)
+    sms = 148;
   const int64_t b = (n + kAdjThreads - 1) / kAdjThreads;
-  return static_cast<unsigned>(b < 1 ? 1 : (b > 65535 * 4 ? 65535 * 4 : b));
+  const int64_t cap = static_cast<int64_t>(sms) * 16;
+  return static_cast<unsigned>(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
 }  // namespace
