@@ -85,6 +85,56 @@ def _ports(ports) -> dict:
     return {p.name: p for p in values}
 
 
+def monitor_projection_phase(component: str, frequencies, dt: float) -> np.ndarray:
+    """Phase that aligns a monitor's DFT phasors to the E sample time
+    (beamz/analysis/modal_projection/geometry.py:41-60): exp(-i pi f dt) for
+    H components (stored half a step earlier), 1 for E."""
+    f = np.atleast_1d(np.asarray(frequencies, dtype=float))
+    if str(component).startswith("H"):
+        return np.exp(-1j * np.pi * f * float(dt))
+    return np.ones_like(f, dtype=np.complex128)
+
+
+def port_projection(e_profile, h_profile, measure, signed_flux_sign: float) -> dict:
+    """Least-squares projection of a port's (E, H) DFT fields onto its
+    forward and backward mode (beamz/analysis/mode_projection.py:485-535, the
+    2D port projection after the mode solve): the solved tangential profiles
+    normalised to unit power 0.5 Re sum w s E conj(H), the mode matrix of the
+    forward [E; H] and backward [E; -H] fields, and its pseudo-inverse,
+    weighted by sqrt(w) when ``measure`` is per point.  The profiles come from
+    a mode solver, which is outside this engine."""
+    e = np.asarray(e_profile, dtype=np.complex128)
+    h = np.asarray(h_profile, dtype=np.complex128)
+    measure = np.asarray(measure, dtype=float)
+    weights = measure if measure.ndim == 0 else measure.reshape(-1)[: e.size]
+    power = 0.5 * np.real(np.sum(weights * signed_flux_sign * e * np.conjugate(h)))
+    norm = np.sqrt(max(abs(power), 1e-30))
+    e_fwd, h_fwd = e / norm, h / norm
+    mode_matrix = np.column_stack([np.concatenate([e_fwd, h_fwd]), np.concatenate([e_fwd, -h_fwd])])
+    out = {"mode_matrix": mode_matrix, "condition_number": float(np.linalg.cond(mode_matrix))}
+    if np.ndim(weights) == 0:  # uniform measure: the unweighted solve, as beamz keeps it
+        out["pinv"] = np.linalg.pinv(mode_matrix)
+    else:
+        pw = np.concatenate([np.broadcast_to(np.sqrt(weights), e_fwd.shape),
+                             np.broadcast_to(np.sqrt(weights), h_fwd.shape)])
+        out["pinv"] = np.linalg.pinv(pw[:, None] * mode_matrix)
+        out["projection_weights"] = pw
+    return out
+
+
+def project_waves(projection: dict, e_values, h_values) -> tuple[complex, complex]:
+    """(a_plus, a_minus) of one frequency: the projection's pseudo-inverse
+    applied to the weighted field vector [E; H] (beamz/analysis/sparameters.py
+    377-393).  ``e_values`` / ``h_values`` are the monitor's DFT values of the
+    port's components (``runtime.monitor_values``) with beamz's phase
+    alignment applied (:func:`monitor_projection_phase`, and in 2D the
+    modal-plane delay)."""
+    field_vec = np.concatenate([np.asarray(e_values, dtype=np.complex128), np.asarray(h_values, dtype=np.complex128)])
+    weights = np.asarray(projection.get("projection_weights", np.ones(field_vec.size)), dtype=float)
+    coeff = projection["pinv"] @ (weights * field_vec)
+    return coeff[0], coeff[1]
+
+
 def modal_flux_diagnostics(ports, waves: dict, frequencies, is_3d: bool = True, monitor_flux=None) -> dict:
     """Per port: the modal powers of both branches, the selected (scattered)
     and rejected ones, and their differences from the monitor's DFT flux

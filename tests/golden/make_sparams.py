@@ -12,6 +12,12 @@ return seeded port waves and monitor records.  ``s_parameters``
 (sparameters.py:424-566) then runs its own wave selection, incident floor,
 ratios, power balance and ``_modal_dft_flux_diagnostics`` (581-644) on them.
 
+It also loads ``beamz/analysis/mode_projection.py`` (its solver and geometry
+imports stood in for) and runs ``_build_port_projection_2d`` (485-535: power
+normalisation, mode matrix, pseudo-inverse) with the mode solver replaced by
+seeded profiles, then the coefficient step of sparameters.py:377-393 on
+seeded field vectors.
+
 Writes ``tests/golden/sparams.npz``.
 """
 
@@ -32,6 +38,8 @@ CASES = (
     ("c3z", True, (("a", "z", "-"), ("b", "z", "+")), "a", ("b",), -20.0),
     ("c2", False, (("p1", "x", "+"), ("p2", "y", "-")), "p2", None, -30.0),
 )
+# (tag, points, measure: "scalar" or "array", signed flux sign)
+PROJ_CASES = (("pu", 23, "scalar", -1.0), ("pw", 31, "array", 1.0))
 DIAG_KEYS = ("P_in", "P_guided_out", "power_sum", "loss_est", "valid_mask")
 FLUX_KEYS = ("monitor_flux", "P_plus", "P_minus", "P_modal_sum", "P_modal_net", "P_selected", "P_rejected",
              "P_selected_modal_net", "flux_minus_modal_net", "flux_minus_selected_modal_net",
@@ -107,6 +115,39 @@ def main(argv=None) -> None:
             for key in FLUX_KEYS:
                 data[f"{tag}_{name}_{key}"] = np.asarray(entry[key])
             data[f"{tag}_{name}_incident"] = np.asarray(entry["incident_wave"])
+    _stub("beamz.analysis.modal_projection.colocation", _discrete_mode_projection_grids_3d=None)
+    _stub("beamz.analysis.modal_projection.diagnostics",
+          _modal_projection_reconstruction_diagnostics_from_matrix=None)
+    _stub("beamz.analysis.modal_projection.geometry", _analysis_plane_sample_area=None,
+          _modal_projection_plane_delay_s=None, _mode_components_for_port=None, _monitor_analysis_plane_3d=None)
+    _stub("beamz.analysis.data", AnalysisData=object)
+    _stub("beamz.devices._placement", line_region_points=None, snap_axis_aligned_line_region_grid=None,
+          snap_plane_region_grid=None)
+    _stub("beamz.devices.modes")
+    _stub("beamz.devices.modes.discrete", DISCRETE_MODE_CONTRACT=None, solve_beamz_mode=None)
+    _stub("beamz.devices.modes.fields", _modal_overlap=None, _normalize_profiles=None)
+    _stub("beamz.devices.modes.plane", solve_mode_plane_3d=None, solve_modes=None)
+    _stub("beamz.devices.monitors")
+    _stub("beamz.devices.monitors.monitors", ModeMonitor=object)
+    mp = _load("beamz.analysis.mode_projection", "beamz/analysis/mode_projection.py")
+    for tag, n, kind, sign in PROJ_CASES:
+        e = (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * 3.0
+        h = (rng.standard_normal(n) + 1j * rng.standard_normal(n)) * 0.01
+        dl = np.float64(2e-8) if kind == "scalar" else rng.uniform(1e-8, 3e-8, n)
+        mp._monitor_profile_slice = lambda *_a, n=n, dl=dl: (np.ones(n), np.arange(n), dl)
+        mp.solve_modes = lambda *_a, e=e, h=h, **_k: ([1.7], [[e]], [[h]], None)
+        mp._modal_projection_plane_delay_s = lambda *_a: 0.0
+        spec = types.SimpleNamespace(mode_index=0, projection_direction="+", polarization=None, name=tag)
+        parts = {"axis": "x", "e_mode_index": 0, "h_mode_index": 0, "signed_flux_sign": sign,
+                 "e_component": "Ez", "h_component": "Hy"}
+        proj = mp._build_port_projection_2d(types.SimpleNamespace(resolution=2e-8), spec=spec, monitor=None,
+                                            frequency=1.9e14, parts=parts, mode_pad_cells=0)
+        field_vec = rng.standard_normal(2 * n) + 1j * rng.standard_normal(2 * n)
+        pw = np.asarray(proj.get("projection_weights", np.ones(field_vec.size)), dtype=float)
+        coeff = proj["pinv"] @ (pw * field_vec)
+        data.update({f"{tag}_e": e, f"{tag}_h": h, f"{tag}_dl": np.asarray(dl), f"{tag}_field": field_vec,
+                     f"{tag}_mode_matrix": proj["mode_matrix"], f"{tag}_pinv": proj["pinv"],
+                     f"{tag}_cond": np.float64(proj["condition_number"]), f"{tag}_coeff": coeff})
     np.savez(args.out, **data)
     print(f"wrote {args.out} ({len(data)} arrays)")
 

@@ -52,3 +52,29 @@ def test_wave_selectors():
         S.PortSpec("p", "w")
     with pytest.raises(ValueError):
         S.s_parameters({}, [S.PortSpec("a", "x")], "b", frequencies=[1.0])
+
+
+@pytest.mark.parametrize("case", ["pu", "pw"])
+def test_port_projection_matches_the_reference(case):
+    """The 2D port projection after the mode solve (power normalisation, mode
+    matrix, pseudo-inverse, sqrt-measure weighting) and the coefficient step,
+    against the reference's ``_build_port_projection_2d`` run on the same
+    seeded profiles (the pseudo-inverse is an SVD: 1e-12 relative)."""
+    g = np.load(GOLDEN)
+    dl = g[f"{case}_dl"]
+    sign = -1.0 if case == "pu" else 1.0
+    proj = S.port_projection(g[f"{case}_e"], g[f"{case}_h"], dl if dl.ndim else float(dl), sign)
+    np.testing.assert_array_equal(proj["mode_matrix"], g[f"{case}_mode_matrix"])
+    np.testing.assert_allclose(proj["pinv"], g[f"{case}_pinv"], rtol=1e-12, atol=0)
+    assert proj["condition_number"] == pytest.approx(float(g[f"{case}_cond"]), rel=1e-12)
+    assert ("projection_weights" in proj) == (case == "pw")
+    n = g[f"{case}_e"].size
+    field = g[f"{case}_field"]
+    a_plus, a_minus = S.project_waves(proj, field[:n], field[n:])
+    np.testing.assert_allclose([a_plus, a_minus], g[f"{case}_coeff"], rtol=1e-12, atol=0)
+
+
+def test_monitor_projection_phase():
+    f = np.array([1.9e14, 2.0e14])
+    np.testing.assert_array_equal(S.monitor_projection_phase("Ez", f, 3e-17), np.ones(2))
+    np.testing.assert_array_equal(S.monitor_projection_phase("Hy", f, 3e-17), np.exp(-1j * np.pi * f * 3e-17))
