@@ -91,3 +91,44 @@ def test_device_flux_of_a_2d_line_monitor():
     got = R.monitor_dft_flux(st, prog, 0, "x", measure=20e-9)
     want = O.monitor_dft_flux(_normalised(st, prog, 0, None), "x", 1.0, None, measure=20e-9)
     np.testing.assert_allclose(got, want, rtol=1e-10)
+
+
+def test_s_parameters_from_device_dft_values():
+    """The S-parameter path on a device run: two x-normal lines of a 2D TM
+    scene, their DFT values (Ez, Hy phase-aligned) projected on a mode that is
+    the input line's own field, then assembled.  Projecting a field on itself
+    gives a pure forward wave (a_plus = its power normalisation, a_minus = 0),
+    so the input port reflects nothing."""
+    from beamz_b200 import sparameters as S
+    from beamz_b200 import workloads as W
+
+    spec = W.scene_2d(total_steps=240, seed=2, shape=(96, 96), pml_cells=10, n_monitors=2)
+    prog = R.compile_program(spec)
+    st = R.initial_state(prog)
+    R.run_steps(st, prog, 240)
+    freqs = np.asarray(spec.monitors[0].freqs, dtype=float)
+    dl = float(spec.resolution)
+    fields = []
+    for m in range(2):
+        v = R.monitor_values(st, prog, m)
+        fields.append((v["Ez"], v["Hy"] * S.monitor_projection_phase("Hy", freqs, spec.dt)[:, None]))
+    waves = {"in": {"a_plus": [], "a_minus": []}, "out": {"a_plus": [], "a_minus": []}}
+    e_in, h_in = fields[0]
+    for f in range(len(freqs)):
+        proj = S.port_projection(e_in[f], h_in[f], dl, -1.0)
+        power = 0.5 * np.real(np.sum(dl * -1.0 * e_in[f] * np.conjugate(h_in[f])))
+        for name, (e, h) in zip(("in", "out"), fields):
+            ap, am = S.project_waves(proj, e[f], h[f])
+            waves[name]["a_plus"].append(ap)
+            waves[name]["a_minus"].append(am)
+        assert abs(waves["in"]["a_plus"][-1] - np.sqrt(abs(power))) <= 1e-9 * np.sqrt(abs(power))
+        assert abs(waves["in"]["a_minus"][-1]) <= 1e-9 * np.sqrt(abs(power))
+    flux = {p: R.monitor_dft_flux(st, prog, m, "x", measure=dl) for m, p in enumerate(("in", "out"))}
+    ports = [S.PortSpec("in", "x", "+"), S.PortSpec("out", "x", "+")]
+    res = S.s_parameters(waves, ports, "in", frequencies=freqs, is_3d=False, monitor_flux=flux)
+    assert res.diagnostics["valid_mask"].all()
+    assert np.abs(res.s_matrix[("in", "in")]).max() <= 1e-9
+    s21 = res.s_matrix[("out", "in")]
+    assert np.isfinite(s21).all() and np.abs(s21).max() > 0
+    np.testing.assert_allclose(res.diagnostics["P_in"], np.abs(np.asarray(waves["in"]["a_plus"])) ** 2)
+    assert np.isfinite(res.diagnostics["monitor_flux_checks"]["out"]["monitor_flux"]).all()
