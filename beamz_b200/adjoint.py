@@ -59,8 +59,6 @@ class AdjointProblem:
         torch = _torch()
         if spec.e_site is None:
             raise ValueError("the adjoint needs a per-site E material (ProgramSpec.e_site)")
-        if spec.metrics is not None:
-            raise ValueError("the adjoint step is the transpose of the isotropic-grid step (no derivative metrics)")
         self.runtime = runtime
         self.spec = spec
         self.nsteps = int(nsteps)
@@ -134,20 +132,47 @@ class AdjointProblem:
         mz = margin[0]
         C, Y, X = slice(mz, mz + bz), slice(1, 1 + by), slice(1, 1 + bx)
         Cm, Ym, Xm = slice(mz - 1, mz - 1 + bz) if mz else None, slice(0, by), slice(0, bx)
+        me = self._box_metrics()
+
+        def sc(diff, axis):  # divided by the cell size, or times the box's E-side inverse distances
+            return diff / res if me[axis] is None else diff * me[axis]
+
         out = [None] * 3
         if "Ex" in self.e_active:
-            cu = (h["Hz"][:, C, Y, X] - h["Hz"][:, C, Ym, X]) / res
+            cu = sc(h["Hz"][:, C, Y, X] - h["Hz"][:, C, Ym, X], 1)
             if "Hy" in h:
-                cu = cu - (h["Hy"][:, C, Y, X] - h["Hy"][:, Cm, Y, X]) / res
+                cu = cu - sc(h["Hy"][:, C, Y, X] - h["Hy"][:, Cm, Y, X], 0)
             out[0] = cu
         if "Ey" in self.e_active:
-            cu = -(h["Hz"][:, C, Y, X] - h["Hz"][:, C, Y, Xm]) / res
+            cu = -sc(h["Hz"][:, C, Y, X] - h["Hz"][:, C, Y, Xm], 2)
             if "Hx" in h:
-                cu = cu + (h["Hx"][:, C, Y, X] - h["Hx"][:, Cm, Y, X]) / res
+                cu = cu + sc(h["Hx"][:, C, Y, X] - h["Hx"][:, Cm, Y, X], 0)
             out[1] = cu
         if "Ez" in self.e_active:
-            out[2] = (h["Hy"][:, C, Y, X] - h["Hy"][:, C, Y, Xm]) / res - (h["Hx"][:, C, Y, X] - h["Hx"][:, C, Ym, X]) / res
+            out[2] = sc(h["Hy"][:, C, Y, X] - h["Hy"][:, C, Y, Xm], 2) - sc(h["Hx"][:, C, Y, X] - h["Hx"][:, C, Ym, X], 1)
         return [None if c is None else c.contiguous() for c in out]
+
+    def _box_metrics(self):
+        """Per axis (z, y, x) the E-side inverse distances of a derivative
+        metric over the box, shaped to broadcast against [steps, z, y, x], or
+        None (the isotropic grid, or z in 2D)."""
+        torch = _torch()
+        out = [None, None, None]
+        metrics = self.spec.metrics
+        if metrics is None:
+            return out
+        cells = tuple(int(v) for v in self.spec.grid_shape)
+        names = ("z", "y", "x") if self.spec.ndim == 3 else (None, "y", "x")
+        if self.spec.ndim == 2:
+            cells = (1, *cells)
+        for a, name in enumerate(names):
+            if name is None:
+                continue
+            m = np.asarray(metrics.along(f"h_to_e_{name}", cells[a] + 1), np.float32)[self.box_lo[a]:self.box_hi[a]]
+            shape = [1, 1, 1, 1]
+            shape[1 + a] = m.size
+            out[a] = torch.as_tensor(m.reshape(shape), device=self.device)
+        return out
 
     # -- coefficients ---------------------------------------------------------
     def set_coefficients(self, coefs: dict) -> None:

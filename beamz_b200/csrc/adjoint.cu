@@ -22,6 +22,10 @@
 //   B^T:   (B^T t)[h] = (r(h) t[h] - r(h+1) t[h+1]) / res, r(m) = 1 for the
 //          rows of B that difference two samples or a metallic ghost, 0 for
 //          the rows whose edge-copy ghost makes them zero.
+//   With derivative metrics (axis-uniform / rectilinear grids) each
+//   difference carries its coordinate's inverse distance instead of 1/res:
+//   (D^T u)[m] = mh[m-1] u[m-1] - mh[m] u[m] and
+//   (B^T t)[h] = r(h) me[h] t[h] - r(h+1) me[h+1] t[h+1].
 // Each transpose is split into a per-target pass that writes lam_d into a
 // scratch array (one per derivative term) and a per-source gather, so no
 // two threads write one element.  The permittivity gradient accumulates
@@ -132,7 +136,13 @@ __global__ void __launch_bounds__(kAdjThreads) adj_hgather_kernel(Step3D p, AdjD
       const int k1 = axis == 0 ? k + 1 : k, j1 = axis == 1 ? j + 1 : j, i1 = axis == 2 ? i + 1 : i;
       const float t0 = row(m) ? a.scratch_e[t][lin(de, k, j, i)] : 0.0f;
       const float t1 = row(m + 1) ? a.scratch_e[t][lin(de, k1, j1, i1)] : 0.0f;
-      acc += (t0 - t1) * inv_res;
+      // Derivative metrics: the backward difference at E coordinate m was
+      // scaled by metric_e[m] (and the ghost rows by metric_e[0] / [N]).
+      const float* me = p.metric_e[axis];
+      if (me != nullptr)
+        acc += t0 * me[m] - t1 * me[m + 1];
+      else
+        acc += (t0 - t1) * inv_res;
     }
     a.lam[h][idx] += acc;
   }
@@ -184,7 +194,13 @@ __global__ void __launch_bounds__(kAdjThreads) adj_egather_kernel(Step3D p, AdjD
       const int k0 = axis == 0 ? k - 1 : k, j0 = axis == 1 ? j - 1 : j, i0 = axis == 2 ? i - 1 : i;
       const float u_prev = m >= 1 ? a.scratch_h[t][lin(dh, k0, j0, i0)] : 0.0f;
       const float u_here = m <= N - 1 ? a.scratch_h[t][lin(dh, k, j, i)] : 0.0f;
-      acc += (u_prev - u_here) * inv_res;
+      // Derivative metrics: the forward difference at H coordinate m was
+      // scaled by metric_h[m].
+      const float* mh = p.metric_h[axis];
+      if (mh != nullptr)
+        acc += (m >= 1 ? u_prev * mh[m - 1] : 0.0f) - (m <= N - 1 ? u_here * mh[m] : 0.0f);
+      else
+        acc += (u_prev - u_here) * inv_res;
     }
     a.lam[e][idx] += acc;
   }
@@ -270,15 +286,22 @@ __global__ void __launch_bounds__(kAdjThreads) adj_curl_kernel(Step3D p, AdjDev 
     const float* Hx = p.hin[0];
     const float* Hy = p.hin[1];
     const float* Hz = p.hin[2];
+    // A backward difference along `axis` at E coordinate `at`: divided by the
+    // cell size, or times the derivative metric there.
+    auto sc = [&](float diff, int axis, int at) {
+      const float* me = p.metric_e[axis];
+      return me != nullptr ? diff * me[at] : diff / res;
+    };
     float curl;
     if (c == 0) {
-      curl = (Hz[lin(dz, k, j, i)] - Hz[lin(dz, k, j - 1, i)]) / res;
-      if (Hy) curl -= (Hy[lin(dy, k, j, i)] - Hy[lin(dy, k - 1, j, i)]) / res;
+      curl = sc(Hz[lin(dz, k, j, i)] - Hz[lin(dz, k, j - 1, i)], 1, j);
+      if (Hy) curl -= sc(Hy[lin(dy, k, j, i)] - Hy[lin(dy, k - 1, j, i)], 0, k);
     } else if (c == 1) {
-      curl = -(Hz[lin(dz, k, j, i)] - Hz[lin(dz, k, j, i - 1)]) / res;
-      if (Hx) curl += (Hx[lin(dx, k, j, i)] - Hx[lin(dx, k - 1, j, i)]) / res;
+      curl = -sc(Hz[lin(dz, k, j, i)] - Hz[lin(dz, k, j, i - 1)], 2, i);
+      if (Hx) curl += sc(Hx[lin(dx, k, j, i)] - Hx[lin(dx, k - 1, j, i)], 0, k);
     } else {
-      curl = (Hy[lin(dy, k, j, i)] - Hy[lin(dy, k, j, i - 1)]) / res - (Hx[lin(dx, k, j, i)] - Hx[lin(dx, k, j - 1, i)]) / res;
+      curl = sc(Hy[lin(dy, k, j, i)] - Hy[lin(dy, k, j, i - 1)], 2, i) -
+             sc(Hx[lin(dx, k, j, i)] - Hx[lin(dx, k, j - 1, i)], 1, j);
     }
     a.curl[c][b] = curl;
   }

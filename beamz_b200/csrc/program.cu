@@ -868,7 +868,6 @@ bool f32_sized(const FdtdBuffer& b, int64_t n) { return is_f32(b) && b.data != n
 int check_adjoint(const FdtdProgram& p, const FdtdAdjointStep& a, const Layout& L, bool need_box) {
   if (a.abi_version != FDTD_ABI_VERSION) return kInvalid;
   if (p.layout != FDTD_LAYOUT_DENSE) return kInvalid;
-  if (has_metric(p)) return kInvalid;  // the transpose is written for the isotropic step
   const int64_t bz = a.box_hi[0] - a.box_lo[0], by = a.box_hi[1] - a.box_lo[1], bx = a.box_hi[2] - a.box_lo[2];
   bool any_box = false;
   for (int c = 0; c < 3; ++c) any_box = any_box || a.curl[c].data != nullptr || a.grad[c].data != nullptr;

@@ -43,15 +43,19 @@ def _dot(a_list, b_list):
                for a, b in zip(a_list, b_list))
 
 
-@pytest.mark.parametrize("case", ["2d", "2d_pec", "3d", "3d_pec"])
+@pytest.mark.parametrize("case", ["2d", "2d_pec", "3d", "3d_pec", "2d_metric", "3d_metric"])
 def test_adjoint_step_is_the_exact_transpose(case):
-    """<lambda', A u> == <A^T lambda', u> over fields and CPML memories."""
+    """<lambda', A u> == <A^T lambda', u> over fields and CPML memories
+    (isotropic and rectilinear grids)."""
     torch = _torch()
     from beamz_b200 import runtime as R
+    from tests.scenarios import with_metrics
 
     metallic = ("left", "top", "front") if case.endswith("pec") else ()
     spec = _site_2d((40, 48), 3, metallic) if case.startswith("2d") else _site_3d((14, 20, 36), 4, 3, metallic)
     spec = dataclasses.replace(spec, sources=[], monitors=[])
+    if case.endswith("metric"):
+        spec = with_metrics(spec, "rectilinear", seed=2)
     fprog = R.compile_program(spec, schedule="fused", layout="dense")
     aprog = R.compile_program(spec, schedule="phases", layout="dense")
     rng = np.random.default_rng(11)
@@ -122,12 +126,16 @@ def _objective_2d(spec):
     return J
 
 
-def test_gradient_2d_matches_finite_differences():
+@pytest.mark.parametrize("grid", ["uniform", "rectilinear"])
+def test_gradient_2d_matches_finite_differences(grid):
     torch = _torch()
     from beamz_b200 import adjoint as A
+    from tests.scenarios import with_metrics
 
     ny = nx = 64
     spec = W.scene_2d(total_steps=420, seed=5, shape=(ny, nx), pml_cells=8, n_monitors=1)
+    if grid != "uniform":
+        spec = with_metrics(spec, grid, seed=4)
     box = ((24, 20), (40, 36))  # Ez sites (y, x), interior, clear of the absorber
     eps_bg = torch.full((ny, nx), W.OXIDE, device="cuda")
     gen = torch.Generator(device="cpu").manual_seed(0)
@@ -187,7 +195,7 @@ def test_gradient_3d_matches_finite_differences():
     assert abs(fd - ad) <= 1e-3 * abs(fd), (fd, ad)
 
 
-@pytest.mark.parametrize("dims", ["2d", "3d"])
+@pytest.mark.parametrize("dims", ["2d", "3d", "3d_metric"])
 def test_recorded_curls_give_the_recomputed_gradient(dims):
     """The backward pass that reads the forward curl from H recorded over the
     box every step (no forward steps in the backward) returns the gradient of
@@ -204,6 +212,10 @@ def test_recorded_curls_give_the_recomputed_gradient(dims):
         coefs = [A.eps_to_coefficients_2d(eps, spec.dt, P.EPS_0)]
     else:
         spec = _site_3d((20, 28, 40), 6)
+        if dims == "3d_metric":
+            from tests.scenarios import with_metrics
+
+            spec = with_metrics(spec, "rectilinear", seed=5)
         nsteps, box = 200, ((7, 9, 12), (13, 19, 28))
         coefs = [torch.as_tensor(spec.e_site[c][1], device="cuda") for c in ("Ex", "Ey", "Ez")]
     grads = []

@@ -168,13 +168,3 @@ def test_validate_rejects_inconsistent_metric_buffers(lib, mutate):
     s, fk = _with_metrics()
     mutate(s, fk)
     assert lib.fdtd_validate(ctypes.byref(s)) == 1
-
-
-def test_adjoint_refuses_metric_programs():
-    pytest.importorskip("torch")
-    from beamz_b200 import adjoint
-    from tests.scenarios import scenario_2d, with_metrics
-
-    spec = with_metrics(scenario_2d(grid=(9, 11), polarization="tm"))
-    with pytest.raises(ValueError, match="metric"):
-        adjoint.AdjointProblem(spec, 4, box=((0, 0, 0), (1, 2, 2)))
