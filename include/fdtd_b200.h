@@ -284,7 +284,8 @@ typedef struct FdtdProgram {
    * backward differences of the E update at each E coordinate (an axis-uniform
    * grid repeats one value).  FDTD_LAYOUT_DENSE, or FDTD_LAYOUT_PITCHED with
    * FDTD_FLAG_CLASSES and neither FDTD_FLAG_FAST_MATH nor FDTD_FLAG_LOSSY (the
-   * class step, 128 x 8 tiles whatever tile_y asks); no adjoint. */
+   * class step, 128 x 8 tiles whatever tile_y asks).  The adjoint entry points
+   * take them on FDTD_LAYOUT_DENSE. */
   FdtdBuffer metric_h[3];
   FdtdBuffer metric_e[3];
   /* Field recorders, run after each step's DFT sample (see FdtdRecorder). */
